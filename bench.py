@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Benchmark of the forward photon + volumetric single-scatter pass on B200.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+                    [--workload prism|rainbow]
+
+One step = one pass of the hot path over one batch: trace the workload's
+photons into the 64-bit spectral film, then the sensor reduction drains the
+film into an f32 XYZ image.  Prints one JSON line (rank 0).
+
+* value: photons/s with the scene resident in HBM (device-pointer ABI on the
+  timing stream; L2 flushed between steps; max over ranks; weak scaling, each
+  rank traces its own photon index range, no data-path collective);
+* e2e: the same metric through the GpuPhotonFilm-shaped ABI object with host
+  buffers: scene upload, trace, sensor reduce, XYZ read back, film clear;
+* roofline of the dominant kernel (the photon kernel), cpu_baseline from the
+  CPU restatement of the reference's point estimator (oracle) on this host.
+
+``--impl reference`` times the reference's CPU path (the oracle restatement of
+spectral-core's render_volumetric_scene_point, all host threads) on the same
+workload; the reference itself is Rust + wgpu and cannot be built or run here.
+"""
+import argparse
+import ctypes as C
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # SF11 prism (apex 60, side 1), 0.02 beam at 45 deg, 2^20
+    # photons, lambda U(380, 780), sigma_s 0.05, sigma_a 0, isotropic, 640x360x64.
+    "prism": dict(width=640, height=360, bins=64, photons=1 << 20, sigma_s=0.05, sigma_t=0.05, g=0.0,
+                  lambda_min=380.0, lambda_max=780.0, max_dist=6.0, max_bounces=8, seed=0xDED),
+    # water sphere r=1, beam width 2.2, 2^26 photons, up to 4
+    # internal bounces (6 surface interactions), sigma_s 0.02, 1920x1080x64.
+    "rainbow": dict(width=1920, height=1080, bins=64, photons=1 << 26, sigma_s=0.02, sigma_t=0.02, g=0.0,
+                    lambda_min=380.0, lambda_max=780.0, max_dist=8.0, max_bounces=6, seed=0x8A1B),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="prism")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps")
+    return ap.parse_args()
+
+
+def build_scene(wl):
+    import spectral_b200 as sb
+    from spectral_b200.scenes import prism_workload, rainbow_workload
+    cfg = WORKLOADS[wl]
+    if wl == "prism":
+        return prism_workload(cfg["width"], cfg["height"])
+    return rainbow_workload(cfg["width"], cfg["height"])
+
+
+# ----------------------------------------------------------------------------
+# CPU reference arm / baseline: the oracle's point estimator on all host cores
+# ----------------------------------------------------------------------------
+def run_cpu(wl, seconds, threads=None):
+    """Photons/s of the CPU restatement on a bounded sample of the workload."""
+    import oracle
+    cfg = WORKLOADS[wl]
+    scene, beam, cam = build_scene(wl)
+    prims, np_, planes, npl, mats, nm = scene.arrays()
+    osc = oracle.OScene(bytes(prims), np_, bytes(planes), npl, bytes(mats), nm, scene.background)
+    ob = oracle.or_beam.from_buffer_copy(bytes(beam.c))
+    oc = oracle.or_camera.from_buffer_copy(bytes(cam.c))
+    p = oracle.vol_params(cfg["width"], cfg["height"], cfg["seed"], cfg["sigma_s"], cfg["sigma_t"], cfg["g"],
+                          cfg["max_dist"], cfg["max_bounces"], cfg["lambda_min"], cfg["lambda_max"], bins=cfg["bins"])
+    threads = threads or os.cpu_count() or 1
+    film = np.zeros(cfg["width"] * cfg["height"] * cfg["bins"], np.int64)
+    fp = film.ctypes.data_as(C.POINTER(C.c_int64))
+    # calibrate on a small sample, then size the timed sample to ~`seconds`
+    n = 4096
+    while True:
+        t0 = time.perf_counter()
+        oracle.lib.or_render_point_mt(C.byref(osc.c), C.byref(oc), C.byref(ob), C.byref(p), None, 0, n, None, fp,
+                                      threads)
+        dt = time.perf_counter() - t0
+        if dt > 0.5 or n >= cfg["photons"]:
+            break
+        n *= 4
+    n_s = int(min(cfg["photons"], max(n, n * seconds / max(dt, 1e-6))))
+    film[:] = 0
+    t0 = time.perf_counter()
+    oracle.lib.or_render_point_mt(C.byref(osc.c), C.byref(oc), C.byref(ob), C.byref(p), None, 0, n_s, None, fp, threads)
+    dt = time.perf_counter() - t0
+    return n_s / dt, n_s, dt, threads
+
+
+def cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ----------------------------------------------------------------------------
+# clocks during the timed region
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid, self.proc, self.lines = uuid, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.uuid, "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nme, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nme)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+# ----------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    import spectral_b200 as sb
+    from spectral_b200 import _lib
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    cfg = WORKLOADS[args.workload]
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ctx = sb.GpuContext(local_rank)
+    scene, beam, cam = build_scene(args.workload)
+    W, H, B, N = cfg["width"], cfg["height"], cfg["bins"], cfg["photons"]
+    prims, np_, planes, npl, mats, nm = scene.arrays()
+
+    def dev_bytes(obj, n):
+        t = torch.frombuffer(bytearray(bytes(obj)[: n * C.sizeof(obj._type_)] or b"\0"), dtype=torch.uint8).to(dev)
+        return t
+
+    d_prims, d_planes, d_mats = dev_bytes(prims, np_), dev_bytes(planes, npl), dev_bytes(mats, nm)
+    opts = _lib.sc_film_options(B, cfg["lambda_min"], cfg["lambda_max"], cfg["max_bounces"], 32, 0)
+    desc = _lib.sc_trace_desc(d_prims.data_ptr(), np_, d_planes.data_ptr(), npl, d_mats.data_ptr(), nm, cam.c, beam.c,
+                              _lib.sc_vol_weights(cfg["sigma_s"], cfg["sigma_t"], cfg["g"]), W, H, cfg["seed"], 1,
+                              cfg["max_dist"], opts, None)
+    film = torch.zeros(_lib.lib.sc_film_bytes(W, H, B) // 8, dtype=torch.int64, device=dev)
+    flags = torch.zeros(_lib.lib.sc_film_flag_bytes(W, H) // 4, dtype=torch.int32, device=dev)
+    xyz = torch.empty(3 * W * H, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+    sp = C.c_void_p(stream.cuda_stream)
+    base = rank * N
+
+    def trace():
+        _lib.check(_lib.lib.sc_trace_photons_device(ctx.h, C.byref(desc), base, N, C.c_void_p(film.data_ptr()),
+                                                    C.c_void_p(flags.data_ptr()), sp))
+
+    def reduce():
+        _lib.check(_lib.lib.sc_sensor_reduce_device(ctx.h, W, H, B, cfg["lambda_min"], cfg["lambda_max"], 32,
+                                                    C.c_void_p(film.data_ptr()), C.c_void_p(flags.data_ptr()),
+                                                    C.c_void_p(xyz.data_ptr()), 1, sp))
+
+    # algorithmic work of one launch (instrumented pass, outside the timed region)
+    stats = torch.zeros(4, dtype=torch.int64, device=dev)
+    _lib.check(_lib.lib.sc_trace_stats_device(ctx.h, C.byref(desc), base, N, C.c_void_p(stats.data_ptr()), sp))
+    photons, segments, splats, scatters = [int(x) for x in stats.cpu()]
+
+    for _ in range(args.warmup):
+        trace()
+        reduce()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    with ClockSampler(uuid) as clk:
+        for k in range(args.steps):
+            flush.zero_()  # evict the film from L2 between steps (outside the events)
+            ev[k][0].record(stream)
+            trace()
+            ev[k][1].record(stream)
+            reduce()
+            ev[k][2].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms = [ev[k][0].elapsed_time(ev[k][2]) for k in range(args.steps)]
+    trace_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps)]
+    reduce_ms = [ev[k][1].elapsed_time(ev[k][2]) for k in range(args.steps)]
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = N * world * args.steps / (total_ms / 1e3)
+
+    # end to end through the GpuPhotonFilm-shaped ABI object with host buffers
+    e2e_steps = args.e2e_steps or args.steps
+    pf = sb.GpuPhotonFilm(ctx, scene, cam, beam, W, H, N, cfg["seed"], cfg["max_dist"],
+                          sb.VolWeights(cfg["sigma_s"], cfg["sigma_t"], cfg["g"]), bins=B,
+                          lambda_min=cfg["lambda_min"], lambda_max=cfg["lambda_max"],
+                          max_bounces=cfg["max_bounces"])
+    host_xyz = np.empty(3 * W * H, np.float32)
+    h2d = C.sizeof(prims._type_) * np_ + C.sizeof(planes._type_) * npl + C.sizeof(mats._type_) * nm + \
+        C.sizeof(cam.c) + C.sizeof(beam.c)
+
+    def e2e_step():
+        _lib.check(_lib.lib.sc_photon_film_set_scene(pf.h, prims, np_, planes, npl, mats, nm, C.byref(cam.c),
+                                                     C.byref(beam.c)))
+        _lib.check(_lib.lib.sc_photon_film_dispatch(pf.h, base, base + N, cfg["seed"]))
+        _lib.check(_lib.lib.sc_photon_film_read_accum(pf.h, host_xyz.ctypes.data_as(C.POINTER(C.c_float))))
+        _lib.check(_lib.lib.sc_photon_film_clear(pf.h))
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = N * world * e2e_steps / e2e_s
+    pf.close()
+
+    if rank != 0:
+        return None
+
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    peak_note = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    trace_s = statistics.mean(trace_ms) / 1e3
+    reduce_s = statistics.mean(reduce_ms) / 1e3
+    # dominant kernel: the photon kernel.  Algorithmic bytes = one 8-byte
+    # fixed-point payload per in-frame haze sample (its film atomic).
+    alg_bytes = splats * 8
+    cl = clk.summary()
+    sm_mhz = cl["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp32_peak = sms * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
+    # counted FP32 work (exp/pow counted as one op each): emission 20, intersect
+    # 14 per plane per segment, 60 per haze sample, 45 per scatter
+    flops = photons * 20 + segments * 14 * npl + segments * 4 * 60 + scatters * 45
+    film_bytes = W * H * B * 8
+    line = {
+        "metric": "photons/s @<=0.5% film err (forward + volumetric single scatter)",
+        "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 transport, int64 fixed-point film", "data": "synthetic (seeded scene)",
+        "config": {"workload": "%s: %s" % (args.workload, {"prism": "SF11 prism apex 60 side 1, beam 0.02 @45deg, "
+                                                                     "2^20 photons, 640x360x64 bins",
+                                                           "rainbow": "water sphere r=1, beam 2.2, 2^26 photons, "
+                                                                      "1920x1080x64 bins"}[args.workload]),
+                   "photons_per_step": N * world, "film": [W, H, B], "band_nm": [cfg["lambda_min"], cfg["lambda_max"]],
+                   "l2": "flushed between steps (256 MB write outside the timed events)",
+                   "parallelism": "photon ranges per rank, no collective"},
+        "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 3 * W * H * 4,
+                "path": "sc_photon_film_set_scene + dispatch + read_accum (host f32 XYZ) + clear"},
+        "gpu_launches": args.steps * 2,
+        "kernels": {"photon_ms": statistics.mean(trace_ms), "reduce_ms": statistics.mean(reduce_ms)},
+        "roofline": {"bound": "hbm", "achieved": alg_bytes / trace_s / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": alg_bytes / trace_s / 1e9 / hbm, "traffic": None, "kernel": "photon_kernel",
+                     "peak_source": "%s hbm_gbs" % peak_note,
+                     "algorithmic": "8 B per in-frame haze sample: %d samples per launch" % splats},
+        "roofline_fp32": {"kernel": "photon_kernel", "counted_flops": flops, "achieved_tflops": flops / trace_s / 1e12,
+                          "peak_tflops": fp32_peak, "frac": flops / trace_s / 1e12 / fp32_peak,
+                          "peak_source": "%d SMs x 128 FP32 lanes x 2 x %.0f MHz (sampled median)" % (sms, sm_mhz)},
+        "roofline_reduce": {"kernel": "reduce_kernel (drain)", "bound": "hbm",
+                            "achieved": 2 * film_bytes / reduce_s / 1e9, "peak": hbm, "unit": "GB/s",
+                            "frac": 2 * film_bytes / reduce_s / 1e9 / hbm,
+                            "algorithmic": "read + zero the whole film (dirty tiles only are touched)"},
+        "work": {"photons": photons, "segments": segments, "in_frame_samples": splats, "scatters": scatters},
+        "clocks": cl,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        rate, n_s, dt, th = run_cpu(args.workload, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": rate, "unit": "photons/s", "cores": th, "kind": "port",
+                                "sample": "first %d photons of the workload (%.1f s), %s" % (n_s, dt, cpu_model())}
+    return line
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        cfg = WORKLOADS[args.workload]
+        rates = []
+        for _ in range(args.warmup):
+            run_cpu(args.workload, 1.0)
+        for _ in range(args.steps):
+            rate, n_s, dt, th = run_cpu(args.workload, max(1.0, args.cpu_seconds / max(1, args.steps)))
+            rates.append((n_s, dt))
+        tot_n, tot_t = sum(n for n, _ in rates), sum(t for _, t in rates)
+        value = tot_n / tot_t
+        line = {"metric": "photons/s @<=0.5% film err (forward + volumetric single scatter)", "value": value,
+                "unit": "photons/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": tot_t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 transport", "data": "synthetic (seeded scene)", "impl": "reference",
+                "config": {"workload": args.workload, "photons_per_step": cfg["photons"],
+                           "film": [cfg["width"], cfg["height"], cfg["bins"]]},
+                "cpu_baseline": {"value": value, "unit": "photons/s", "cores": th, "kind": "port",
+                                 "sample": "per step the first %d photons of the workload; CPU restatement of "
+                                           "spectral-core render_volumetric_scene_point, %s" % (rates[0][0],
+                                                                                                 cpu_model())},
+                "e2e": {"value": value, "unit": "photons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    line = run_gpu(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

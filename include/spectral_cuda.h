@@ -1,0 +1,206 @@
+/*
+ * spectral_cuda.h -- C ABI of the B200 (sm_100a) spectral forward / volumetric /
+ * camera-tracer path.
+ *
+ * This is the drop-in boundary for the reference renderer's `spectral-gpu` crate
+ * (TSavo/spectral, Rust + wgpu).  Every entry point names the reference item it
+ * replaces (file:line in the reference checkout).  Conventions:
+ *   - every call returns an int status: SC_OK (0) or a negative SC_E_* code;
+ *     sc_last_error() returns a thread-local message for the last failure;
+ *   - handles are opaque; each handle owns one CUDA stream; calls on one handle
+ *     are serialised by a mutex, different handles may be used concurrently;
+ *   - host buffers are caller-allocated; sizes are in elements unless stated;
+ *   - no C++ exception crosses the ABI;
+ *   - the library never falls back to a CPU path: without a usable sm_100 device
+ *     sc_ctx_create fails with SC_E_CUDA.
+ *
+ * Films are 64-bit fixed point (value = count / 2^scale_log2): exact and
+ * independent of the order in which splats land.
+ */
+#ifndef SPECTRAL_CUDA_H
+#define SPECTRAL_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SC_OK 0
+#define SC_E_INVALID (-1)   /* bad argument (null pointer, size, range) */
+#define SC_E_CUDA (-2)      /* CUDA runtime error (message has the CUDA string) */
+#define SC_E_NOMEM (-3)     /* device allocation failed or HBM budget exceeded */
+#define SC_E_LIMIT (-4)     /* scene or film exceeds a documented compile-time limit */
+#define SC_E_TIMEOUT (-5)   /* a bounded device-side wait gave up */
+#define SC_E_STATE (-6)     /* call not valid in the handle's current state */
+
+/* ---- limits ------------------------------------------------------------ */
+#define SC_MAX_PRIMS 64
+#define SC_MAX_PLANES 256
+#define SC_MAX_BINS 256
+
+/* ---- plain data records ------------------------------------------------ */
+/* Scene records, byte-identical to spectral-gpu/src/upload.rs:7-32
+ * (GpuPrimitive 32 B, GpuMaterial 16 B, GpuPlane 16 B). */
+typedef struct { float center[3]; float radius; uint32_t plane_start, plane_count, kind, material; } sc_primitive; /* kind 0 sphere, 1 convex solid */
+typedef struct { float reflectance; uint32_t glass, kind, pad; } sc_material; /* kind 0 Lambertian, 1 dielectric; glass 0 BK7, 1 SF11, 2 water, 3 fused silica */
+typedef struct { float normal[3]; float d; } sc_plane;
+
+/* spectral-core/src/lighttrace.rs:116-121 (Beam). */
+typedef struct { float corner[3], u[3], v[3], dir[3]; } sc_beam;
+/* spectral-core/src/camera.rs:5-10 (Camera, the view_basis of camera.rs:36-38). */
+typedef struct { float origin[3], lower_left[3], horizontal[3], vertical[3]; } sc_camera;
+/* spectral-gpu/src/vol_photons.rs:256-267 (VolWeights). */
+typedef struct { float sigma_s, sigma_t, g; } sc_vol_weights;
+/* spectral-gpu/src/vol_photons.rs:85-93 (DebugPhotonGpu, 304 bytes). */
+typedef struct { uint32_t num_states; float lambda; uint32_t pad0, pad1; float states[18][4]; } sc_debug_photon;
+
+/* Film options beyond the reference: spectral binning and band.  Zero-initialise
+ * and set what you need; zeros select the reference's defaults. */
+typedef struct {
+    uint32_t bins;          /* 0: XYZ film (3 channels, the reference film); N>0: N spectral bins */
+    float lambda_min;       /* emission band start, nm (0 -> 380) */
+    float lambda_max;       /* emission band end, nm (0 -> 730) */
+    uint32_t max_bounces;   /* bounce loop length (0 -> 8, volume.rs:126) */
+    uint32_t scale_log2;    /* fixed-point scale 2^k (0 -> 32) */
+    uint32_t estimator;     /* 0 point estimator (volume.rs:99-168), 1 legacy isotropic (volume.rs:22-85) */
+} sc_film_options;
+
+/* ---- errors / context (spectral-gpu/src/lib.rs:21-41 GpuContext::new) ---- */
+const char* sc_last_error(void);
+const char* sc_version(void);
+typedef struct sc_ctx sc_ctx;
+/* tables: the 5x71 sensor table [xbar;71][ybar;71][zbar;71][d65;71][a;71]
+ * (spectral-gpu/src/data.rs:12-22 sample_tables). */
+int sc_ctx_create(int device, const float* tables_5x71, sc_ctx** out);
+int sc_ctx_destroy(sc_ctx* ctx);
+int sc_ctx_synchronize(sc_ctx* ctx);
+/* Parse the 5-column sensor CSV shipped with the library into a 5x71 table. */
+int sc_load_sensor_tables(const char* csv_path, float* out_5x71);
+
+/* ---- host helpers that mirror spectral-core constructors ---------------- */
+/* Camera::look_at (spectral-core/src/camera.rs:15-27). */
+int sc_camera_look_at(const float origin[3], const float target[3], const float up[3],
+                      float vfov_deg, float aspect, sc_camera* out);
+/* Glass::n (spectral-core/src/sellmeier.rs:28-44), f64 internally. */
+float sc_glass_n(uint32_t glass, float lambda_nm);
+/* Device RNG stream: n draws of PathRng(key, seed).next_u32() computed on the GPU
+ * into host `out` (the kernel of spectral-gpu/tests/rng_parity.rs:4-16). */
+int sc_rng_draws(sc_ctx* ctx, uint32_t key, uint32_t seed, uint32_t n, uint32_t* out);
+/* dsotm_scene (spectral-gpu/src/vol_photons.rs:188-222): writes 1 primitive,
+ * 5 planes, 1 material, the beam and the camera for the given aspect. */
+int sc_dsotm_scene(float aspect, sc_primitive* prim, sc_plane* planes5, sc_material* mat,
+                   sc_beam* beam, sc_camera* cam);
+
+/* ---- photon film: GpuPhotonFilm (spectral-gpu/src/vol_photons.rs:228-851) */
+typedef struct sc_photon_film sc_photon_film;
+/* GpuPhotonFilm::new (vol_photons.rs:275-573).  zbuffer: host, width*height
+ * floats, or NULL for no occlusion.  opts may be NULL (reference XYZ film). */
+int sc_photon_film_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims,
+                          const sc_plane* planes, uint32_t n_planes,
+                          const sc_material* mats, uint32_t n_mats, float background,
+                          const sc_camera* cam, const sc_beam* beam, uint32_t width,
+                          uint32_t height, uint32_t n_photons, uint32_t seed, float max_dist,
+                          const sc_vol_weights* weights, const float* zbuffer,
+                          const sc_film_options* opts, sc_photon_film** out);
+int sc_photon_film_destroy(sc_photon_film* f);
+/* trace_and_resolve (vol_photons.rs:582-585): photons [0, n_photons). */
+int sc_photon_film_trace_and_resolve(sc_photon_film* f, uint32_t n_photons, uint32_t seed);
+/* trace_chunked (vol_photons.rs:590-598). */
+int sc_photon_film_trace_chunked(sc_photon_film* f, uint32_t total_photons, uint32_t seed);
+/* dispatch_photons (vol_photons.rs:633-635): photons [photon_base, n_photons), asynchronous. */
+int sc_photon_film_dispatch(sc_photon_film* f, uint32_t photon_base, uint32_t n_photons, uint32_t seed);
+/* trace_debug (vol_photons.rs:727-779): records photons [0, debug_count); the
+ * film is not touched.  out: debug_count records. */
+int sc_photon_film_trace_debug(sc_photon_film* f, uint32_t n_photons, uint32_t seed,
+                               uint32_t debug_count, sc_debug_photon* out);
+/* set_spectral / spectral (vol_photons.rs:658-666). */
+int sc_photon_film_set_spectral(sc_photon_film* f, int on);
+int sc_photon_film_get_spectral(sc_photon_film* f, int* on);
+/* set the camera used by the next trace and by the rim pass. */
+int sc_photon_film_set_camera(sc_photon_film* f, const sc_camera* cam);
+/* recompute_surface (vol_photons.rs:685-714): rim pass for `cam` (NULL: current camera). */
+int sc_photon_film_recompute_surface(sc_photon_film* f, const sc_camera* cam);
+/* surface (vol_photons.rs:717-719): out 3*w*h interleaved XYZ. */
+int sc_photon_film_read_surface(sc_photon_film* f, float* out);
+/* accum (vol_photons.rs:807-809): out 3*w*h interleaved XYZ f32 (film / 2^scale,
+ * sensor-reduced for spectral films). */
+int sc_photon_film_read_accum(sc_photon_film* f, float* out);
+/* raw film: int64 in row-major [h][w][channels] (channels = 3 or bins). */
+int sc_photon_film_read_raw(sc_photon_film* f, int64_t* out);
+/* clear_film (vol_photons.rs:800-804): zero the 64-bit film (it is the accumulator). */
+int sc_photon_film_clear(sc_photon_film* f);
+/* auto_expose, auto_expose_p997, to_rgb8 (vol_photons.rs:823-850), on the device. */
+int sc_photon_film_auto_expose(sc_photon_film* f, float scale, float* exposure);
+int sc_photon_film_auto_expose_p997(sc_photon_film* f, float* exposure);
+int sc_photon_film_to_rgb8(sc_photon_film* f, float exposure, uint8_t* out_rgb);
+/* Viewer reconstruction (spectral-viewer/src/main.rs:132-173): normalized
+ * Gaussian gather of radius kradius over the accumulated film scaled by
+ * target_n / total_photons, plus the rim surface, XYZ->sRGB, Reinhard,
+ * gamma 1/2.2.  out: w*h RGBA8. */
+int sc_photon_film_gather_rgba8(sc_photon_film* f, uint64_t total_photons, float target_n,
+                                float kradius, float exposure, uint8_t* out_rgba);
+int sc_photon_film_dims(sc_photon_film* f, uint32_t* width, uint32_t* height, uint32_t* channels);
+/* Replace the scene records, camera and beam (host -> device upload on the
+ * film's stream); the film keeps accumulating.  Same limits as create. */
+int sc_photon_film_set_scene(sc_photon_film* f, const sc_primitive* prims, uint32_t n_prims,
+                             const sc_plane* planes, uint32_t n_planes, const sc_material* mats,
+                             uint32_t n_mats, const sc_camera* cam, const sc_beam* beam);
+/* Work counters of photons [photon_base, photon_base+count) without touching
+ * the film: out[0..3] = photons, path segments, in-frame haze samples (film
+ * splats), surface scatters. */
+int sc_photon_film_trace_stats(sc_photon_film* f, uint32_t photon_base, uint32_t count, uint32_t seed,
+                               uint64_t out[4]);
+
+/* ---- atomic film: AtomicFilm (spectral-gpu/src/film.rs:40-305) --------- */
+typedef struct sc_atomic_film sc_atomic_film;
+int sc_atomic_film_create(sc_ctx* ctx, uint32_t width, uint32_t height, sc_atomic_film** out);
+int sc_atomic_film_destroy(sc_atomic_film* f);
+/* splat (film.rs:174-192): vol_splat.wgsl semantics (u32, x4096, truncation). */
+int sc_atomic_film_splat(sc_atomic_film* f, uint32_t seed, uint32_t n_splats);
+/* read_film_raw (film.rs:197-214): out 3*w*h u32. */
+int sc_atomic_film_read_raw(sc_atomic_film* f, uint32_t* out);
+/* resolve (film.rs:218-224) + accum (film.rs:239-241). */
+int sc_atomic_film_resolve(sc_atomic_film* f);
+int sc_atomic_film_read_accum(sc_atomic_film* f, float* out);
+int sc_atomic_film_clear_film(sc_atomic_film* f);
+int sc_atomic_film_clear_accum(sc_atomic_film* f);
+/* check_determinism (film.rs:282-305): returns SC_OK and *first_diff=-1 when identical. */
+int sc_atomic_film_check_determinism(sc_ctx* ctx, uint32_t width, uint32_t height, uint32_t seed,
+                                     uint32_t n_splats, int64_t* first_diff);
+
+/* ---- device-pointer entry points (zero-copy; caller owns device memory) -- */
+/* One plain launch of the forward photon + haze kernel over photons
+ * [photon_base, photon_base+count) into a device film the caller allocated
+ * with sc_film_bytes().  All pointers are device pointers; stream may be 0. */
+typedef struct {
+    const sc_primitive* prims; uint32_t n_prims;
+    const sc_plane* planes; uint32_t n_planes;
+    const sc_material* mats; uint32_t n_mats;
+    sc_camera cam; sc_beam beam; sc_vol_weights weights;
+    uint32_t width, height, seed, spectral;
+    float max_dist;
+    sc_film_options opts;
+    const float* zbuffer;   /* device, or NULL */
+} sc_trace_desc;
+size_t sc_film_bytes(uint32_t width, uint32_t height, uint32_t channels);
+size_t sc_film_flag_bytes(uint32_t width, uint32_t height);
+int sc_trace_photons_device(sc_ctx* ctx, const sc_trace_desc* desc, uint32_t photon_base,
+                            uint32_t count, void* film_dev, uint32_t* flags_dev, void* stream);
+/* Work counters (see sc_photon_film_trace_stats) for a device-pointer desc;
+ * out_dev: 4 uint64 on the device, accumulated into (zero it first). */
+int sc_trace_stats_device(sc_ctx* ctx, const sc_trace_desc* desc, uint32_t photon_base, uint32_t count,
+                          uint64_t* out_dev, void* stream);
+/* Sensor reduction of a device film to interleaved f32 XYZ (3*w*h, device);
+ * drain != 0 also zeroes the film and its tile flags (ready for the next pass). */
+int sc_sensor_reduce_device(sc_ctx* ctx, uint32_t width, uint32_t height, uint32_t channels,
+                            float lambda_min, float lambda_max, uint32_t scale_log2,
+                            void* film_dev, uint32_t* flags_dev, float* xyz_dev, int drain,
+                            void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

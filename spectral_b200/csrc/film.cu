@@ -1,0 +1,354 @@
+// Film kernels: sensor reduction / drain, exposure, tonemap, Gaussian gather,
+// and the synthetic atomic-film splat.
+#include <cmath>
+
+#include "internal.h"
+
+namespace sc {
+
+namespace {
+
+constexpr int kReduceThreads = 256;
+
+// One film tile (64 pixels x C channels of int64) is staged into shared memory
+// with 16-byte coalesced loads, optionally zeroed behind the load (drain), then
+// reduced per pixel: XYZ film -> value / 2^scale; spectral film -> sum over bins
+// of count * bin-averaged CMF (f64 accumulation, fixed order per pixel).
+// Tiles whose dirty flag is clear are never read: their pixels are written as 0.
+__device__ __forceinline__ void reduce_tile(const ReduceParams& p, uint32_t tile, bool drain,
+                                            unsigned long long* sm, double* part) {
+    const uint32_t C = p.channels;
+    const uint32_t tx = tile % p.tiles_x, ty = tile / p.tiles_x;
+    const bool dirty = p.flags == nullptr || p.flags[tile] != 0u;
+    const uint32_t tid = threadIdx.x;
+    if (!dirty) {
+        for (uint32_t i = tid; i < kTilePixels * 3u; i += blockDim.x) {
+            const uint32_t l = i / 3u, c = i % 3u;
+            const uint32_t px = tx * 8u + (l & 7u), py = ty * 8u + (l >> 3);
+            if (px < p.width && py < p.height) p.xyz[((size_t)py * p.width + px) * 3u + c] = 0.0f;
+        }
+        return;
+    }
+    ulonglong2* src = reinterpret_cast<ulonglong2*>(p.film + (size_t)tile * kTilePixels * C);
+    ulonglong2* dst = reinterpret_cast<ulonglong2*>(sm);
+    const uint32_t n2 = kTilePixels * C / 2u;
+    for (uint32_t i = tid; i < n2; i += blockDim.x) {
+        dst[i] = __ldcs(src + i);
+        if (drain) __stcs(src + i, make_ulonglong2(0ull, 0ull));
+    }
+    __syncthreads();
+    if (C == 3u) {
+        for (uint32_t i = tid; i < kTilePixels * 3u; i += blockDim.x) {
+            const uint32_t l = i / 3u, c = i % 3u;
+            const uint32_t px = tx * 8u + (l & 7u), py = ty * 8u + (l >> 3);
+            if (px < p.width && py < p.height)
+                p.xyz[((size_t)py * p.width + px) * 3u + c] = (float)((double)(long long)sm[i] * p.inv_scale);
+        }
+    } else {
+        // 4 threads per pixel, each a contiguous quarter of the bins; partials
+        // are summed in quarter order so the result does not depend on timing.
+        const uint32_t l = tid & 63u, q = tid >> 6;
+        if (q < 4u) {
+            const uint32_t b0 = q * C / 4u, b1 = (q + 1u) * C / 4u, span = b1 - b0;
+            double x = 0.0, y = 0.0, z = 0.0;
+            const unsigned long long* row = sm + (size_t)l * C;
+            for (uint32_t j = 0; j < span; ++j) {
+                const uint32_t b = b0 + (j + l) % span;  // rotate to spread banks
+                const double v = (double)(long long)row[b];
+                x += v * (double)p.binw[b];
+                y += v * (double)p.binw[C + b];
+                z += v * (double)p.binw[2u * C + b];
+            }
+            part[(q * 64u + l) * 3u] = x; part[(q * 64u + l) * 3u + 1u] = y; part[(q * 64u + l) * 3u + 2u] = z;
+        }
+        __syncthreads();
+        if (tid < 64u) {
+            const uint32_t px = tx * 8u + (tid & 7u), py = ty * 8u + (tid >> 3);
+            if (px < p.width && py < p.height) {
+                float* o = p.xyz + ((size_t)py * p.width + px) * 3u;
+                for (uint32_t c = 0; c < 3u; ++c) {
+                    const double s = ((part[tid * 3u + c] + part[(64u + tid) * 3u + c]) + part[(128u + tid) * 3u + c]) +
+                                     part[(192u + tid) * 3u + c];
+                    o[c] = (float)(s * p.inv_scale);
+                }
+            }
+        }
+    }
+    if (drain && p.flags && tid == 0) p.flags[tile] = 0u;
+    __syncthreads();
+}
+
+template <bool DRAIN>
+__global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const ReduceParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* part = reinterpret_cast<double*>(smem);
+    unsigned long long* sm = reinterpret_cast<unsigned long long*>(smem + 4 * 64 * 3 * sizeof(double));
+    const uint32_t ntiles = p.tiles_x * p.tiles_y;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) reduce_tile(p, tile, DRAIN, sm, part);
+}
+
+// Many films in one persistent launch: global tile index -> (film, tile) by a
+// binary search over the films' tile prefix.
+template <bool DRAIN>
+__global__ void __launch_bounds__(kReduceThreads) reduce_many_kernel(const FilmDesc* __restrict__ descs, uint32_t n_films,
+                                                                     uint32_t total_tiles) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* part = reinterpret_cast<double*>(smem);
+    unsigned long long* sm = reinterpret_cast<unsigned long long*>(smem + 4 * 64 * 3 * sizeof(double));
+    for (uint32_t g = blockIdx.x; g < total_tiles; g += gridDim.x) {
+        uint32_t lo = 0, hi = n_films;
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (descs[mid].tile_begin <= g) lo = mid; else hi = mid;
+        }
+        const FilmDesc& d = descs[lo];
+        ReduceParams p;
+        p.film = d.film; p.flags = d.flags; p.xyz = d.xyz; p.width = d.width; p.height = d.height;
+        p.tiles_x = d.tiles_x; p.tiles_y = d.tiles_y; p.channels = d.channels; p.binw = d.binw;
+        p.inv_scale = d.inv_scale;
+        reduce_tile(p, g - d.tile_begin, DRAIN, sm, part);
+    }
+}
+
+__global__ void composite_max_y_kernel(const float* __restrict__ xyz, const float* __restrict__ surface,
+                                       uint32_t n, uint32_t* out_bits) {
+    float m = 0.0f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float y = xyz[3u * i + 1u] + (surface ? surface[3u * i + 1u] : 0.0f);
+        m = fmaxf(m, y);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(out_bits, __float_as_uint(m));
+}
+
+// Radix select of the k-th smallest composited luminance (values >= 0, so the
+// IEEE bit patterns order like the floats).  work: [0..255] histogram,
+// [256] prefix, [257] k remaining, [258] result bits.
+__global__ void select_hist_kernel(const float* __restrict__ xyz, const float* __restrict__ surface, uint32_t n,
+                                   uint32_t* work, int shift) {
+    __shared__ uint32_t hist[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0u;
+    __syncthreads();
+    const uint32_t prefix = work[256];
+    const uint32_t hi_mask = shift >= 24 ? 0u : (0xFFFFFFFFu << (shift + 8));
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float y = xyz[3u * i + 1u] + (surface ? surface[3u * i + 1u] : 0.0f);
+        y = fmaxf(y, 0.0f);
+        const uint32_t bits = __float_as_uint(y);
+        if ((bits & hi_mask) == (prefix & hi_mask)) atomicAdd(&hist[(bits >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (hist[i]) atomicAdd(&work[i], hist[i]);
+}
+__global__ void select_pick_kernel(uint32_t* work, int shift) {
+    if (threadIdx.x != 0) return;
+    uint32_t k = work[257], acc = 0;
+    uint32_t b = 0;
+    for (; b < 255u; ++b) {
+        if (acc + work[b] > k) break;
+        acc += work[b];
+    }
+    work[256] |= b << shift;
+    work[257] = k - acc;
+    for (int i = 0; i < 256; ++i) work[i] = 0u;
+    if (shift == 0) work[258] = work[256];
+}
+
+__global__ void to_rgb8_kernel(const float* __restrict__ xyz, const float* __restrict__ surface, uint32_t n,
+                               float exposure, uint8_t* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float c[3];
+    for (int k = 0; k < 3; ++k) c[k] = xyz[3u * i + k] + (surface ? surface[3u * i + k] : 0.0f);
+    // xyz_to_linear_srgb + tonemap_to_u8 (spectral-core/src/cie.rs:121-144)
+    const float lin[3] = {3.2406f * c[0] - 1.5372f * c[1] - 0.4986f * c[2],
+                          -0.9689f * c[0] + 1.8758f * c[1] + 0.0415f * c[2],
+                          0.0557f * c[0] - 0.2040f * c[1] + 1.0570f * c[2]};
+    for (int k = 0; k < 3; ++k) {
+        const float v = fmaxf(lin[k] * exposure, 0.0f);
+        const float mapped = v / (1.0f + v);
+        float gm = mapped <= 0.0031308f ? 12.92f * mapped : 1.055f * powf(mapped, 1.0f / 2.4f) - 0.055f;
+        gm = fminf(fmaxf(gm, 0.0f), 1.0f);
+        const float q = gm * 255.0f + 0.5f;
+        out[3u * i + k] = (uint8_t)(q >= 255.0f ? 255.0f : q);
+    }
+}
+
+// Viewer reconstruction (spectral-viewer/src/main.rs:132-173): normalized
+// Gaussian gather, radius kradius, sigma max(kradius/2, 0.5), scaled by k, plus
+// the rim surface, XYZ -> linear sRGB, Reinhard, gamma 1/2.2, RGBA8.
+__global__ void gather_kernel(const float* __restrict__ xyz, const float* __restrict__ surface, uint32_t w,
+                              uint32_t h, float k, float kradius, float exposure, uint8_t* out) {
+    const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+    if (px >= w || py >= h) return;
+    const int radius = (int)kradius;
+    const float sigma = fmaxf(kradius * 0.5f, 0.5f);
+    const float inv2s2 = 1.0f / (2.0f * sigma * sigma);
+    float acc[3] = {0.f, 0.f, 0.f}, wsum = 0.0f;
+    for (int dy = -radius; dy <= radius; ++dy)
+        for (int dx = -radius; dx <= radius; ++dx) {
+            const int sx = (int)px + dx, sy = (int)py + dy;
+            if (sx >= 0 && sx < (int)w && sy >= 0 && sy < (int)h) {
+                const size_t si = (size_t)sy * w + sx;
+                const float g = expf(-(float)(dx * dx + dy * dy) * inv2s2);
+                for (int c = 0; c < 3; ++c) acc[c] = acc[c] + xyz[3 * si + c] * g;
+                wsum = wsum + g;
+            }
+        }
+    const size_t i = (size_t)py * w + px;
+    const float kk = k / fmaxf(wsum, 1e-6f);
+    float comp[3];
+    for (int c = 0; c < 3; ++c) comp[c] = (acc[c] * kk + (surface ? surface[3 * i + c] : 0.0f)) * exposure;
+    const float lin[3] = {3.2406f * comp[0] - 1.5372f * comp[1] - 0.4986f * comp[2],
+                          -0.9689f * comp[0] + 1.8758f * comp[1] + 0.0415f * comp[2],
+                          0.0557f * comp[0] - 0.2040f * comp[1] + 1.0570f * comp[2]};
+    const float inv_gamma = (float)(1.0 / 2.2);
+    for (int c = 0; c < 3; ++c) {
+        const float tt = lin[c] / (1.0f + lin[c]);
+        float v = powf(fmaxf(tt, 0.0f), inv_gamma);
+        v = fminf(fmaxf(v, 0.0f), 1.0f);
+        out[4 * i + c] = (uint8_t)(v * 255.0f + 0.5f);
+    }
+    out[4 * i + 3] = 255;
+}
+
+// Synthetic splat (spectral-gpu/src/shaders/vol_splat.wgsl:34-55): one thread
+// per splat, a hashed pixel, XYZ in [0,2), x4096 truncated, three u32 atomics.
+__global__ void synthetic_splat_kernel(uint32_t* film, uint32_t w, uint32_t h, uint32_t seed, uint32_t n) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    Rng r = Rng::make(t, seed);
+    const uint32_t idx = r.u32() % (w * h);
+    const float x = r.f32() * 2.0f, y = r.f32() * 2.0f, z = r.f32() * 2.0f;
+    atomicAdd(film + 3u * idx, (uint32_t)(fmaxf(x, 0.0f) * 4096.0f));
+    atomicAdd(film + 3u * idx + 1u, (uint32_t)(fmaxf(y, 0.0f) * 4096.0f));
+    atomicAdd(film + 3u * idx + 2u, (uint32_t)(fmaxf(z, 0.0f) * 4096.0f));
+}
+// AtomicFilm::resolve (spectral-gpu/src/film.rs:218-224), on the device.
+__global__ void atomic_resolve_kernel(uint32_t* film, float* accum, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t v = film[i];
+        film[i] = 0u;
+        accum[i] += (float)v / 4096.0f;
+    }
+}
+
+size_t reduce_smem(uint32_t channels) {
+    return 4 * 64 * 3 * sizeof(double) + (size_t)kTilePixels * channels * sizeof(unsigned long long);
+}
+
+}  // namespace
+
+cudaError_t launch_reduce(const ReduceParams& p, bool drain, cudaStream_t s) {
+    const size_t smem = reduce_smem(p.channels);
+    const uint32_t ntiles = p.tiles_x * p.tiles_y;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void* fn = drain ? reinterpret_cast<const void*>(&reduce_kernel<true>)
+                           : reinterpret_cast<const void*>(&reduce_kernel<false>);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kReduceThreads, smem);
+    uint32_t grid = (uint32_t)sms * (uint32_t)(per_sm > 0 ? per_sm : 1);
+    if (grid > ntiles) grid = ntiles;
+    if (grid == 0) return cudaSuccess;
+    if (drain) reduce_kernel<true><<<grid, kReduceThreads, smem, s>>>(p);
+    else reduce_kernel<false><<<grid, kReduceThreads, smem, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_many(const FilmDesc* descs, uint32_t n_films, uint32_t total_tiles, bool drain,
+                               uint32_t max_channels, cudaStream_t s) {
+    if (total_tiles == 0) return cudaSuccess;
+    const size_t smem = reduce_smem(max_channels);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void* fn = drain ? reinterpret_cast<const void*>(&reduce_many_kernel<true>)
+                           : reinterpret_cast<const void*>(&reduce_many_kernel<false>);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kReduceThreads, smem);
+    uint32_t grid = (uint32_t)sms * (uint32_t)(per_sm > 0 ? per_sm : 1);
+    if (grid > total_tiles) grid = total_tiles;
+    if (drain) reduce_many_kernel<true><<<grid, kReduceThreads, smem, s>>>(descs, n_films, total_tiles);
+    else reduce_many_kernel<false><<<grid, kReduceThreads, smem, s>>>(descs, n_films, total_tiles);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_composite_max_y(const float* xyz, const float* surface, uint32_t n, uint32_t* out_bits,
+                                   cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out_bits, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    uint32_t grid = (n + 255) / 256;
+    if (grid > 1184) grid = 1184;
+    if (grid == 0) grid = 1;
+    composite_max_y_kernel<<<grid, 256, 0, s>>>(xyz, surface, n, out_bits);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_composite_select(const float* xyz, const float* surface, uint32_t n, uint32_t k, uint32_t* work,
+                                    cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(work, 0, 259 * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(work + 257, &k, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    uint32_t grid = (n + 255) / 256;
+    if (grid > 1184) grid = 1184;
+    if (grid == 0) grid = 1;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        select_hist_kernel<<<grid, 256, 0, s>>>(xyz, surface, n, work, shift);
+        select_pick_kernel<<<1, 32, 0, s>>>(work, shift);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_rgb8(const float* xyz, const float* surface, uint32_t n, float exposure, uint8_t* out,
+                           cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    to_rgb8_kernel<<<(n + 255) / 256, 256, 0, s>>>(xyz, surface, n, exposure, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rgba8(const float* xyz, const float* surface, uint32_t w, uint32_t h, float k,
+                                float kradius, float exposure, uint8_t* out, cudaStream_t s) {
+    dim3 block(16, 16), grid((w + 15) / 16, (h + 15) / 16);
+    gather_kernel<<<grid, block, 0, s>>>(xyz, surface, w, h, k, kradius, exposure, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_synthetic_splat(uint32_t* film, uint32_t w, uint32_t h, uint32_t seed, uint32_t n,
+                                   cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    synthetic_splat_kernel<<<(n + 255) / 256, 256, 0, s>>>(film, w, h, seed, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_atomic_resolve(uint32_t* film, float* accum, size_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    size_t grid = (n + 255) / 256;
+    if (grid > 4096) grid = 4096;
+    atomic_resolve_kernel<<<(unsigned)grid, 256, 0, s>>>(film, accum, n);
+    return cudaGetLastError();
+}
+
+// Bin-averaged colour matching: for bin b of [lambda_min, lambda_max), the mean
+// of the clamped table lerp over 16 sub-bin midpoints (what a photon drawn
+// uniformly inside the bin would deposit on average).
+void bin_weights(const float* tables, uint32_t bins, float lambda_min, float lambda_max, float* out) {
+    const double width = ((double)lambda_max - (double)lambda_min) / (double)bins;
+    for (uint32_t b = 0; b < bins; ++b) {
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int j = 0; j < 16; ++j) {
+            const float nm = (float)((double)lambda_min + width * ((double)b + ((double)j + 0.5) / 16.0));
+            for (int c = 0; c < 3; ++c) acc[c] += (double)tab_sample(tables + c * kTableN, nm);
+        }
+        for (int c = 0; c < 3; ++c) out[c * bins + b] = (float)(acc[c] / 16.0);
+    }
+}
+
+Proj make_proj(const sc_camera& c) { return proj_make(c); }
+
+}  // namespace sc

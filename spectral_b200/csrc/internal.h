@@ -1,0 +1,85 @@
+// Internal interface between the host runtime (capi.cu, batch.cu, server.cu)
+// and the kernel files.  Not part of the public ABI.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+
+namespace sc {
+
+// One forward photon pass over photons [photon_base, photon_base + photon_count).
+struct PhotonParams {
+    f3 corner, bu, bv, bdir;          // Beam (lighttrace.rs:116-121)
+    Proj proj;                        // Camera::project basis
+    uint32_t width, height, tiles_x, channels;
+    uint32_t photon_base, photon_count, seed, max_bounces;
+    float sigma_s, sigma_t, g, max_dist;
+    float lambda_min, lambda_range, bin_min, bin_inv_width;
+    float scale;
+    uint32_t spectral, estimator, bins;
+    const float* zbuf;                // device, nullable
+    unsigned long long* film;         // tile-major int64 film
+    uint32_t* flags;                  // per-tile dirty flags, nullable
+    const sc_primitive* prims; const sc_plane* planes; const sc_material* mats;
+    uint32_t n_prims, n_planes, n_mats;
+    const float* cmf;                 // device 3x71 (xbar, ybar, zbar)
+    sc_debug_photon* debug;           // debug launches only
+};
+
+struct LaunchShape { uint32_t block, grid; int aggregate; };
+
+size_t scene_smem_bytes(uint32_t n_prims, uint32_t n_planes, uint32_t n_mats);
+cudaError_t launch_photons(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s);
+cudaError_t launch_photon_debug(const PhotonParams& p, cudaStream_t s);
+cudaError_t launch_photon_count(const PhotonParams& p, unsigned long long* out, uint32_t grid, cudaStream_t s);
+int photon_occupancy_blocks(uint32_t block, bool spectral, int aggregate, size_t smem);
+
+struct RimParams {
+    sc_camera cam;
+    uint32_t width, height;
+    const sc_primitive* prims; const sc_plane* planes; const sc_material* mats;
+    uint32_t n_prims, n_planes, n_mats;
+    float* out;                       // 3*w*h
+};
+cudaError_t launch_rim(const RimParams& p, cudaStream_t s);
+cudaError_t launch_rng_draws(uint32_t key, uint32_t seed, uint32_t n, uint32_t* out, cudaStream_t s);
+
+// Film reduction: tile-major int64 film -> interleaved f32 XYZ (3*w*h).
+struct ReduceParams {
+    unsigned long long* film;
+    uint32_t* flags;                  // nullable: every tile is read
+    float* xyz;
+    uint32_t width, height, tiles_x, tiles_y, channels;
+    const float* binw;                // 3*channels bin-averaged CMF (spectral films)
+    double inv_scale;
+};
+cudaError_t launch_reduce(const ReduceParams& p, bool drain, cudaStream_t s);
+
+// Batched reduction over many films described in device memory.
+struct FilmDesc {
+    unsigned long long* film; uint32_t* flags; float* xyz; const float* binw;
+    uint32_t width, height, tiles_x, tiles_y, channels, tile_begin;  // tile_begin: prefix over films
+    double inv_scale;
+};
+cudaError_t launch_reduce_many(const FilmDesc* descs, uint32_t n_films, uint32_t total_tiles,
+                               bool drain, uint32_t max_channels, cudaStream_t s);
+
+cudaError_t launch_composite_max_y(const float* xyz, const float* surface, uint32_t n_pixels,
+                                   uint32_t* out_bits, cudaStream_t s);
+cudaError_t launch_composite_select(const float* xyz, const float* surface, uint32_t n_pixels,
+                                    uint32_t k, uint32_t* work /*260 u32*/, cudaStream_t s);
+cudaError_t launch_to_rgb8(const float* xyz, const float* surface, uint32_t n_pixels, float exposure,
+                           uint8_t* out, cudaStream_t s);
+cudaError_t launch_gather_rgba8(const float* xyz, const float* surface, uint32_t w, uint32_t h,
+                                float k, float kradius, float exposure, uint8_t* out, cudaStream_t s);
+cudaError_t launch_synthetic_splat(uint32_t* film, uint32_t w, uint32_t h, uint32_t seed, uint32_t n,
+                                   cudaStream_t s);
+cudaError_t launch_atomic_resolve(uint32_t* film, float* accum, size_t n, cudaStream_t s);
+
+// Host helpers shared by the runtime objects.
+void bin_weights(const float* tables_5x71, uint32_t bins, float lambda_min, float lambda_max, float* out_3xbins);
+Proj make_proj(const sc_camera& c);
+
+}  // namespace sc

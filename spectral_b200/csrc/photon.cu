@@ -1,0 +1,337 @@
+// Forward photon emitter / tracer with point-estimator haze splatting.
+//
+// One thread per photon, restating render_volumetric_scene_point
+// (spectral-core/src/volume.rs:99-168) and its GPU mirror
+// (spectral-gpu/src/shaders/volume.wgsl:542-647): emission from the beam
+// aperture, hero wavelength, up to max_bounces segments, 4 uniform haze samples
+// per segment connected to the camera (HG phase x transmittance / d^2), then the
+// Fresnel / refract / TIR scatter at the hit.  The RNG stream is consumed in
+// exactly the reference order, so paths are bit-identical to the CPU crate.
+//
+// Splats land in a 64-bit fixed-point film with red.global.add.u64; the film is
+// tile-major (8x8 pixel tiles) and every touched tile raises a dirty flag so the
+// drain/reduce pass reads only tiles that received light.
+#include "internal.h"
+
+namespace sc {
+
+namespace {
+
+constexpr float kInv4Pi = 1.0f / (4.0f * 3.14159265358979323846f);
+
+__device__ __forceinline__ void red_u64(unsigned long long* a, unsigned long long v) {
+    if (v) atomicAdd(a, v);
+}
+
+// Exact segmented sum of 64-bit values over the lanes of `peers` using three
+// 26-bit chunks (no chunk sum can overflow 32 bits for <= 32 lanes).
+__device__ __forceinline__ unsigned long long peer_sum64(unsigned peers, unsigned long long v) {
+    unsigned c0 = (unsigned)(v & 0x3FFFFFFull);
+    unsigned c1 = (unsigned)((v >> 26) & 0x3FFFFFFull);
+    unsigned c2 = (unsigned)(v >> 52);
+    unsigned s0 = __reduce_add_sync(peers, c0);
+    unsigned s1 = __reduce_add_sync(peers, c1);
+    unsigned s2 = __reduce_add_sync(peers, c2);
+    return (unsigned long long)s0 + ((unsigned long long)s1 << 26) + ((unsigned long long)s2 << 52);
+}
+
+__device__ __forceinline__ void mark_tile(uint32_t* flags, uint32_t tile) {
+    if (flags) {
+        volatile uint32_t* f = flags + tile;
+        if (*f == 0u) *f = 1u;
+    }
+}
+
+// Deposit one haze sample.  AGG=1 merges lanes of the warp that hit the same
+// film cell before issuing the atomic.
+template <bool SPEC, int AGG>
+__device__ __forceinline__ void deposit(const PhotonParams& p, bool ok, uint32_t px, uint32_t py,
+                                        float contrib, float cx, float cy, float cz, uint32_t bin) {
+    size_t cell = 0;
+    uint32_t tile = 0;
+    unsigned long long v0 = 0, v1 = 0, v2 = 0;
+    if (ok) {
+        tile = film_tile(px, py, p.tiles_x);
+        cell = film_cell(px, py, p.tiles_x, p.channels) + (SPEC ? bin : 0u);
+        if (SPEC) {
+            v0 = to_fixed(contrib, p.scale);
+        } else {
+            v0 = to_fixed(cx * contrib, p.scale);
+            v1 = to_fixed(cy * contrib, p.scale);
+            v2 = to_fixed(cz * contrib, p.scale);
+        }
+    }
+    if (AGG == 0) {
+        if (!ok) return;
+        mark_tile(p.flags, tile);
+        red_u64(p.film + cell, v0);
+        if (!SPEC) { red_u64(p.film + cell + 1, v1); red_u64(p.film + cell + 2, v2); }
+        return;
+    }
+    const unsigned mask = __activemask();
+    const uint32_t key = ok ? (uint32_t)cell : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(mask, key);
+    if (!ok) return;
+    const unsigned lane = threadIdx.x & 31u;
+    if (peers != (1u << lane)) {
+        v0 = peer_sum64(peers, v0);
+        if (!SPEC) { v1 = peer_sum64(peers, v1); v2 = peer_sum64(peers, v2); }
+        if ((int)lane != __ffs(peers) - 1) return;
+    }
+    mark_tile(p.flags, tile);
+    red_u64(p.film + cell, v0);
+    if (!SPEC) { red_u64(p.film + cell + 1, v1); red_u64(p.film + cell + 2, v2); }
+}
+
+__device__ __forceinline__ void record_pair(sc_debug_photon* rec, uint32_t pair, f3 o, f3 d) {
+    if (pair >= 9u) return;
+    float* q = rec->states[2 * pair];
+    q[0] = o.x; q[1] = o.y; q[2] = o.z; q[3] = 0.0f;
+    q = rec->states[2 * pair + 1];
+    q[0] = d.x; q[1] = d.y; q[2] = d.z; q[3] = 0.0f;
+}
+
+// Work counters of one photon (instrumented launches only): segments traced,
+// haze samples that land in frame (= film splats), dielectric/diffuse scatters.
+struct PhotonCounts { uint32_t segments, splats, scatters; };
+
+template <bool SPEC, int AGG, bool DEBUG, bool COUNT = false>
+__device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneView& S, const float* cmf,
+                                             uint32_t idx, PhotonCounts* cnt = nullptr) {
+    Rng r = Rng::make(idx, p.seed);
+    const float r1 = r.f32();
+    const float r2 = r.f32();
+    f3 o = add(add(p.corner, mul(p.bu, r1)), mul(p.bv, r2));
+    const float lambda = p.lambda_min + p.lambda_range * r.f32();
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    uint32_t bin = 0;
+    if (!DEBUG) {
+        if (SPEC) {
+            float fb = (lambda - p.bin_min) * p.bin_inv_width;
+            int bi = (int)fb;
+            bin = fb < 0.0f ? 0u : (bi >= (int)p.bins ? p.bins - 1u : (uint32_t)bi);
+        } else {
+            cx = tab_sample(cmf, lambda);
+            cy = tab_sample(cmf + kTableN, lambda);
+            cz = tab_sample(cmf + 2 * kTableN, lambda);
+        }
+    }
+    f3 d = p.bdir;
+    float power = 1.0f;
+    sc_debug_photon* rec = nullptr;
+    uint32_t pairs = 1;
+    if (DEBUG) {
+        rec = p.debug + idx;
+        rec->lambda = lambda;
+        rec->pad0 = rec->pad1 = 0u;
+        record_pair(rec, 0, o, d);
+    }
+    for (uint32_t b = 0; b < p.max_bounces; ++b) {
+        Hit h;
+        uint32_t mi = 0;
+        const bool any = scene_hit(S, o, d, h, mi);
+        const float seg = any ? h.t : p.max_dist;
+        if (COUNT) ++cnt->segments;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float dist = r.f32() * seg;
+            if (DEBUG) continue;
+            const f3 q = add(o, mul(d, dist));
+            float s, t;
+            bool ok = project(p.proj, q, s, t);
+            uint32_t px = 0, py = 0;
+            float contrib = 0.0f;
+            if (ok) {
+                px = min((uint32_t)(s * (float)p.width), p.width - 1u);
+                py = min((uint32_t)((1.0f - t) * (float)p.height), p.height - 1u);
+                if (p.estimator == 0u) {
+                    const f3 to = sub(p.proj.o, q);
+                    const float dd = fmaxf(length(to), 1e-3f);
+                    if (p.zbuf && !(dd < p.zbuf[py * p.width + px])) {
+                        ok = false;
+                    } else {
+                        const float ct = dot(d, vdiv(to, dd));
+                        const float phase = phase_hg(p.g, ct);
+                        const float trans = expf(-p.sigma_t * dd);
+                        contrib = power * p.sigma_s * phase * trans / (dd * dd) * seg / 4.0f;
+                    }
+                } else {
+                    contrib = power * p.sigma_s * seg / 4.0f * kInv4Pi;
+                }
+            }
+            if (COUNT) { if (ok) ++cnt->splats; continue; }
+            deposit<SPEC, AGG>(p, ok, px, py, contrib, cx, cy, cz, bin);
+        }
+        if (!any) break;
+        const sc_material& m = S.mats[mi];
+        const float nh = m.kind == 1u ? glass_n(m.glass, p.spectral ? lambda : 550.0f) : 1.0f;
+        f3 nd;
+        float w;
+        if (COUNT) ++cnt->scatters;
+        scatter(m, d, h, nh, r, nd, w);
+        power *= w;
+        o = h.point;
+        d = nd;
+        if (DEBUG) { record_pair(rec, pairs, o, d); ++pairs; }
+    }
+    if (DEBUG) rec->num_states = pairs < 9u ? pairs : 9u;
+}
+
+// Stage the scene records and the CMF table in shared memory.
+__device__ __forceinline__ SceneView load_scene(const PhotonParams& p, unsigned char* smem, const float** cmf_out) {
+    sc_primitive* sp = reinterpret_cast<sc_primitive*>(smem);
+    sc_plane* spl = reinterpret_cast<sc_plane*>(sp + p.n_prims);
+    sc_material* sm = reinterpret_cast<sc_material*>(spl + p.n_planes);
+    float* scmf = reinterpret_cast<float*>(sm + p.n_mats);
+    for (uint32_t i = threadIdx.x; i < p.n_prims; i += blockDim.x) sp[i] = p.prims[i];
+    for (uint32_t i = threadIdx.x; i < p.n_planes; i += blockDim.x) spl[i] = p.planes[i];
+    for (uint32_t i = threadIdx.x; i < p.n_mats; i += blockDim.x) sm[i] = p.mats[i];
+    for (uint32_t i = threadIdx.x; i < 3u * kTableN; i += blockDim.x) scmf[i] = p.cmf[i];
+    __syncthreads();
+    *cmf_out = scmf;
+    SceneView S;
+    S.prims = sp; S.planes = spl; S.mats = sm; S.n_prims = p.n_prims;
+    return S;
+}
+
+template <bool SPEC, int AGG>
+__global__ void __launch_bounds__(512) photon_kernel(const PhotonParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const float* cmf;
+    const SceneView S = load_scene(p, smem, &cmf);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += stride)
+        trace_photon<SPEC, AGG, false>(p, S, cmf, p.photon_base + i);
+}
+
+// Instrumented pass: same transport, no film writes; sums the per-photon work
+// counters into out[0..3] = photons, segments, in-frame samples, scatters.
+__global__ void __launch_bounds__(256) photon_count_kernel(const PhotonParams p, unsigned long long* out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const float* cmf;
+    const SceneView S = load_scene(p, smem, &cmf);
+    unsigned long long seg = 0, spl = 0, sca = 0, ph = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += gridDim.x * blockDim.x) {
+        PhotonCounts c = {0u, 0u, 0u};
+        trace_photon<false, 0, false, true>(p, S, cmf, p.photon_base + i, &c);
+        seg += c.segments; spl += c.splats; sca += c.scatters; ++ph;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        seg += __shfl_xor_sync(0xffffffffu, seg, o);
+        spl += __shfl_xor_sync(0xffffffffu, spl, o);
+        sca += __shfl_xor_sync(0xffffffffu, sca, o);
+        ph += __shfl_xor_sync(0xffffffffu, ph, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, ph); atomicAdd(out + 1, seg); atomicAdd(out + 2, spl); atomicAdd(out + 3, sca);
+    }
+}
+
+__global__ void __launch_bounds__(256) photon_debug_kernel(const PhotonParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const float* cmf;
+    const SceneView S = load_scene(p, smem, &cmf);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < p.photon_count) trace_photon<false, 0, true>(p, S, cmf, i);
+}
+
+// Surface rim pass (spectral-gpu/src/shaders/volume.wgsl:668-703 and its CPU
+// oracle cpu_surface_rim, spectral-gpu/src/vol_photons.rs:1517-1538): one camera
+// primary ray per pixel, nearest hit, rim = (1 - |n.d|)^2, tinted constant XYZ.
+__global__ void __launch_bounds__(256) rim_kernel(const RimParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    sc_primitive* sp = reinterpret_cast<sc_primitive*>(smem);
+    sc_plane* spl = reinterpret_cast<sc_plane*>(sp + p.n_prims);
+    sc_material* sm = reinterpret_cast<sc_material*>(spl + p.n_planes);
+    const uint32_t tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    for (uint32_t i = tid; i < p.n_prims; i += nt) sp[i] = p.prims[i];
+    for (uint32_t i = tid; i < p.n_planes; i += nt) spl[i] = p.planes[i];
+    for (uint32_t i = tid; i < p.n_mats; i += nt) sm[i] = p.mats[i];
+    __syncthreads();
+    const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+    if (px >= p.width || py >= p.height) return;
+    SceneView S;
+    S.prims = sp; S.planes = spl; S.mats = sm; S.n_prims = p.n_prims;
+    const float s = ((float)px + 0.5f) / (float)p.width;
+    const float t = 1.0f - ((float)py + 0.5f) / (float)p.height;
+    const f3 o = ld3(p.cam.origin), d = primary_dir(p.cam, s, t);
+    Hit h;
+    uint32_t mi;
+    const size_t i = (size_t)py * p.width + px;
+    float x = 0.f, y = 0.f, z = 0.f;
+    if (scene_hit(S, o, d, h, mi)) {
+        const float c = fminf(fmaxf(fabsf(dot(h.normal, d)), 0.0f), 1.0f);
+        const float rim = (1.0f - c) * (1.0f - c);
+        x = 0.015f + rim * 0.45f; y = 0.02f + rim * 0.5f; z = 0.04f + rim * 0.6f;
+    }
+    p.out[3 * i] = x; p.out[3 * i + 1] = y; p.out[3 * i + 2] = z;
+}
+
+__global__ void rng_draws_kernel(uint32_t key, uint32_t seed, uint32_t n, uint32_t* out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    Rng r = Rng::make(key, seed);
+    for (uint32_t i = 0; i < n; ++i) out[i] = r.u32();
+}
+
+}  // namespace
+
+cudaError_t launch_rng_draws(uint32_t key, uint32_t seed, uint32_t n, uint32_t* out, cudaStream_t s) {
+    rng_draws_kernel<<<1, 32, 0, s>>>(key, seed, n, out);
+    return cudaGetLastError();
+}
+
+size_t scene_smem_bytes(uint32_t n_prims, uint32_t n_planes, uint32_t n_mats) {
+    return n_prims * sizeof(sc_primitive) + n_planes * sizeof(sc_plane) + n_mats * sizeof(sc_material) +
+           3 * kTableN * sizeof(float);
+}
+
+template <bool SPEC, int AGG>
+static const void* photon_fn() { return reinterpret_cast<const void*>(&photon_kernel<SPEC, AGG>); }
+
+int photon_occupancy_blocks(uint32_t block, bool spectral, int aggregate, size_t smem) {
+    const void* fn = spectral ? (aggregate ? photon_fn<true, 1>() : photon_fn<true, 0>())
+                              : (aggregate ? photon_fn<false, 1>() : photon_fn<false, 0>());
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)block, smem) != cudaSuccess) return 1;
+    return n > 0 ? n : 1;
+}
+
+cudaError_t launch_photons(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s) {
+    if (p.photon_count == 0) return cudaSuccess;
+    const size_t smem = scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats);
+    const bool spec = p.channels != 3u || p.bins != 0u;
+    const uint32_t need = (p.photon_count + shape.block - 1) / shape.block;
+    const uint32_t grid = need < shape.grid ? need : shape.grid;
+    if (spec) {
+        if (shape.aggregate) photon_kernel<true, 1><<<grid, shape.block, smem, s>>>(p);
+        else photon_kernel<true, 0><<<grid, shape.block, smem, s>>>(p);
+    } else {
+        if (shape.aggregate) photon_kernel<false, 1><<<grid, shape.block, smem, s>>>(p);
+        else photon_kernel<false, 0><<<grid, shape.block, smem, s>>>(p);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_photon_debug(const PhotonParams& p, cudaStream_t s) {
+    if (p.photon_count == 0) return cudaSuccess;
+    const size_t smem = scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats);
+    photon_debug_kernel<<<(p.photon_count + 255) / 256, 256, smem, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_photon_count(const PhotonParams& p, unsigned long long* out, uint32_t grid, cudaStream_t s) {
+    if (p.photon_count == 0) return cudaSuccess;
+    const size_t smem = scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats);
+    const uint32_t need = (p.photon_count + 255) / 256;
+    photon_count_kernel<<<need < grid ? need : grid, 256, smem, s>>>(p, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rim(const RimParams& p, cudaStream_t s) {
+    const size_t smem = p.n_prims * sizeof(sc_primitive) + p.n_planes * sizeof(sc_plane) + p.n_mats * sizeof(sc_material);
+    dim3 block(16, 16), grid((p.width + 15) / 16, (p.height + 15) / 16);
+    rim_kernel<<<grid, block, smem, s>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace sc

@@ -1,0 +1,62 @@
+"""Shared test helpers: hand one scene to both the CUDA library and the oracle,
+and the film metrics the reference's gates use."""
+import ctypes as C
+
+import numpy as np
+
+import oracle
+import spectral_b200 as sb
+
+
+def oscene(scene):
+    """Oracle copy of a product Scene (same flat record bytes)."""
+    prims, np_, planes, npl, mats, nm = scene.arrays()
+    return oracle.OScene(bytes(prims), np_, bytes(planes), npl, bytes(mats), nm, scene.background, scene.horizon)
+
+
+def obeam(beam):
+    return oracle.or_beam.from_buffer_copy(bytes(beam.c))
+
+
+def ocam(cam):
+    return oracle.or_camera.from_buffer_copy(bytes(cam.c))
+
+
+def rel_l1(gpu, cpu):
+    gpu = np.asarray(gpu, np.float64)
+    cpu = np.asarray(cpu, np.float64)
+    den = np.abs(cpu).sum()
+    return float(np.abs(gpu - cpu).sum() / den) if den > 0 else 0.0
+
+
+def energy_delta(gpu_xyz, cpu_xyz):
+    gy = float(np.asarray(gpu_xyz, np.float64)[1::3].sum())
+    cy = float(np.asarray(cpu_xyz, np.float64)[1::3].sum())
+    return abs(gy - cy) / cy if cy > 0 else 0.0
+
+
+def axis_box(lo, hi):
+    """ConvexSolid::axis_box (spectral-core/src/geom.rs:73-84)."""
+    return [((1, 0, 0), -hi[0]), ((-1, 0, 0), lo[0]), ((0, 1, 0), -hi[1]), ((0, -1, 0), lo[1]),
+            ((0, 0, 1), -hi[2]), ((0, 0, -1), lo[2])]
+
+
+def triangular_prism(size, depth):
+    """ConvexSolid::triangular_prism (spectral-core/src/geom.rs:89-103), f32 trig."""
+    out = []
+    for k in range(3):
+        ang = np.float32(np.float32(np.pi / 2) + np.float32(k) * np.float32(2.0) * np.float32(np.pi) / np.float32(3.0))
+        out.append(((float(np.cos(ang)), float(np.sin(ang)), 0.0), -size))
+    out += [((0, 0, 1), -depth / 2.0), ((0, 0, -1), -depth / 2.0)]
+    return out
+
+
+def wedge(apex_deg, size, depth):
+    """ConvexSolid::wedge (spectral-core/src/geom.rs:110-121)."""
+    a = np.float32(apex_deg) * np.float32(np.float32(np.pi) / np.float32(180.0))
+    return [((-1, 0, 0), -size), ((float(np.cos(a)), float(np.sin(a)), 0.0), -size), ((0, -1, 0), -size),
+            ((0, 0, 1), -depth / 2.0), ((0, 0, -1), -depth / 2.0)]
+
+
+def dsotm_params(width, height, seed, **kw):
+    return oracle.vol_params(width, height, seed, **kw)

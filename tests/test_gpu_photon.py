@@ -1,0 +1,300 @@
+"""GPU parity of the forward photon + haze path against the CPU oracle.
+
+Restates the reference's GPU gates (spectral-gpu/src/vol_photons.rs tests,
+spectral-gpu/tests/rng_parity.rs, spectral-gpu/src/film.rs tests) with the
+tolerances of this build:
+  * RNG stream: bit-identical;
+  * per-photon states: exact bounce count, origin/direction within PATH_TOL
+    (the reference asserts 1e-4, its README claims ~1e-6);
+  * films: relative L1 within FILM_TOL of the oracle (reference gate 5 %).
+"""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import spectral_b200 as sb
+from spectral_b200 import _lib
+
+from helpers import energy_delta, obeam, ocam, oscene, rel_l1
+
+pytestmark = pytest.mark.gpu
+
+PATH_TOL = 1e-6      # per-photon origin / direction
+FILM_TOL = 5e-3      # relative L1 of films / XYZ images (0.5 %)
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_rng_stream_bit_identical(ctx):
+    out = (C.c_uint32 * 16)()
+    _lib.check(_lib.lib.sc_rng_draws(ctx.h, 0xABCD, 0x1234, 16, out))
+    golden = json.load(open(os.path.join(GOLDEN, "rng_draws.json")))["key_0xABCD_seed_0x1234"]
+    assert list(out) == golden
+    assert list(out)[:4] == [0xA1DD5847, 0x13248A2D, 0x37278DEF, 0xDE1D5B62]
+    cpu = (C.c_uint32 * 1000)()
+    oracle.lib.or_rng_draws_u32(0xFFFFFFFF, 99, 1000, cpu)
+    gpu = (C.c_uint32 * 1000)()
+    _lib.check(_lib.lib.sc_rng_draws(ctx.h, 0xFFFFFFFF, 99, 1000, gpu))
+    assert list(cpu) == list(gpu)
+
+
+def run_parity_for_beam(ctx, beam, seed, count, label, spectral=True, max_bounces=8):
+    scene, _, cam = sb.dsotm_scene(1.0)
+    film = sb.GpuPhotonFilm(ctx, scene, cam, beam, 256, 256, count, seed, 14.0, sb.VolWeights(),
+                            max_bounces=max_bounces)
+    film.set_spectral(spectral)
+    num, lam, states = film.trace_debug(count, seed, count)
+    osc, ob = oscene(scene), obeam(beam)
+    p = oracle.vol_params(256, 256, seed, max_dist=14.0, spectral=1 if spectral else 0, max_bounces=max_bounces)
+    max_o = max_d = 0.0
+    total_tir, violet, tir_probe = 0, None, None
+    for i in range(count):
+        n, l, st, tir = oracle.simulate_photon(osc, ob, p, i)
+        assert np.float32(lam[i]).tobytes() == np.float32(l).tobytes(), (label, i)
+        assert num[i] == min(n, 9), "[%s] photon %d lambda %.1f: GPU bounce count %d != CPU %d" % (
+            label, i, l, num[i], n)
+        for b in range(min(n, 9)):
+            go, gd = states[i, 2 * b, :3], states[i, 2 * b + 1, :3]
+            co, cd = st[b, 0, :3], st[b, 1, :3]
+            od, dd = float(np.linalg.norm(go - co)), float(np.linalg.norm(gd - cd))
+            max_o, max_d = max(max_o, od), max(max_d, dd)
+            assert od <= PATH_TOL and dd <= PATH_TOL, (label, i, b, go, co, gd, cd)
+        if l < 430.0 and n > 1 and violet is None:
+            violet = i
+        if tir > 0 and tir_probe is None:
+            tir_probe = i
+        total_tir += tir
+    return max_o, max_d, total_tir, violet, tir_probe
+
+
+def test_forward_parity_gpu_matches_cpu(ctx):
+    _, dsotm, _ = sb.dsotm_scene(1.0)
+    mo, md, tir1, violet, _ = run_parity_for_beam(ctx, dsotm, 42, 512, "dsotm")
+    assert violet is not None, "no violet photon entered the prism"
+    mo2, md2, tir2, _, tir_probe = run_parity_for_beam(ctx, sb.tir_beam(), 42, 512, "tir")
+    assert tir2 > 0 and tir_probe is not None, "TIR beam produced no total internal reflection"
+    print("parity dsotm max dO=%.3g dD=%.3g; tir max dO=%.3g dD=%.3g, %d TIR bounces" % (mo, md, mo2, md2, tir2))
+
+
+def test_forward_parity_against_golden_fixture(ctx):
+    g = np.load(os.path.join(GOLDEN, "dsotm_photons.npz"))
+    for name, beam in [("dsotm", sb.dsotm_scene(1.0)[1]), ("tir", sb.tir_beam())]:
+        scene, _, cam = sb.dsotm_scene(1.0)
+        film = sb.GpuPhotonFilm(ctx, scene, cam, beam, 256, 256, 64, 42, 14.0, sb.VolWeights())
+        num, lam, states = film.trace_debug(64, 42, 64)
+        assert (num == np.minimum(g[name + "_num_states"], 9)).all()
+        assert lam.tobytes() == g[name + "_lambda"].tobytes()
+        for i in range(64):
+            k = int(num[i])
+            gs = g[name + "_states"][i, :k].reshape(2 * k, 4)
+            assert np.abs(states[i, :2 * k] - gs).max() <= PATH_TOL
+
+
+def test_parity_spectral_off_and_short_bounce_loop(ctx):
+    _, dsotm, _ = sb.dsotm_scene(1.0)
+    run_parity_for_beam(ctx, dsotm, 5, 256, "n550", spectral=False)
+    run_parity_for_beam(ctx, sb.tir_beam(), 9, 256, "mb3", max_bounces=3)
+
+
+def dsotm_film(ctx, w, h, n, seed, **kw):
+    scene, beam, cam = sb.dsotm_scene(1.0)
+    zbuf = kw.pop("zbuffer", None)
+    f = sb.GpuPhotonFilm(ctx, scene, cam, beam, w, h, n, seed, 14.0, kw.pop("weights", sb.VolWeights()),
+                         zbuffer=zbuf, **kw)
+    return f, scene, beam, cam
+
+
+def test_vol_diff_gate(ctx):
+    w, h, n, seed = 200, 200, 200_000, 7
+    zbuf = np.full(w * h, np.inf, np.float32)
+    film, scene, beam, cam = dsotm_film(ctx, w, h, n, seed, zbuffer=zbuf)
+    film.trace_and_resolve(n, seed)
+    gpu = film.accum()
+    raw = film.read_raw().reshape(-1)
+    p = oracle.vol_params(w, h, seed, 0.5, 0.06, 0.5, 14.0)
+    img, fx, _ = oracle.render_point(oscene(scene), ocam(cam), obeam(beam), p, 0, n, zbuf=zbuf)
+    l1, ed = rel_l1(gpu, img), energy_delta(gpu, img)
+    diff = np.abs(raw - fx)
+    print("vol_diff_gate: rel L1 %.3e energy %.3e; fixed-point cells differing %d, max %d quanta" % (
+        l1, ed, int((diff > 0).sum()), int(diff.max())))
+    assert img[1::3].sum() > 0
+    assert l1 < FILM_TOL and ed < FILM_TOL
+    # the 64-bit films agree to a few quanta (expf/powf last-bit differences only)
+    assert diff.max() <= 64 and rel_l1(raw, fx) < 1e-6
+    assert ((gpu > 0).reshape(-1, 3).any(1) == (img > 0).reshape(-1, 3).any(1)).mean() > 0.999
+
+
+def test_film_against_golden_fixture(ctx):
+    g = np.load(os.path.join(GOLDEN, "dsotm_film_64.npz"))
+    film, *_ = dsotm_film(ctx, 64, 64, 4096, 7)
+    film.trace_and_resolve(4096, 7)
+    raw = film.read_raw().reshape(-1)
+    assert rel_l1(raw, g["film_xyz"]) < 1e-6 and rel_l1(film.accum(), g["img_f32"]) < FILM_TOL
+
+
+def test_forward_gpu_determinism_and_chunking(ctx):
+    a, *_ = dsotm_film(ctx, 128, 128, 100_000, 99)
+    a.trace_and_resolve(100_000, 99)
+    b, *_ = dsotm_film(ctx, 128, 128, 100_000, 99)
+    b.trace_and_resolve(100_000, 99)
+    c, *_ = dsotm_film(ctx, 128, 128, 100_000, 99)
+    for base in range(0, 100_000, 30_000):
+        c.dispatch_photons(base, min(base + 30_000, 100_000), 99)
+    ra, rb, rc = a.read_raw(), b.read_raw(), c.read_raw()
+    assert (ra == rb).all() and (ra == rc).all() and ra.sum() > 0
+    assert a.accum().tobytes() == c.accum().tobytes()
+
+
+@pytest.mark.parametrize("aggregate", [0, 1])
+def test_warp_aggregated_splats_identical(ctx, aggregate, monkeypatch):
+    monkeypatch.setenv("SPECTRAL_CUDA_AGGREGATE", str(aggregate))
+    f, *_ = dsotm_film(ctx, 96, 96, 50_000, 3)
+    f.trace_and_resolve(50_000, 3)
+    monkeypatch.setenv("SPECTRAL_CUDA_AGGREGATE", "0")
+    g, *_ = dsotm_film(ctx, 96, 96, 50_000, 3)
+    g.trace_and_resolve(50_000, 3)
+    assert (f.read_raw() == g.read_raw()).all()
+
+
+@pytest.mark.parametrize("bins,band", [(64, (380.0, 730.0)), (32, (380.0, 780.0)), (7, (400.0, 700.0))])
+def test_spectral_film_parity(ctx, bins, band):
+    w, h, n, seed = 72, 41, 60_000, 11
+    film, scene, beam, cam = dsotm_film(ctx, w, h, n, seed, bins=bins, lambda_min=band[0], lambda_max=band[1])
+    film.trace_and_resolve(n, seed)
+    raw = film.read_raw()
+    p = oracle.vol_params(w, h, seed, 0.5, 0.06, 0.5, 14.0, bins=bins, lambda_min=band[0], lambda_max=band[1])
+    _, _, fs = oracle.render_point(oscene(scene), ocam(cam), obeam(beam), p, 0, n, f32=False, xyz=False, spec=True)
+    fs = fs.reshape(h, w, bins)
+    assert rel_l1(raw, fs) < 1e-6 and np.abs(raw - fs).max() <= 64
+    # sensor reduction: sum_b count * bin-averaged CMF / 2^32
+    wts = oracle.bin_weights(bins, *band).astype(np.float64)
+    expect = (fs.reshape(-1, bins).astype(np.float64) @ wts.T) * 2.0 ** -32
+    got = film.accum().reshape(-1, 3)
+    assert rel_l1(got, expect) < 1e-6
+
+
+def test_zbuffer_occlusion_and_legacy_estimator(ctx):
+    w, h, n, seed = 80, 60, 40_000, 21
+    zb = np.full(w * h, np.inf, np.float32)
+    zb[: w * h // 2] = 11.5  # occlude the top half behind depth 11.5
+    film, scene, beam, cam = dsotm_film(ctx, w, h, n, seed, zbuffer=zb)
+    film.trace_and_resolve(n, seed)
+    p = oracle.vol_params(w, h, seed, 0.5, 0.06, 0.5, 14.0)
+    _, fx, _ = oracle.render_point(oscene(scene), ocam(cam), obeam(beam), p, 0, n, zbuf=zb, f32=False)
+    assert rel_l1(film.read_raw().reshape(-1), fx) < 1e-6
+    film2, *_ = dsotm_film(ctx, w, h, n, seed, estimator=1, weights=sb.VolWeights(0.05, 0.05, 0.0))
+    film2.trace_and_resolve(n, seed)
+    p2 = oracle.vol_params(w, h, seed, 0.05, 0.05, 0.0, 14.0, estimator=1)
+    _, fx2, _ = oracle.render_point(oscene(scene), ocam(cam), obeam(beam), p2, 0, n, f32=False)
+    assert rel_l1(film2.read_raw().reshape(-1), fx2) < 1e-6
+
+
+def test_surface_rim_matches_cpu(ctx):
+    w, h = 300, 300
+    scene, beam, cam = sb.dsotm_scene(1.0)
+    film = sb.GpuPhotonFilm(ctx, scene, cam, beam, w, h, 1, 0, 14.0)
+    film.recompute_surface(cam)
+    gpu = film.surface()
+    cpu = np.zeros(3 * w * h, np.float32)
+    oracle.lib.or_surface_rim(C.byref(oscene(scene).c), C.byref(ocam(cam)), w, h, oracle.fp(cpu))
+    gnz, cnz = (gpu.reshape(-1, 3) > 0).any(1).sum(), (cpu.reshape(-1, 3) > 0).any(1).sum()
+    assert gnz == cnz and cnz > 0
+    assert np.abs(gpu - cpu).max() < 1e-4
+
+
+def test_exposure_tonemap_and_gather(ctx):
+    w, h, n = 160, 120, 50_000
+    film, scene, beam, cam = dsotm_film(ctx, w, h, n, 4)
+    film.trace_and_resolve(n, 4)
+    film.recompute_surface()
+    acc, surf = film.accum(), film.surface()
+    comp_y = acc[1::3] + surf[1::3]
+    assert abs(film.auto_expose(1.0) - max(1.0 / max(float(comp_y.max()), 1e-6), 1.0)) < 1e-6 * film.auto_expose(1.0)
+    k = min(int(np.float32(w * h) * np.float32(0.997)), w * h - 1)
+    assert film.auto_expose_p997() == np.float32(1.0) / max(np.sort(comp_y)[k], np.float32(1e-9))
+    exp = film.auto_expose_p997()
+    rgb = film.to_rgb8(exp).reshape(-1, 3).astype(int)
+    ref = np.zeros_like(rgb)
+    out = (C.c_uint8 * 3)()
+    lin = np.zeros(3, np.float32)
+    for i in range(w * h):
+        c = (acc[3 * i:3 * i + 3] + surf[3 * i:3 * i + 3]).astype(np.float32)
+        oracle.lib.or_xyz_to_linear_srgb(oracle.fp(c), oracle.fp(lin))
+        oracle.lib.or_tonemap_to_u8(oracle.fp(lin), exp, out)
+        ref[i] = list(out)
+    assert np.abs(rgb - ref).max() <= 1 and (rgb != ref).mean() < 1e-3
+    g = film.gather_rgba8(n, 4_000_000.0, 2.0, 1.0).reshape(-1, 4).astype(int)
+    gr = np.zeros((w * h, 4), np.uint8)
+    oracle.lib.or_gather_tonemap(oracle.fp(acc), oracle.fp(surf), w, h, np.float32(1.0) / np.float32(n) *
+                                 np.float32(4e6), 2.0, 1.0, gr.ctypes.data_as(C.POINTER(C.c_uint8)))
+    assert np.abs(g - gr.astype(int)).max() <= 1 and (g != gr).mean() < 1e-3
+
+
+def test_edge_cases(ctx):
+    scene, beam, cam = sb.dsotm_scene(1.0)
+    # odd film sizes, a single pixel, zero photons, photon ranges with an offset
+    for w, h in [(1, 1), (9, 7), (17, 33)]:
+        f = sb.GpuPhotonFilm(ctx, scene, cam, beam, w, h, 10, 1, 14.0)
+        f.trace_and_resolve(0, 1)
+        assert not f.accum().any()
+        f.trace_and_resolve(5000, 1)
+        p = oracle.vol_params(w, h, 1, 0.5, 0.06, 0.5, 14.0)
+        _, fx, _ = oracle.render_point(oscene(scene), ocam(cam), obeam(beam), p, 0, 5000, f32=False)
+        assert rel_l1(f.read_raw().reshape(-1), fx) < 1e-6
+    f = sb.GpuPhotonFilm(ctx, scene, cam, beam, 40, 40, 10, 1, 14.0)
+    f.dispatch_photons(1000, 3000, 5)
+    p = oracle.vol_params(40, 40, 5, 0.5, 0.06, 0.5, 14.0)
+    _, fx, _ = oracle.render_point(oscene(scene), ocam(cam), obeam(beam), p, 1000, 3000, f32=False)
+    assert rel_l1(f.read_raw().reshape(-1), fx) < 1e-6
+    # empty scene: photons stream straight through the haze
+    empty = sb.Scene(background=0.0)
+    f = sb.GpuPhotonFilm(ctx, empty, cam, beam, 32, 32, 10, 1, 14.0)
+    f.trace_and_resolve(2000, 2)
+    p = oracle.vol_params(32, 32, 2, 0.5, 0.06, 0.5, 14.0)
+    _, fx, _ = oracle.render_point(oscene(empty), ocam(cam), obeam(beam), p, 0, 2000, f32=False)
+    assert rel_l1(f.read_raw().reshape(-1), fx) < 1e-6 and fx.sum() > 0
+    # clear resets the accumulator
+    f.clear_film()
+    assert not f.read_raw().any()
+    # max bins
+    f = sb.GpuPhotonFilm(ctx, scene, cam, beam, 16, 16, 10, 1, 14.0, bins=256)
+    f.trace_and_resolve(3000, 1)
+    assert f.read_raw().shape == (16, 16, 256) and f.accum().sum() > 0
+
+
+def test_invalid_arguments_raise(ctx):
+    scene, beam, cam = sb.dsotm_scene(1.0)
+    bad = sb.Scene()
+    bad.add_solid([((1, 0, 0), -1)], sb.Dielectric(7))  # glass id out of range
+    with pytest.raises(_lib.SpectralError) as e:
+        sb.GpuPhotonFilm(ctx, bad, cam, beam, 8, 8, 1, 1, 14.0)
+    assert e.value.code == _lib.SC_E_INVALID
+    big = sb.Scene()
+    for i in range(70):
+        big.add_sphere((i, 0, 0), 0.1, sb.Lambertian(0.5))
+    with pytest.raises(_lib.SpectralError) as e:
+        sb.GpuPhotonFilm(ctx, big, cam, beam, 8, 8, 1, 1, 14.0)
+    assert e.value.code == _lib.SC_E_LIMIT
+    with pytest.raises(_lib.SpectralError):
+        sb.GpuPhotonFilm(ctx, scene, cam, beam, 8, 8, 1, 1, 14.0, bins=300)
+    with pytest.raises(ValueError):
+        sb.GpuPhotonFilm(ctx, scene, cam, beam, 8, 8, 1, 1, 14.0, zbuffer=np.zeros(3))
+
+
+def test_atomic_film(ctx):
+    w, h = 32, 32
+    assert sb.check_determinism(ctx, w, h, 0xDEADBEEF, 4096) is None
+    f = sb.AtomicFilm(ctx, w, h)
+    f.splat(0xABCD1234, 8192)
+    raw = f.read_film_raw()
+    ref = np.zeros(3 * w * h, np.uint32)
+    oracle.lib.or_synthetic_splat(w, h, 0xABCD1234, 8192, ref.ctypes.data_as(C.POINTER(C.c_uint32)))
+    assert (raw == ref).all() and (raw > 0).any()
+    f.resolve()
+    assert not f.read_film_raw().any()
+    assert np.array_equal(f.accum(), ref.astype(np.float32) / np.float32(4096.0))
+    f.clear_accum()
+    assert not f.accum().any()
