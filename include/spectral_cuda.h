@@ -154,6 +154,39 @@ int sc_photon_film_set_scene(sc_photon_film* f, const sc_primitive* prims, uint3
 int sc_photon_film_trace_stats(sc_photon_film* f, uint32_t photon_base, uint32_t count, uint32_t seed,
                                uint64_t out[4]);
 
+/* ---- camera tracer: GpuTracer (spectral-gpu/src/lib.rs:165-389) -------- */
+typedef struct sc_tracer sc_tracer;
+/* Extensions beyond the reference (zero = reference behaviour). */
+typedef struct {
+    uint32_t max_depth;        /* 0 -> 8 (tracer.rs:26) */
+    uint32_t rr_start;         /* Russian roulette once this many scatters happened (0 = off) */
+    float emitter_center[3];   /* spherical emitter (radius 0 = none) */
+    float emitter_radius;
+    float emitter_scale;       /* emitted radiance = scale * illuminant(lambda) */
+} sc_tracer_options;
+/* GpuTracer::new (lib.rs:179-187), CpuTracer::new (tracer.rs:20-37).
+ * illuminant 0 D65, 1 A; has_horizon/horizon: Scene::horizon (scene.rs:25-28). */
+int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims,
+                     const sc_plane* planes, uint32_t n_planes, const sc_material* mats,
+                     uint32_t n_mats, float background, int has_horizon, float horizon,
+                     const sc_camera* cam, uint32_t width, uint32_t height,
+                     uint32_t illuminant, uint32_t seed, const sc_tracer_options* opts,
+                     sc_tracer** out);
+int sc_tracer_destroy(sc_tracer* t);
+/* accumulate (lib.rs:307-321): spp more samples per pixel; sample indices
+ * continue across calls as in CpuTracer::accumulate (tracer.rs:115-141).
+ * Asynchronous. */
+int sc_tracer_accumulate(sc_tracer* t, uint32_t spp);
+/* read_xyz (lib.rs:324-357): per-pixel mean XYZ, out 3*w*h. */
+int sc_tracer_read_xyz(sc_tracer* t, float* out);
+/* set_camera (lib.rs:376-383). */
+int sc_tracer_set_camera(sc_tracer* t, const sc_camera* cam);
+/* clear_accum (lib.rs:386-389): zero the sum and the sample count. */
+int sc_tracer_clear_accum(sc_tracer* t);
+int sc_tracer_dims(sc_tracer* t, uint32_t* width, uint32_t* height);
+/* paths of the last accumulate and path segments traced since creation. */
+int sc_tracer_last_stats(sc_tracer* t, uint64_t* paths, uint64_t* segments);
+
 /* ---- atomic film: AtomicFilm (spectral-gpu/src/film.rs:40-305) --------- */
 typedef struct sc_atomic_film sc_atomic_film;
 int sc_atomic_film_create(sc_ctx* ctx, uint32_t width, uint32_t height, sc_atomic_film** out);

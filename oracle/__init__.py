@@ -64,6 +64,10 @@ class or_vol_params(C.Structure):
                 ("scale", C.c_float), ("estimator", C.c_uint32)]
 
 
+class or_tracer_ext(C.Structure):
+    _fields_ = [("center", F3), ("radius", C.c_float), ("scale", C.c_float), ("rr_start", C.c_uint32)]
+
+
 P = C.POINTER
 _lib = C.CDLL(LIB_PATH)
 _u32, _f32, _i32, _vp = C.c_uint32, C.c_float, C.c_int, C.c_void_p
@@ -100,6 +104,7 @@ for name, res, args in [
     ("or_tracer_accumulate_mt", None, [P(or_scene), P(or_camera), _u32, _u32, _u32, _u32, _u32, _u32, _u32, P(_f32),
                                        _i32]),
     ("or_tracer_sample", None, [P(or_scene), P(or_camera), _u32, _u32, _u32, _u32, _u32, _u32, _u32, _u32, P(_f32)]),
+    ("or_tracer_set_ext", None, [_vp]),
     ("or_scatter", _i32, [_u32, _f32, P(_f32), P(_f32), _i32, _f32, _u32, _u32, P(_f32), P(_f32)]),
     ("or_simulate_photon_fixed", _u32, [P(or_scene), P(or_beam), P(or_vol_params), _u32, _f32, _u32, P(_f32)]),
     ("or_mean_landing", _u32, [P(or_scene), P(_f32), P(or_beam), _f32, _u32, _u32, P(_f32)]),
@@ -174,6 +179,17 @@ def simulate_photon(scene, beam, p, idx, max_pairs=9):
     n = _lib.or_simulate_photon(C.byref(scene.c), C.byref(beam), C.byref(p), idx, max_pairs, fp(st), C.byref(lam),
                                 C.byref(tir))
     return n, lam.value, st.reshape(max_pairs, 2, 4), tir.value
+
+
+def tracer_accumulate(scene, cam, w, h, illuminant, seed, spp, base=0, max_bounces=8, threads=8, ext=None,
+                      out=None):
+    """CpuTracer::accumulate into `out` (3*w*h f32 running sum); returns it."""
+    out = np.zeros(3 * w * h, np.float32) if out is None else out
+    _lib.or_tracer_set_ext(C.byref(ext) if ext is not None else None)
+    _lib.or_tracer_accumulate_mt(C.byref(scene.c), C.byref(cam), w, h, illuminant, seed, spp, base, max_bounces,
+                                 fp(out), threads)
+    _lib.or_tracer_set_ext(None)
+    return out
 
 
 def tables():

@@ -642,6 +642,11 @@ void or_lighttrace(const or_scene* sc, const float scr[9], uint32_t W, uint32_t 
 /* ------------------------------------------------------------------------ */
 /* tracer.rs:44-111, spectrum.rs:20-32, scene.rs:44-50                      */
 /* ------------------------------------------------------------------------ */
+static or_tracer_ext g_ext; /* zero: reference behaviour */
+void or_tracer_set_ext(const or_tracer_ext* ext) {
+    if (ext) g_ext = *ext; else memset(&g_ext, 0, sizeof g_ext);
+}
+
 void or_tracer_sample(const or_scene* sc, const or_camera* cam, uint32_t W, uint32_t H,
                       uint32_t illum, uint32_t seed, uint32_t px, uint32_t py, uint32_t sidx,
                       uint32_t max_bounces, float out[3]) {
@@ -663,7 +668,16 @@ void or_tracer_sample(const or_scene* sc, const or_camera* cam, uint32_t W, uint
     uint32_t valid = 4;
     for (uint32_t b = 0; b < max_bounces; ++b) {
         hit_t h; uint32_t mi = 0;
-        if (!scene_hit(sc, o, d, &h, &mi)) {
+        int any = scene_hit(sc, o, d, &h, &mi);
+        if (g_ext.radius > 0.0f) {
+            or_prim em = {{g_ext.center[0], g_ext.center[1], g_ext.center[2]}, g_ext.radius, 0, 0, 0, 0};
+            hit_t he;
+            if (sphere_hit(&em, o, d, 1e-3f, any ? h.t : INFINITY, &he)) {
+                for (int k = 0; k < 4; ++k) rad[k] += tp[k] * g_ext.scale * or_illuminant(illum, lam[k]);
+                break;
+            }
+        }
+        if (!any) {
             float bg = sc->background + ((sc->has_horizon && d.y > 0.0f) ? sc->horizon : 0.0f);
             for (int k = 0; k < 4; ++k) rad[k] += tp[k] * bg * or_illuminant(illum, lam[k]);
             break;
@@ -675,6 +689,11 @@ void or_tracer_sample(const or_scene* sc, const or_camera* cam, uint32_t W, uint
         for (int k = 0; k < 4; ++k) tp[k] *= w;
         if (m->kind == 1u && valid > 1) { tp[1] = tp[2] = tp[3] = 0.0f; valid = 1; }
         o = h.point; d = nd;
+        if (g_ext.rr_start && b + 1 >= g_ext.rr_start) {
+            float q = fminf(tp[0], 0.95f);
+            if (!(rng_f32(&r) < q)) break;
+            for (int k = 0; k < 4; ++k) tp[k] = tp[k] / q;
+        }
     }
     float x = 0, y = 0, z = 0;
     for (int k = 0; k < 4; ++k) {

@@ -109,6 +109,13 @@ void or_render_beam(const or_scene* sc, const or_camera* cam, const or_beam* bea
 void or_lighttrace(const or_scene* sc, const float screen_cuv[9], uint32_t w, uint32_t h,
                    const or_beam* beam, const or_vol_params* p, uint32_t n, float* sum_xyz);
 
+/* Camera-tracer extensions with no counterpart in the reference (all zero =
+ * reference behaviour): a spherical emitter whose radiance is
+ * emitter_scale * illuminant(lambda), and Russian roulette after rr_start
+ * scatters (survival p = min(throughput, 0.95), throughput /= p). */
+typedef struct { float center[3]; float radius; float scale; uint32_t rr_start; } or_tracer_ext;
+void or_tracer_set_ext(const or_tracer_ext* ext);
+
 /* Hero-wavelength camera tracer (tracer.rs:44-141). Accumulates spp samples starting
  * at sample index `base` into sum_xyz (3*w*h); rows [row0,row1). */
 void or_tracer_accumulate(const or_scene* sc, const or_camera* cam, uint32_t w, uint32_t h,

@@ -321,6 +321,61 @@ class GpuPhotonFilm:
             pass
 
 
+class GpuTracer:
+    """GpuTracer (spectral-gpu/src/lib.rs:165-389): wavefront hero-wavelength
+    camera tracer.  Keyword extensions (no reference counterpart): max_depth,
+    rr_start, emitter=(center, radius, scale)."""
+
+    def __init__(self, ctx, scene, camera, width, height, illuminant=D65, seed=0, max_depth=8, rr_start=0,
+                 emitter=None):
+        self.width, self.height = int(width), int(height)
+        prims, np_, planes, npl, mats, nm = scene.arrays()
+        opts = _lib.sc_tracer_options()
+        opts.max_depth, opts.rr_start = int(max_depth), int(rr_start)
+        if emitter is not None:
+            c, r, s = emitter
+            opts.emitter_center, opts.emitter_radius, opts.emitter_scale = _f3(c), float(r), float(s)
+        self.h = C.c_void_p()
+        check(lib.sc_tracer_create(ctx.h, prims, np_, planes, npl, mats, nm, scene.background,
+                                   1 if scene.horizon is not None else 0,
+                                   float(scene.horizon) if scene.horizon is not None else 0.0, C.byref(camera.c),
+                                   self.width, self.height, int(illuminant), int(seed), C.byref(opts),
+                                   C.byref(self.h)))
+
+    def accumulate(self, spp):
+        check(lib.sc_tracer_accumulate(self.h, int(spp)))
+
+    def read_xyz(self):
+        out = np.empty(3 * self.width * self.height, np.float32)
+        check(lib.sc_tracer_read_xyz(self.h, _fptr(out)))
+        return out
+
+    def set_camera(self, camera):
+        check(lib.sc_tracer_set_camera(self.h, C.byref(camera.c)))
+
+    def clear_accum(self):
+        check(lib.sc_tracer_clear_accum(self.h))
+
+    def dims(self):
+        return self.width, self.height
+
+    def stats(self):
+        p, s = C.c_uint64(), C.c_uint64()
+        check(lib.sc_tracer_last_stats(self.h, C.byref(p), C.byref(s)))
+        return p.value, s.value
+
+    def close(self):
+        if self.h:
+            lib.sc_tracer_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 N_SPLATS = 1_000_000
 
 

@@ -59,6 +59,11 @@ class sc_film_options(C.Structure):
                 ("max_bounces", C.c_uint32), ("scale_log2", C.c_uint32), ("estimator", C.c_uint32)]
 
 
+class sc_tracer_options(C.Structure):
+    _fields_ = [("max_depth", C.c_uint32), ("rr_start", C.c_uint32), ("emitter_center", F3),
+                ("emitter_radius", C.c_float), ("emitter_scale", C.c_float)]
+
+
 class sc_trace_desc(C.Structure):
     _fields_ = [("prims", C.c_void_p), ("n_prims", C.c_uint32), ("planes", C.c_void_p), ("n_planes", C.c_uint32),
                 ("mats", C.c_void_p), ("n_mats", C.c_uint32), ("cam", sc_camera), ("beam", sc_beam),
@@ -110,6 +115,15 @@ PROTOTYPES = {
                                         P(sc_camera), P(sc_beam)]),
     "sc_photon_film_trace_stats": (_i32, [_vp, _u32, _u32, _u32, P(_u64)]),
     "sc_trace_stats_device": (_i32, [_vp, P(sc_trace_desc), _u32, _u32, _vp, _vp]),
+    "sc_tracer_create": (_i32, [_vp, P(sc_primitive), _u32, P(sc_plane), _u32, P(sc_material), _u32, _f32, _i32,
+                                _f32, P(sc_camera), _u32, _u32, _u32, _u32, P(sc_tracer_options), P(_vp)]),
+    "sc_tracer_destroy": (_i32, [_vp]),
+    "sc_tracer_accumulate": (_i32, [_vp, _u32]),
+    "sc_tracer_read_xyz": (_i32, [_vp, P(_f32)]),
+    "sc_tracer_set_camera": (_i32, [_vp, P(sc_camera)]),
+    "sc_tracer_clear_accum": (_i32, [_vp]),
+    "sc_tracer_dims": (_i32, [_vp, P(_u32), P(_u32)]),
+    "sc_tracer_last_stats": (_i32, [_vp, P(_u64), P(_u64)]),
     "sc_atomic_film_create": (_i32, [_vp, _u32, _u32, P(_vp)]),
     "sc_atomic_film_destroy": (_i32, [_vp]),
     "sc_atomic_film_splat": (_i32, [_vp, _u32, _u32]),

@@ -68,10 +68,18 @@ static void resolve_options(const sc_film_options* in, sc_film_options& o) {
     if (o.scale_log2 == 0u) o.scale_log2 = 32u;
 }
 
+static size_t mask_smem(uint32_t w, uint32_t h) {
+    const uint32_t words = flag_words(w, h);
+    return words <= kMaxSmemMaskWords ? words * sizeof(uint32_t) : 0;
+}
+
 static int default_shape(sc_ctx* ctx, bool spectral, int aggregate, size_t smem, LaunchShape& s) {
     s.block = 256;
     s.aggregate = aggregate;
-    const int per_sm = photon_occupancy_blocks(s.block, spectral, aggregate, smem);
+    s.minb = 4;
+    if (const char* agg = std::getenv("SPECTRAL_CUDA_AGGREGATE")) s.aggregate = std::atoi(agg) ? 1 : 0;
+    if (const char* mb = std::getenv("SPECTRAL_CUDA_MINB")) s.minb = std::atoi(mb) >= 5 ? 5 : 4;
+    const int per_sm = photon_occupancy_blocks(s, spectral, smem);
     s.grid = (uint32_t)(ctx->sms * per_sm);
     return SC_OK;
 }
@@ -331,7 +339,7 @@ int sc_photon_film_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_pri
     if ((e = f->planes.alloc(n_planes)) != cudaSuccess) return fail(e);
     if ((e = f->mats.alloc(n_mats)) != cudaSuccess) return fail(e);
     if ((e = f->film.alloc(f->geom.cells())) != cudaSuccess) return fail(e);
-    if ((e = f->flags.alloc(f->geom.tiles())) != cudaSuccess) return fail(e);
+    if ((e = f->flags.alloc(flag_words(width, height))) != cudaSuccess) return fail(e);
     if ((e = f->xyz.alloc(3 * npx)) != cudaSuccess) return fail(e);
     if ((e = f->surface.alloc(3 * npx)) != cudaSuccess) return fail(e);
     if ((e = f->work.alloc(264)) != cudaSuccess) return fail(e);
@@ -352,8 +360,8 @@ int sc_photon_film_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_pri
     if ((e = cudaMemsetAsync(f->flags.p, 0, f->flags.bytes(), f->stream)) != cudaSuccess) return fail(e);
     if ((e = cudaMemsetAsync(f->surface.p, 0, f->surface.bytes(), f->stream)) != cudaSuccess) return fail(e);
     if ((e = cudaStreamSynchronize(f->stream)) != cudaSuccess) return fail(e);
-    default_shape(ctx, o.bins != 0, 0, scene_smem_bytes(n_prims, n_planes, n_mats), f->shape);
-    if (const char* agg = std::getenv("SPECTRAL_CUDA_AGGREGATE")) f->shape.aggregate = std::atoi(agg) ? 1 : 0;
+    default_shape(ctx, o.bins != 0, 0, scene_smem_bytes(n_prims, n_planes, n_mats) + mask_smem(width, height),
+                  f->shape);
     *out = f;
     return SC_OK;
     SC_GUARD_END
@@ -635,7 +643,7 @@ int sc_photon_film_trace_stats(sc_photon_film* f, uint32_t base, uint32_t count,
 
 // ---------------------------- device-pointer API ---------------------------
 size_t sc_film_bytes(uint32_t w, uint32_t h, uint32_t channels) { return film_geom(w, h, channels).cells() * 8u; }
-size_t sc_film_flag_bytes(uint32_t w, uint32_t h) { return film_geom(w, h, 1).tiles() * 4u; }
+size_t sc_film_flag_bytes(uint32_t w, uint32_t h) { return (size_t)flag_words(w, h) * 4u; }
 
 int sc_trace_photons_device(sc_ctx* ctx, const sc_trace_desc* d, uint32_t base, uint32_t count, void* film_dev,
                             uint32_t* flags_dev, void* stream) {
@@ -657,8 +665,9 @@ int sc_trace_photons_device(sc_ctx* ctx, const sc_trace_desc* d, uint32_t base, 
     p.prims = d->prims; p.planes = d->planes; p.mats = d->mats; p.zbuf = d->zbuffer;
     p.film = static_cast<unsigned long long*>(film_dev); p.flags = flags_dev;
     LaunchShape shape;
-    default_shape(ctx, o.bins != 0, 0, scene_smem_bytes(d->n_prims, d->n_planes, d->n_mats), shape);
-    if (const char* agg = std::getenv("SPECTRAL_CUDA_AGGREGATE")) shape.aggregate = std::atoi(agg) ? 1 : 0;
+    default_shape(ctx, o.bins != 0, 0,
+                  scene_smem_bytes(d->n_prims, d->n_planes, d->n_mats) + (flags_dev ? mask_smem(d->width, d->height) : 0),
+                  shape);
     SC_CUDA(launch_photons(p, shape, static_cast<cudaStream_t>(stream)));
     return SC_OK;
     SC_GUARD_END

@@ -19,7 +19,7 @@ __device__ __forceinline__ void reduce_tile(const ReduceParams& p, uint32_t tile
                                             unsigned long long* sm, double* part) {
     const uint32_t C = p.channels;
     const uint32_t tx = tile % p.tiles_x, ty = tile / p.tiles_x;
-    const bool dirty = p.flags == nullptr || p.flags[tile] != 0u;
+    const bool dirty = p.flags == nullptr || (p.flags[tile >> 5] >> (tile & 31u)) & 1u;
     const uint32_t tid = threadIdx.x;
     if (!dirty) {
         for (uint32_t i = tid; i < kTilePixels * 3u; i += blockDim.x) {
@@ -74,7 +74,7 @@ __device__ __forceinline__ void reduce_tile(const ReduceParams& p, uint32_t tile
             }
         }
     }
-    if (drain && p.flags && tid == 0) p.flags[tile] = 0u;
+    if (drain && p.flags && tid == 0) atomicAnd(p.flags + (tile >> 5), ~(1u << (tile & 31u)));
     __syncthreads();
 }
 

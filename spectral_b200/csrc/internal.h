@@ -28,13 +28,24 @@ struct PhotonParams {
     sc_debug_photon* debug;           // debug launches only
 };
 
-struct LaunchShape { uint32_t block, grid; int aggregate; };
+// Photon launch: CTAs of 256 threads, `grid` CTAs (grid-stride), warp
+// aggregation on/off, register bound (minimum CTAs per SM: 4 or 5).
+struct LaunchShape { uint32_t block, grid; int aggregate; int minb; };
+
+// Dirty-tile masks up to this many 32-bit words (16 KB, 524288 tiles) are
+// accumulated in shared memory by each photon CTA.
+constexpr uint32_t kMaxSmemMaskWords = 4096;
+// Dirty-tile mask: one bit per 8x8 tile, 32-bit words.
+__host__ __device__ __forceinline__ uint32_t flag_words(uint32_t width, uint32_t height) {
+    return (((width + 7u) / 8u) * ((height + 7u) / 8u) + 31u) / 32u;
+}
 
 size_t scene_smem_bytes(uint32_t n_prims, uint32_t n_planes, uint32_t n_mats);
+uint32_t photon_mask_words(const PhotonParams& p);
 cudaError_t launch_photons(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s);
 cudaError_t launch_photon_debug(const PhotonParams& p, cudaStream_t s);
 cudaError_t launch_photon_count(const PhotonParams& p, unsigned long long* out, uint32_t grid, cudaStream_t s);
-int photon_occupancy_blocks(uint32_t block, bool spectral, int aggregate, size_t smem);
+int photon_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem);
 
 struct RimParams {
     sc_camera cam;

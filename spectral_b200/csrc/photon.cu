@@ -35,17 +35,23 @@ __device__ __forceinline__ unsigned long long peer_sum64(unsigned peers, unsigne
     return (unsigned long long)s0 + ((unsigned long long)s1 << 26) + ((unsigned long long)s2 << 52);
 }
 
-__device__ __forceinline__ void mark_tile(uint32_t* flags, uint32_t tile) {
-    if (flags) {
-        volatile uint32_t* f = flags + tile;
-        if (*f == 0u) *f = 1u;
+// Dirty-tile bitmask: bits go to this CTA's shared-memory copy (flushed to the
+// global mask when the CTA finishes) or, for films whose mask does not fit,
+// straight to the global mask with a fire-and-forget red.or.
+__device__ __forceinline__ void mark_tile(const PhotonParams& p, uint32_t* smask, uint32_t tile) {
+    if (!p.flags) return;
+    const uint32_t w = tile >> 5, bit = 1u << (tile & 31u);
+    if (smask) {
+        if (!(smask[w] & bit)) atomicOr(smask + w, bit);
+    } else {
+        atomicOr(p.flags + w, bit);
     }
 }
 
 // Deposit one haze sample.  AGG=1 merges lanes of the warp that hit the same
 // film cell before issuing the atomic.
 template <bool SPEC, int AGG>
-__device__ __forceinline__ void deposit(const PhotonParams& p, bool ok, uint32_t px, uint32_t py,
+__device__ __forceinline__ void deposit(const PhotonParams& p, uint32_t* smask, bool ok, uint32_t px, uint32_t py,
                                         float contrib, float cx, float cy, float cz, uint32_t bin) {
     size_t cell = 0;
     uint32_t tile = 0;
@@ -63,7 +69,7 @@ __device__ __forceinline__ void deposit(const PhotonParams& p, bool ok, uint32_t
     }
     if (AGG == 0) {
         if (!ok) return;
-        mark_tile(p.flags, tile);
+        mark_tile(p, smask, tile);
         red_u64(p.film + cell, v0);
         if (!SPEC) { red_u64(p.film + cell + 1, v1); red_u64(p.film + cell + 2, v2); }
         return;
@@ -78,7 +84,7 @@ __device__ __forceinline__ void deposit(const PhotonParams& p, bool ok, uint32_t
         if (!SPEC) { v1 = peer_sum64(peers, v1); v2 = peer_sum64(peers, v2); }
         if ((int)lane != __ffs(peers) - 1) return;
     }
-    mark_tile(p.flags, tile);
+    mark_tile(p, smask, tile);
     red_u64(p.film + cell, v0);
     if (!SPEC) { red_u64(p.film + cell + 1, v1); red_u64(p.film + cell + 2, v2); }
 }
@@ -97,7 +103,7 @@ struct PhotonCounts { uint32_t segments, splats, scatters; };
 
 template <bool SPEC, int AGG, bool DEBUG, bool COUNT = false>
 __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneView& S, const float* cmf,
-                                             uint32_t idx, PhotonCounts* cnt = nullptr) {
+                                             uint32_t idx, uint32_t* smask, PhotonCounts* cnt = nullptr) {
     Rng r = Rng::make(idx, p.seed);
     const float r1 = r.f32();
     const float r2 = r.f32();
@@ -150,8 +156,9 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
                     if (p.zbuf && !(dd < p.zbuf[py * p.width + px])) {
                         ok = false;
                     } else {
-                        const float ct = dot(d, vdiv(to, dd));
-                        const float phase = phase_hg(p.g, ct);
+                        // g == 0: phase_hg is exactly 1/(4 pi) (pow(1, 1.5) == 1), so
+                        // the direction to the camera is not needed.
+                        const float phase = p.g == 0.0f ? kInv4Pi : phase_hg(p.g, dot(d, vdiv(to, dd)));
                         const float trans = expf(-p.sigma_t * dd);
                         contrib = power * p.sigma_s * phase * trans / (dd * dd) * seg / 4.0f;
                     }
@@ -160,7 +167,7 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
                 }
             }
             if (COUNT) { if (ok) ++cnt->splats; continue; }
-            deposit<SPEC, AGG>(p, ok, px, py, contrib, cx, cy, cz, bin);
+            deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, cx, cy, cz, bin);
         }
         if (!any) break;
         const sc_material& m = S.mats[mi];
@@ -177,31 +184,44 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
     if (DEBUG) rec->num_states = pairs < 9u ? pairs : 9u;
 }
 
-// Stage the scene records and the CMF table in shared memory.
-__device__ __forceinline__ SceneView load_scene(const PhotonParams& p, unsigned char* smem, const float** cmf_out) {
+// Stage the scene records and the CMF table in shared memory; when `mask_words`
+// is non-zero a zeroed dirty-tile bitmask of that many words follows them.
+__device__ __forceinline__ SceneView load_scene(const PhotonParams& p, unsigned char* smem, const float** cmf_out,
+                                                uint32_t** mask_out = nullptr, uint32_t mask_words = 0) {
     sc_primitive* sp = reinterpret_cast<sc_primitive*>(smem);
     sc_plane* spl = reinterpret_cast<sc_plane*>(sp + p.n_prims);
     sc_material* sm = reinterpret_cast<sc_material*>(spl + p.n_planes);
     float* scmf = reinterpret_cast<float*>(sm + p.n_mats);
+    uint32_t* mask = reinterpret_cast<uint32_t*>(scmf + 3 * kTableN);
     for (uint32_t i = threadIdx.x; i < p.n_prims; i += blockDim.x) sp[i] = p.prims[i];
     for (uint32_t i = threadIdx.x; i < p.n_planes; i += blockDim.x) spl[i] = p.planes[i];
     for (uint32_t i = threadIdx.x; i < p.n_mats; i += blockDim.x) sm[i] = p.mats[i];
     for (uint32_t i = threadIdx.x; i < 3u * kTableN; i += blockDim.x) scmf[i] = p.cmf[i];
+    for (uint32_t i = threadIdx.x; i < mask_words; i += blockDim.x) mask[i] = 0u;
     __syncthreads();
     *cmf_out = scmf;
+    if (mask_out) *mask_out = mask_words ? mask : nullptr;
     SceneView S;
     S.prims = sp; S.planes = spl; S.mats = sm; S.n_prims = p.n_prims;
     return S;
 }
 
-template <bool SPEC, int AGG>
-__global__ void __launch_bounds__(512) photon_kernel(const PhotonParams p) {
+// 256 threads per CTA; MINB CTAs per SM bound the registers (4: 63 registers,
+// no spills; 5: 48 registers, a few spills, more warps in flight).
+template <bool SPEC, int AGG, int MINB>
+__global__ void __launch_bounds__(256, MINB) photon_kernel(const PhotonParams p, uint32_t mask_words) {
     extern __shared__ __align__(16) unsigned char smem[];
     const float* cmf;
-    const SceneView S = load_scene(p, smem, &cmf);
+    uint32_t* smask;
+    const SceneView S = load_scene(p, smem, &cmf, &smask, mask_words);
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += stride)
-        trace_photon<SPEC, AGG, false>(p, S, cmf, p.photon_base + i);
+        trace_photon<SPEC, AGG, false>(p, S, cmf, p.photon_base + i, smask);
+    if (smask) {  // publish this CTA's dirty tiles
+        __syncthreads();
+        for (uint32_t w = threadIdx.x; w < mask_words; w += blockDim.x)
+            if (smask[w]) atomicOr(p.flags + w, smask[w]);
+    }
 }
 
 // Instrumented pass: same transport, no film writes; sums the per-photon work
@@ -213,7 +233,7 @@ __global__ void __launch_bounds__(256) photon_count_kernel(const PhotonParams p,
     unsigned long long seg = 0, spl = 0, sca = 0, ph = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += gridDim.x * blockDim.x) {
         PhotonCounts c = {0u, 0u, 0u};
-        trace_photon<false, 0, false, true>(p, S, cmf, p.photon_base + i, &c);
+        trace_photon<false, 0, false, true>(p, S, cmf, p.photon_base + i, nullptr, &c);
         seg += c.segments; spl += c.splats; sca += c.scatters; ++ph;
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -232,7 +252,7 @@ __global__ void __launch_bounds__(256) photon_debug_kernel(const PhotonParams p)
     const float* cmf;
     const SceneView S = load_scene(p, smem, &cmf);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < p.photon_count) trace_photon<false, 0, true>(p, S, cmf, i);
+    if (i < p.photon_count) trace_photon<false, 0, true>(p, S, cmf, i, nullptr);
 }
 
 // Surface rim pass (spectral-gpu/src/shaders/volume.wgsl:668-703 and its CPU
@@ -285,30 +305,39 @@ size_t scene_smem_bytes(uint32_t n_prims, uint32_t n_planes, uint32_t n_mats) {
            3 * kTableN * sizeof(float);
 }
 
-template <bool SPEC, int AGG>
-static const void* photon_fn() { return reinterpret_cast<const void*>(&photon_kernel<SPEC, AGG>); }
+using PhotonKernelFn = void (*)(const PhotonParams, uint32_t);
 
-int photon_occupancy_blocks(uint32_t block, bool spectral, int aggregate, size_t smem) {
-    const void* fn = spectral ? (aggregate ? photon_fn<true, 1>() : photon_fn<true, 0>())
-                              : (aggregate ? photon_fn<false, 1>() : photon_fn<false, 0>());
+static PhotonKernelFn photon_fn(bool spec, int agg, int minb) {
+    if (minb >= 5) {
+        if (spec) return agg ? photon_kernel<true, 1, 5> : photon_kernel<true, 0, 5>;
+        return agg ? photon_kernel<false, 1, 5> : photon_kernel<false, 0, 5>;
+    }
+    if (spec) return agg ? photon_kernel<true, 1, 4> : photon_kernel<true, 0, 4>;
+    return agg ? photon_kernel<false, 1, 4> : photon_kernel<false, 0, 4>;
+}
+
+int photon_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)block, smem) != cudaSuccess) return 1;
+    const void* fn = reinterpret_cast<const void*>(photon_fn(spectral, shape.aggregate, shape.minb));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)shape.block, smem) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
+}
+
+uint32_t photon_mask_words(const PhotonParams& p) {
+    if (!p.flags) return 0u;
+    const uint32_t tiles = p.tiles_x * ((p.height + 7u) / 8u);
+    const uint32_t words = (tiles + 31u) / 32u;
+    return words <= kMaxSmemMaskWords ? words : 0u;
 }
 
 cudaError_t launch_photons(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s) {
     if (p.photon_count == 0) return cudaSuccess;
-    const size_t smem = scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats);
+    const uint32_t mw = photon_mask_words(p);
+    const size_t smem = scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats) + mw * sizeof(uint32_t);
     const bool spec = p.channels != 3u || p.bins != 0u;
-    const uint32_t need = (p.photon_count + shape.block - 1) / shape.block;
+    const uint32_t need = (p.photon_count + 255u) / 256u;
     const uint32_t grid = need < shape.grid ? need : shape.grid;
-    if (spec) {
-        if (shape.aggregate) photon_kernel<true, 1><<<grid, shape.block, smem, s>>>(p);
-        else photon_kernel<true, 0><<<grid, shape.block, smem, s>>>(p);
-    } else {
-        if (shape.aggregate) photon_kernel<false, 1><<<grid, shape.block, smem, s>>>(p);
-        else photon_kernel<false, 0><<<grid, shape.block, smem, s>>>(p);
-    }
+    photon_fn(spec, shape.aggregate, shape.minb)<<<grid, 256, smem, s>>>(p, mw);
     return cudaGetLastError();
 }
 

@@ -1,0 +1,265 @@
+// Wavefront hero-wavelength camera path tracer.
+//
+// Restates CpuTracer::sample_pixel / accumulate (spectral-core/src/tracer.rs:44-141;
+// GPU mirror spectral-gpu/src/shaders/trace.wgsl:419-537) as a wavefront:
+//   generate  one path per (pixel, sample): stream key mix2(pixel, sample index),
+//             jittered primary ray, hero-comb wavelength draw (spectrum.rs:20-32);
+//   intersect nearest scene hit (+ the optional spherical emitter) per queued ray;
+//   shade     background / emission at termination, Fresnel / refract / TIR or
+//             Lambertian scatter, dispersion collapse to the hero lane, optional
+//             Russian roulette; survivors are compacted into the next queue with
+//             warp ballots, one atomic per block and shared-memory staging so the
+//             SoA writes are contiguous;
+//   accumulate each pixel's samples summed in sample order (the CPU's order), so
+//             the image is deterministic and, for scenes without Lambertian
+//             surfaces, bit-identical to the CPU tracer.
+// Queue counts stay on the device: the launch sequence of an accumulate call is
+// fixed, needs no host synchronisation and is replayed from a CUDA graph.
+#include "internal.h"
+#include "tracer.h"
+
+namespace sc {
+
+namespace {
+
+constexpr int kShadeThreads = 256;
+constexpr float kLambdaMin = 380.0f, kLambdaRange = 350.0f;
+
+struct TracerSmem {
+    TracerParams p;
+    float tables[5 * kTableN];
+    sc_primitive prims[SC_MAX_PRIMS];
+    sc_material mats[SC_MAX_PRIMS];
+};
+
+// Stage params, scene records and sensor tables in shared memory.  Planes live
+// after the fixed part (dynamic size).
+__device__ __forceinline__ SceneView load_tracer(const TracerParams* gp, TracerSmem& s, sc_plane* planes) {
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) s.p = *gp;
+    for (uint32_t i = tid; i < 5u * kTableN; i += blockDim.x) s.tables[i] = gp->tables[i];
+    __syncthreads();
+    for (uint32_t i = tid; i < s.p.n_prims; i += blockDim.x) s.prims[i] = s.p.prims[i];
+    for (uint32_t i = tid; i < s.p.n_mats; i += blockDim.x) s.mats[i] = s.p.mats[i];
+    for (uint32_t i = tid; i < s.p.n_planes; i += blockDim.x) planes[i] = s.p.planes[i];
+    __syncthreads();
+    SceneView S;
+    S.prims = s.prims; S.planes = planes; S.mats = s.mats; S.n_prims = s.p.n_prims;
+    return S;
+}
+
+__device__ __forceinline__ float lane_lambda(float u, int k) {
+    // SpectralSample::from_hero_u: (u*RANGE + k*RANGE/4).rem_euclid(RANGE)
+    float off = fmodf(u * kLambdaRange + (float)k * (kLambdaRange / 4.0f), kLambdaRange);
+    if (off < 0.0f) off += kLambdaRange;
+    return kLambdaMin + off;
+}
+
+// XYZ of a terminated comb whose lanes carry radiance rad_k = tp_k * e * S(lambda_k).
+__device__ __forceinline__ void comb_xyz(const TracerSmem& s, float u, float tp, uint32_t valid, float e,
+                                         float out[3]) {
+    const float pdf = 1.0f / kLambdaRange;
+    const float* ill = s.tables + (s.p.illuminant == 1u ? 4 : 3) * kTableN;
+    float x = 0.0f, y = 0.0f, z = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float lam = lane_lambda(u, k);
+        const float tk = (k == 0 || valid > 1u) ? tp : 0.0f;
+        const float rad = 0.0f + tk * e * tab_sample(ill, lam);
+        const float wk = rad / pdf / (float)valid;
+        x += tab_sample(s.tables, lam) * wk;
+        y += tab_sample(s.tables + kTableN, lam) * wk;
+        z += tab_sample(s.tables + 2 * kTableN, lam) * wk;
+    }
+    out[0] = x; out[1] = y; out[2] = z;
+}
+
+__global__ void __launch_bounds__(256) tr_generate(const TracerParams* __restrict__ gp, uint32_t first_pixel,
+                                                   uint32_t n_paths, uint32_t spp, const uint32_t* __restrict__ base,
+                                                   RayQueue q, uint32_t* counts, float* result) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        counts[0] = n_paths;
+        for (uint32_t b = 1; b <= gp->max_depth; ++b) counts[b] = 0u;
+    }
+    if (i >= n_paths) return;
+    const uint32_t W = gp->width, H = gp->height;
+    const uint32_t pixel = first_pixel + i / spp, s = i % spp;
+    const uint32_t px = pixel % W, py = pixel / W;
+    Rng r = Rng::make(mix2(pixel, *base + s), gp->seed);
+    const float fs = ((float)px + r.f32()) / (float)W;
+    const float ft = 1.0f - ((float)py + r.f32()) / (float)H;
+    const float u = r.f32();
+    const f3 d = primary_dir(gp->cam, fs, ft);
+    q.ox[i] = gp->cam.origin[0]; q.oy[i] = gp->cam.origin[1]; q.oz[i] = gp->cam.origin[2];
+    q.dx[i] = d.x; q.dy[i] = d.y; q.dz[i] = d.z;
+    q.rng[i] = r.state; q.tp[i] = 1.0f; q.u[i] = u; q.id[i] = i; q.flags[i] = 4u;
+    result[3 * i] = 0.0f; result[3 * i + 1] = 0.0f; result[3 * i + 2] = 0.0f;
+}
+
+__global__ void __launch_bounds__(256) tr_intersect(const TracerParams* __restrict__ gp, uint32_t bounce, RayQueue q,
+                                                    const uint32_t* __restrict__ counts, HitQueue hq) {
+    __shared__ TracerSmem s;
+    extern __shared__ __align__(16) unsigned char dyn[];
+    const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
+    const uint32_t n = counts[bounce];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const f3 o = mk(q.ox[i], q.oy[i], q.oz[i]), d = mk(q.dx[i], q.dy[i], q.dz[i]);
+        Hit h;
+        uint32_t mi = 0;
+        const bool any = scene_hit(S, o, d, h, mi);
+        uint32_t kind = any ? 1u : 0u;
+        float t = any ? h.t : __int_as_float(0x7f800000);
+        if (s.p.em_radius > 0.0f) {
+            sc_primitive em;
+            em.center[0] = s.p.em_center.x; em.center[1] = s.p.em_center.y; em.center[2] = s.p.em_center.z;
+            em.radius = s.p.em_radius;
+            Hit he;
+            if (sphere_hit(em, o, d, 1e-3f, t, he)) { kind = 2u; t = he.t; }
+        }
+        hq.t[i] = t;
+        if (kind == 1u) { hq.nx[i] = h.normal.x; hq.ny[i] = h.normal.y; hq.nz[i] = h.normal.z; }
+        hq.info[i] = mi | (((any && h.front_face) ? 1u : 0u) << 16) | (kind << 24);
+    }
+}
+
+__global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __restrict__ gp, uint32_t bounce,
+                                                          RayQueue q, HitQueue hq, RayQueue out, uint32_t* counts,
+                                                          float* result) {
+    __shared__ TracerSmem s;
+    __shared__ uint32_t warp_base[kShadeThreads / 32 + 1];
+    __shared__ uint32_t block_base;
+    __shared__ float st_f[8][kShadeThreads];      // staged survivors: ox oy oz dx dy dz tp u
+    __shared__ uint32_t st_u[3][kShadeThreads];   // rng id flags
+    extern __shared__ __align__(16) unsigned char dyn[];
+    const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
+    const uint32_t n = counts[bounce];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (uint32_t tile = blockIdx.x * blockDim.x; tile < n; tile += gridDim.x * blockDim.x) {
+        const uint32_t i = tile + threadIdx.x;
+        bool survive = false;
+        f3 o, d;
+        float tp = 0.0f, u = 0.0f;
+        uint32_t rs = 0, id = 0, flags = 0;
+        if (i < n) {
+            o = mk(q.ox[i], q.oy[i], q.oz[i]);
+            d = mk(q.dx[i], q.dy[i], q.dz[i]);
+            tp = q.tp[i]; u = q.u[i]; rs = q.rng[i]; id = q.id[i]; flags = q.flags[i];
+            const uint32_t info = hq.info[i];
+            const uint32_t kind = info >> 24;
+            uint32_t valid = flags & 0xFFu;
+            if (kind != 1u) {
+                float e;
+                if (kind == 0u) e = s.p.background + ((s.p.has_horizon && d.y > 0.0f) ? s.p.horizon : 0.0f);
+                else e = s.p.em_scale;
+                float xyz[3];
+                comb_xyz(s, u, tp, valid, e, xyz);
+                result[3 * id] = xyz[0]; result[3 * id + 1] = xyz[1]; result[3 * id + 2] = xyz[2];
+            } else {
+                const sc_material& m = S.mats[info & 0xFFFFu];
+                Hit h;
+                h.t = hq.t[i];
+                h.point = add(o, mul(d, h.t));
+                h.normal = mk(hq.nx[i], hq.ny[i], hq.nz[i]);
+                h.front_face = ((info >> 16) & 1u) != 0u;
+                const float nh = m.kind == 1u ? glass_n(m.glass, lane_lambda(u, 0)) : 1.0f;
+                Rng r;
+                r.state = rs;
+                f3 nd;
+                float w;
+                scatter(m, d, h, nh, r, nd, w);
+                tp *= w;
+                if (m.kind == 1u && valid > 1u) valid = 1u;
+                const uint32_t depth = bounce + 1u;
+                survive = depth < s.p.max_depth;
+                if (s.p.rr_start && depth >= s.p.rr_start) {
+                    const float qv = fminf(tp, 0.95f);
+                    if (!(r.f32() < qv)) survive = false;
+                    else tp = tp / qv;
+                }
+                o = h.point; d = nd; rs = r.state;
+                flags = valid | (depth << 8);
+            }
+        }
+        // block-level compaction: ballot per warp, prefix over warps, one atomic
+        const unsigned ball = __ballot_sync(0xffffffffu, survive);
+        const uint32_t rank = __popc(ball & ((1u << lane) - 1u));
+        if (lane == 0) warp_base[warp] = __popc(ball);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+            for (int w = 0; w < kShadeThreads / 32; ++w) { const uint32_t c = warp_base[w]; warp_base[w] = acc; acc += c; }
+            warp_base[kShadeThreads / 32] = acc;
+            block_base = acc ? atomicAdd(&counts[bounce + 1], acc) : 0u;
+        }
+        __syncthreads();
+        if (survive) {
+            const uint32_t j = warp_base[warp] + rank;
+            st_f[0][j] = o.x; st_f[1][j] = o.y; st_f[2][j] = o.z;
+            st_f[3][j] = d.x; st_f[4][j] = d.y; st_f[5][j] = d.z;
+            st_f[6][j] = tp; st_f[7][j] = u;
+            st_u[0][j] = rs; st_u[1][j] = id; st_u[2][j] = flags;
+        }
+        __syncthreads();
+        const uint32_t total = warp_base[kShadeThreads / 32];
+        if (threadIdx.x < total) {
+            const uint32_t j = threadIdx.x, g = block_base + j;
+            out.ox[g] = st_f[0][j]; out.oy[g] = st_f[1][j]; out.oz[g] = st_f[2][j];
+            out.dx[g] = st_f[3][j]; out.dy[g] = st_f[4][j]; out.dz[g] = st_f[5][j];
+            out.tp[g] = st_f[6][j]; out.u[g] = st_f[7][j];
+            out.rng[g] = st_u[0][j]; out.id[g] = st_u[1][j]; out.flags[g] = st_u[2][j];
+        }
+        __syncthreads();
+    }
+}
+
+// Per-pixel sample sum in sample order (tracer.rs:121-135), added to the running sum.
+__global__ void __launch_bounds__(256) tr_accumulate(uint32_t first_pixel, uint32_t n_pixels, uint32_t spp,
+                                                     const float* __restrict__ result, float* sum,
+                                                     const uint32_t* __restrict__ counts, uint32_t max_depth,
+                                                     unsigned long long* segments) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j == 0) {
+        unsigned long long t = 0;
+        for (uint32_t b = 0; b < max_depth; ++b) t += counts[b];
+        *segments += t;
+    }
+    if (j >= n_pixels) return;
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+    const float* r = result + (size_t)j * spp * 3u;
+    for (uint32_t s = 0; s < spp; ++s) { a0 += r[3 * s]; a1 += r[3 * s + 1]; a2 += r[3 * s + 2]; }
+    float* o = sum + 3u * (size_t)(first_pixel + j);
+    o[0] += a0; o[1] += a1; o[2] += a2;
+}
+
+}  // namespace
+
+size_t tracer_dyn_smem(uint32_t n_planes) { return (size_t)(n_planes ? n_planes : 1u) * sizeof(sc_plane); }
+
+int tracer_grid(int sms) {
+    int a = 0, b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, tr_intersect, 256, tracer_dyn_smem(SC_MAX_PLANES));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tr_shade, kShadeThreads, tracer_dyn_smem(SC_MAX_PLANES));
+    int k = a < b ? a : b;
+    return sms * (k > 0 ? k : 1);
+}
+
+cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch& L, uint32_t first_pixel,
+                               uint32_t n_pixels, cudaStream_t st) {
+    const uint32_t n_paths = n_pixels * L.spp;
+    tr_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(d_params, first_pixel, n_paths, L.spp, L.d_base, L.qa,
+                                                       L.counts, L.result);
+    const size_t dyn = tracer_dyn_smem(L.n_planes);
+    for (uint32_t b = 0; b < L.max_depth; ++b) {
+        const RayQueue& in = (b & 1u) ? L.qb : L.qa;
+        const RayQueue& out = (b & 1u) ? L.qa : L.qb;
+        uint32_t g = L.grid;
+        tr_intersect<<<g, 256, dyn, st>>>(d_params, b, in, L.counts, L.hits);
+        tr_shade<<<g, kShadeThreads, dyn, st>>>(d_params, b, in, L.hits, out, L.counts, L.result);
+    }
+    tr_accumulate<<<(n_pixels + 255) / 256, 256, 0, st>>>(first_pixel, n_pixels, L.spp, L.result, L.sum, L.counts,
+                                                           L.max_depth, L.segments);
+    return cudaGetLastError();
+}
+
+}  // namespace sc

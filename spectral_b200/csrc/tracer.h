@@ -1,0 +1,48 @@
+// Wavefront camera tracer: device structures shared by tracer.cu and the host
+// object in tracer_api.cu.
+#pragma once
+#include "internal.h"
+
+namespace sc {
+
+// Everything a wave needs, kept in device memory so a captured graph stays
+// valid when the camera or scene changes.
+struct TracerParams {
+    sc_camera cam;
+    uint32_t width, height, seed, illuminant;
+    float background, horizon;
+    uint32_t has_horizon, max_depth, rr_start;
+    f3 em_center;
+    float em_radius, em_scale;
+    const sc_primitive* prims; const sc_plane* planes; const sc_material* mats;
+    uint32_t n_prims, n_planes, n_mats;
+    const float* tables;  // device 5 x 71 sensor table
+};
+
+// Structure-of-arrays ray / path queue.
+struct RayQueue {
+    float *ox, *oy, *oz, *dx, *dy, *dz, *tp, *u;
+    uint32_t *rng, *id, *flags;  // flags: valid lanes (bits 0-7), depth (bits 8-15)
+};
+struct HitQueue {
+    float *t, *nx, *ny, *nz;
+    uint32_t* info;  // material | front_face << 16 | kind << 24 (0 miss, 1 surface, 2 emitter)
+};
+
+struct TracerLaunch {
+    RayQueue qa, qb;
+    HitQueue hits;
+    uint32_t* counts;       // max_depth + 1 queue lengths
+    float* result;          // 3 per path of the wave
+    float* sum;             // 3 * w * h running sum
+    const uint32_t* d_base; // sample index of the first sample of this accumulate
+    unsigned long long* segments;  // running count of traced segments
+    uint32_t spp, max_depth, n_planes, grid;
+};
+
+size_t tracer_dyn_smem(uint32_t n_planes);
+int tracer_grid(int sms);
+cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch& L, uint32_t first_pixel,
+                               uint32_t n_pixels, cudaStream_t st);
+
+}  // namespace sc

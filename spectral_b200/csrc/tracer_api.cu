@@ -1,0 +1,255 @@
+// extern "C" camera tracer object: GpuTracer (spectral-gpu/src/lib.rs:165-389)
+// over the wavefront kernels of tracer.cu.
+#include <algorithm>
+#include <vector>
+
+#include "host_util.h"
+#include "tracer.h"
+
+using namespace sc;
+
+namespace {
+constexpr uint32_t kWavePaths = 1u << 20;  // queues of one wave stay resident in L2
+}
+
+struct sc_tracer {
+    sc_ctx* ctx = nullptr;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    uint32_t w = 0, h = 0, samples = 0;
+    TracerParams hp{};
+    DevBuf<TracerParams> params;
+    DevBuf<float> tables;
+    DevBuf<sc_primitive> prims;
+    DevBuf<sc_plane> planes;
+    DevBuf<sc_material> mats;
+    DevBuf<float> sum, result, qbuf;
+    DevBuf<uint32_t> counts, base;
+    DevBuf<unsigned long long> segments;
+    DevBuf<uint32_t> qbuf_u;
+    uint32_t wave_cap = 0;  // paths per wave the queues are sized for
+    TracerLaunch L{};
+    cudaGraphExec_t graph = nullptr;
+    uint32_t graph_spp = 0;
+    uint64_t last_paths = 0, last_segments = 0;
+
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        graph_spp = 0;
+    }
+    int upload_params() {
+        SC_CUDA(cudaMemcpyAsync(params.p, &hp, sizeof hp, cudaMemcpyHostToDevice, stream));
+        return SC_OK;
+    }
+    int ensure_queues(uint32_t paths) {
+        if (paths <= wave_cap) return SC_OK;
+        drop_graph();
+        const size_t n = paths;
+        SC_CUDA(qbuf.alloc(n * 8 * 2 + n * 4 + 3 * n));    // 2 ray queues x 8 floats, hits 4 floats, result 3
+        SC_CUDA(qbuf_u.alloc(n * 3 * 2 + n));               // 2 ray queues x 3 u32, hit info
+        float* f = qbuf.p;
+        uint32_t* u = qbuf_u.p;
+        RayQueue* qs[2] = {&L.qa, &L.qb};
+        for (RayQueue* q : qs) {
+            q->ox = f; q->oy = f + n; q->oz = f + 2 * n; q->dx = f + 3 * n; q->dy = f + 4 * n; q->dz = f + 5 * n;
+            q->tp = f + 6 * n; q->u = f + 7 * n;
+            f += 8 * n;
+            q->rng = u; q->id = u + n; q->flags = u + 2 * n;
+            u += 3 * n;
+        }
+        L.hits.t = f; L.hits.nx = f + n; L.hits.ny = f + 2 * n; L.hits.nz = f + 3 * n;
+        f += 4 * n;
+        L.result = f;
+        L.hits.info = u;
+        wave_cap = paths;
+        return SC_OK;
+    }
+    int run(uint32_t spp) {
+        const uint32_t npx = w * h;
+        const uint32_t px_per_wave = std::max(1u, kWavePaths / spp);
+        int rc = ensure_queues(std::min(npx, px_per_wave) * spp);
+        if (rc != SC_OK) return rc;
+        L.spp = spp;
+        SC_CUDA(cudaMemcpyAsync(base.p, &samples, 4, cudaMemcpyHostToDevice, stream));
+        if (!graph || graph_spp != spp) {
+            drop_graph();
+            cudaGraph_t g = nullptr;
+            SC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = cudaSuccess;
+            for (uint32_t first = 0; first < npx && e == cudaSuccess; first += px_per_wave)
+                e = launch_tracer_wave(params.p, L, first, std::min(px_per_wave, npx - first), stream);
+            cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+            if (e == cudaSuccess) e = e2;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&graph, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                graph = nullptr;
+                set_error("tracer graph capture failed: %s", cudaGetErrorString(e));
+                return SC_E_CUDA;
+            }
+            graph_spp = spp;
+        }
+        SC_CUDA(cudaGraphLaunch(graph, stream));
+        samples += spp;
+        last_paths = (uint64_t)npx * spp;
+        return SC_OK;
+    }
+};
+
+extern "C" {
+
+int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, const sc_plane* planes,
+                     uint32_t n_planes, const sc_material* mats, uint32_t n_mats, float background, int has_horizon,
+                     float horizon, const sc_camera* cam, uint32_t width, uint32_t height, uint32_t illuminant,
+                     uint32_t seed, const sc_tracer_options* opts, sc_tracer** out) {
+    SC_GUARD_BEGIN
+    SC_REQUIRE(ctx && cam && out, SC_E_INVALID, "null argument");
+    *out = nullptr;
+    SC_REQUIRE(n_prims <= SC_MAX_PRIMS && n_planes <= SC_MAX_PLANES && n_mats <= SC_MAX_PRIMS, SC_E_LIMIT,
+               "scene exceeds %d primitives / %d planes", SC_MAX_PRIMS, SC_MAX_PLANES);
+    SC_REQUIRE((n_prims == 0 || prims) && (n_planes == 0 || planes) && (n_mats == 0 || mats), SC_E_INVALID,
+               "null scene array");
+    for (uint32_t i = 0; i < n_prims; ++i) {
+        SC_REQUIRE(prims[i].kind <= 1u && prims[i].material < n_mats, SC_E_INVALID, "primitive %u invalid", i);
+        if (prims[i].kind == 1u)
+            SC_REQUIRE((uint64_t)prims[i].plane_start + prims[i].plane_count <= n_planes, SC_E_INVALID,
+                       "primitive %u plane range", i);
+    }
+    for (uint32_t i = 0; i < n_mats; ++i)
+        SC_REQUIRE(mats[i].kind <= 1u && (mats[i].kind == 0u || mats[i].glass <= 3u), SC_E_INVALID, "material %u", i);
+    SC_REQUIRE(width > 0 && height > 0 && (uint64_t)width * height <= (1ull << 26), SC_E_INVALID, "image %ux%u",
+               width, height);
+    SC_REQUIRE(illuminant <= 1u, SC_E_INVALID, "illuminant %u (0 D65, 1 A)", illuminant);
+    sc_tracer_options o{};
+    if (opts) o = *opts;
+    if (o.max_depth == 0) o.max_depth = 8;
+    SC_REQUIRE(o.max_depth <= 64, SC_E_LIMIT, "max_depth %u > 64", o.max_depth);
+    sc_tracer* t = new sc_tracer();
+    t->ctx = ctx; t->w = width; t->h = height;
+    DeviceGuard g(ctx->device);
+    auto fail = [&](cudaError_t e) {
+        set_error("tracer setup failed: %s", cudaGetErrorString(e));
+        if (t->stream) cudaStreamDestroy(t->stream);
+        delete t;
+        return e == cudaErrorMemoryAllocation ? SC_E_NOMEM : SC_E_CUDA;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(e);
+    if ((e = t->params.alloc(1)) != cudaSuccess) return fail(e);
+    if ((e = t->tables.alloc(5 * kTableN)) != cudaSuccess) return fail(e);
+    if ((e = t->prims.alloc(std::max(1u, n_prims))) != cudaSuccess) return fail(e);
+    if ((e = t->planes.alloc(std::max(1u, n_planes))) != cudaSuccess) return fail(e);
+    if ((e = t->mats.alloc(std::max(1u, n_mats))) != cudaSuccess) return fail(e);
+    if ((e = t->sum.alloc(3ull * width * height)) != cudaSuccess) return fail(e);
+    if ((e = t->counts.alloc(o.max_depth + 1)) != cudaSuccess) return fail(e);
+    if ((e = t->base.alloc(1)) != cudaSuccess) return fail(e);
+    if ((e = t->segments.alloc(1)) != cudaSuccess) return fail(e);
+    cudaMemcpy(t->tables.p, ctx->tables, 5 * kTableN * sizeof(float), cudaMemcpyHostToDevice);
+    if (n_prims) cudaMemcpy(t->prims.p, prims, n_prims * sizeof(sc_primitive), cudaMemcpyHostToDevice);
+    if (n_planes) cudaMemcpy(t->planes.p, planes, n_planes * sizeof(sc_plane), cudaMemcpyHostToDevice);
+    if (n_mats) cudaMemcpy(t->mats.p, mats, n_mats * sizeof(sc_material), cudaMemcpyHostToDevice);
+    cudaMemset(t->sum.p, 0, t->sum.bytes());
+    cudaMemset(t->segments.p, 0, 8);
+    TracerParams& hp = t->hp;
+    hp.cam = *cam; hp.width = width; hp.height = height; hp.seed = seed; hp.illuminant = illuminant;
+    hp.background = background; hp.horizon = horizon; hp.has_horizon = has_horizon ? 1u : 0u;
+    hp.max_depth = o.max_depth; hp.rr_start = o.rr_start;
+    hp.em_center = ld3(o.emitter_center); hp.em_radius = o.emitter_radius; hp.em_scale = o.emitter_scale;
+    hp.prims = t->prims.p; hp.planes = t->planes.p; hp.mats = t->mats.p;
+    hp.n_prims = n_prims; hp.n_planes = n_planes; hp.n_mats = n_mats;
+    hp.tables = t->tables.p;
+    TracerLaunch& L = t->L;
+    L.counts = t->counts.p; L.sum = t->sum.p; L.d_base = t->base.p; L.segments = t->segments.p;
+    L.max_depth = o.max_depth; L.n_planes = n_planes; L.grid = (uint32_t)tracer_grid(ctx->sms);
+    if ((e = cudaMemcpy(t->params.p, &hp, sizeof hp, cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e);
+    *out = t;
+    return SC_OK;
+    SC_GUARD_END
+}
+
+int sc_tracer_destroy(sc_tracer* t) {
+    SC_GUARD_BEGIN
+    if (!t) return SC_OK;
+    {
+        DeviceGuard g(t->ctx->device);
+        if (t->stream) cudaStreamSynchronize(t->stream);
+        t->drop_graph();
+        t->params.reset(); t->tables.reset(); t->prims.reset(); t->planes.reset(); t->mats.reset();
+        t->sum.reset(); t->result.reset(); t->qbuf.reset(); t->qbuf_u.reset(); t->counts.reset(); t->base.reset();
+        t->segments.reset();
+        if (t->stream) cudaStreamDestroy(t->stream);
+    }
+    delete t;
+    return SC_OK;
+    SC_GUARD_END
+}
+
+#define TR_LOCK(t)                                           \
+    SC_REQUIRE((t), SC_E_INVALID, "null tracer");            \
+    std::lock_guard<std::mutex> _lk((t)->mu);                \
+    DeviceGuard _dg((t)->ctx->device)
+
+int sc_tracer_accumulate(sc_tracer* t, uint32_t spp) {
+    SC_GUARD_BEGIN
+    TR_LOCK(t);
+    if (spp == 0) return SC_OK;
+    SC_REQUIRE(spp <= (1u << 16), SC_E_INVALID, "spp %u > 65536", spp);
+    return t->run(spp);
+    SC_GUARD_END
+}
+
+int sc_tracer_read_xyz(sc_tracer* t, float* out) {
+    SC_GUARD_BEGIN
+    TR_LOCK(t);
+    SC_REQUIRE(out, SC_E_INVALID, "null output");
+    SC_CUDA(cudaMemcpyAsync(out, t->sum.p, t->sum.bytes(), cudaMemcpyDeviceToHost, t->stream));
+    SC_CUDA(cudaStreamSynchronize(t->stream));
+    // AccumBuffer::mean (spectral-core/src/lib.rs:16-20): sum / max(samples, 1)
+    const float n = (float)std::max(t->samples, 1u);
+    for (size_t i = 0; i < 3ull * t->w * t->h; ++i) out[i] = out[i] / n;
+    return SC_OK;
+    SC_GUARD_END
+}
+
+int sc_tracer_set_camera(sc_tracer* t, const sc_camera* cam) {
+    SC_GUARD_BEGIN
+    TR_LOCK(t);
+    SC_REQUIRE(cam, SC_E_INVALID, "null camera");
+    t->hp.cam = *cam;
+    return t->upload_params();
+    SC_GUARD_END
+}
+
+int sc_tracer_clear_accum(sc_tracer* t) {
+    SC_GUARD_BEGIN
+    TR_LOCK(t);
+    SC_CUDA(cudaMemsetAsync(t->sum.p, 0, t->sum.bytes(), t->stream));
+    t->samples = 0;
+    return SC_OK;
+    SC_GUARD_END
+}
+
+int sc_tracer_dims(sc_tracer* t, uint32_t* w, uint32_t* h) {
+    SC_GUARD_BEGIN
+    SC_REQUIRE(t, SC_E_INVALID, "null tracer");
+    if (w) *w = t->w;
+    if (h) *h = t->h;
+    return SC_OK;
+    SC_GUARD_END
+}
+
+int sc_tracer_last_stats(sc_tracer* t, uint64_t* paths, uint64_t* segments) {
+    SC_GUARD_BEGIN
+    TR_LOCK(t);
+    unsigned long long s = 0;
+    SC_CUDA(cudaMemcpyAsync(&s, t->segments.p, 8, cudaMemcpyDeviceToHost, t->stream));
+    SC_CUDA(cudaStreamSynchronize(t->stream));
+    if (paths) *paths = t->last_paths;
+    if (segments) *segments = s;
+    return SC_OK;
+    SC_GUARD_END
+}
+
+}  // extern "C"

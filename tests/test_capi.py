@@ -79,7 +79,7 @@ def test_tir_beam_dir_is_normalized_f32():
 
 def test_film_sizes():
     assert _lib.lib.sc_film_bytes(640, 360, 64) == 80 * 45 * 64 * 64 * 8
-    assert _lib.lib.sc_film_flag_bytes(641, 361) == 81 * 46 * 4
+    assert _lib.lib.sc_film_flag_bytes(641, 361) == (81 * 46 + 31) // 32 * 4
 
 
 def test_null_arguments_fail_with_status():
