@@ -68,6 +68,9 @@ typedef struct {
     uint32_t estimator;     /* 0 point estimator (volume.rs:99-168), 1 legacy isotropic (volume.rs:22-85) */
 } sc_film_options;
 
+typedef struct sc_batch sc_batch;
+typedef struct sc_server sc_server;
+
 /* ---- errors / context (spectral-gpu/src/lib.rs:21-41 GpuContext::new) ---- */
 const char* sc_last_error(void);
 const char* sc_version(void);
@@ -148,6 +151,13 @@ int sc_photon_film_dims(sc_photon_film* f, uint32_t* width, uint32_t* height, ui
 int sc_photon_film_set_scene(sc_photon_film* f, const sc_primitive* prims, uint32_t n_prims,
                              const sc_plane* planes, uint32_t n_planes, const sc_material* mats,
                              uint32_t n_mats, const sc_camera* cam, const sc_beam* beam);
+/* Device buffers of the film (tile-major int64 cells and the dirty-tile mask),
+ * for collectives over several GPUs: films of disjoint photon ranges add up
+ * exactly.  Valid until the film is destroyed. */
+int sc_photon_film_device_buffers(sc_photon_film* f, void** film_dev, size_t* film_bytes, void** flags_dev,
+                                  size_t* flag_bytes, void** stream);
+/* Mark every tile as lit (after another process added its film into this one). */
+int sc_photon_film_mark_all_dirty(sc_photon_film* f);
 /* Work counters of photons [photon_base, photon_base+count) without touching
  * the film: out[0..3] = photons, path segments, in-frame haze samples (film
  * splats), surface scatters. */
@@ -232,6 +242,92 @@ int sc_sensor_reduce_device(sc_ctx* ctx, uint32_t width, uint32_t height, uint32
                             float lambda_min, float lambda_max, uint32_t scale_log2,
                             void* film_dev, uint32_t* flags_dev, float* xyz_dev, int drain,
                             void* stream);
+
+/* ---- batched uneven workload (no counterpart in the reference) ----------
+ * Many independent scenes with different photon budgets, film sizes and bins
+ * traced by ONE persistent launch (warps steal photon chunks, largest scene
+ * first), then one persistent drain + sensor reduction over every film; the
+ * pair is captured in a CUDA graph and replayed.  Photon i of a scene is keyed
+ * by its index inside that scene, so each film is bit-identical to the film of
+ * a plain per-scene launch. */
+#define SC_BATCH_MAX_PRIMS 4
+#define SC_BATCH_MAX_PLANES 16
+typedef struct {
+    uint32_t n_prims, n_planes, n_mats, spectral;   /* spectral: 1 n(lambda), 0 n(550 nm) */
+    sc_primitive prims[SC_BATCH_MAX_PRIMS];
+    sc_plane planes[SC_BATCH_MAX_PLANES];
+    sc_material mats[SC_BATCH_MAX_PRIMS];
+    sc_camera cam;
+    sc_beam beam;
+    sc_vol_weights weights;
+    uint32_t width, height, n_photons, seed;
+    float max_dist;
+    sc_film_options opts;                           /* bins must be >= 1 */
+} sc_scene_job;
+/* Tuning knobs, 0 = default: photons per work chunk (queue granularity),
+ * register bound (minimum CTAs per SM, 4 or 5), warp-aggregated splats, grid. */
+typedef struct { uint32_t chunk_photons, minb, aggregate, grid; } sc_batch_tuning;
+int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs,
+                    const sc_batch_tuning* tuning, sc_batch** out);
+int sc_batch_destroy(sc_batch* b);
+/* Time every candidate tuning on this batch and keep the fastest. */
+int sc_batch_autotune(sc_batch* b, sc_batch_tuning* chosen);
+int sc_batch_set_tuning(sc_batch* b, const sc_batch_tuning* tuning);
+int sc_batch_get_tuning(sc_batch* b, sc_batch_tuning* tuning);
+/* New cameras / beams / seeds / weights for the same films and budgets. */
+int sc_batch_update_jobs(sc_batch* b, const sc_scene_job* jobs, uint32_t n_jobs);
+/* One pass over every job (graph replay); stream NULL = the batch's stream.
+ * Asynchronous; afterwards each job's XYZ image is ready and its film drained. */
+int sc_batch_run(sc_batch* b, void* stream);
+/* The same work as plain per-scene launches (trace + drain/reduce per job). */
+int sc_batch_run_plain(sc_batch* b, void* stream);
+int sc_batch_synchronize(sc_batch* b);
+int sc_batch_read_xyz(sc_batch* b, uint32_t job, float* out);
+/* All jobs' XYZ images concatenated in job order (sum of 3*w*h floats). */
+int sc_batch_read_all_xyz(sc_batch* b, float* out, size_t capacity, void* stream);
+/* job_table_bytes: bytes uploaded host -> device by sc_batch_update_jobs. */
+int sc_batch_info(sc_batch* b, uint64_t* total_photons, uint64_t* film_bytes, uint64_t* xyz_floats,
+                  uint64_t* job_table_bytes);
+/* Work of one pass, measured by an instrumented pass (not timed work):
+ * out[0..5] = photons, path segments, in-frame haze samples, scatters, film
+ * tiles that received light, bytes of those tiles. */
+int sc_batch_stats(sc_batch* b, uint64_t out[6]);
+int sc_batch_device_xyz(sc_batch* b, uint32_t job, const float** xyz_dev);
+
+/* ---- serving loop: continuous batching (no counterpart in the reference) -
+ * Requests are admitted against a device-memory budget (one arena allocated
+ * at creation), and each sc_server_step traces the current frame of every
+ * admitted request in one persistent launch.  A request's photons are keyed by
+ * its own photon index, so its image is the same alone or in any mix. */
+typedef struct {
+    uint64_t hbm_budget_bytes;  /* arena for films, masks and images of admitted requests */
+    uint32_t max_slots;         /* requests on the device at once (0 -> 256) */
+    uint32_t chunk_photons;     /* work-chunk size of the batched launch (0 -> 2048) */
+} sc_server_config;
+typedef struct {
+    sc_scene_job job;           /* scene, film (bins >= 1), photons per frame (n_photons), seed, camera */
+    uint32_t frames;            /* 1: a single render; F > 1: an orbit session of F frames */
+    float orbit_deg;            /* camera azimuth step per frame around orbit_target (about +y) */
+    float orbit_target[3];
+    float orbit_up[3];
+    float vfov_deg;             /* camera of frame f rebuilt with Camera::look_at */
+} sc_request;
+int sc_server_create(sc_ctx* ctx, const sc_server_config* cfg, sc_server** out);
+int sc_server_destroy(sc_server* s);
+/* Queue a request; SC_E_NOMEM when it could never fit the budget. */
+int sc_server_submit(sc_server* s, const sc_request* r, uint64_t* id);
+/* Admit what fits, trace one frame of every admitted request (one launch),
+ * retire finished requests.  Blocks until the step's work is done. */
+int sc_server_step(sc_server* s, uint32_t* active);
+/* Pop a finished request: its last frame's XYZ image (3*w*h floats) and the
+ * steady-clock times [submit, admit, first frame done, done] in seconds.
+ * SC_E_STATE when nothing is finished. */
+int sc_server_poll(sc_server* s, uint64_t* id, float* xyz_out, size_t capacity, uint32_t* width,
+                   uint32_t* height, double times[4]);
+/* Drop a queued or active request (between steps nothing of it is in flight). */
+int sc_server_cancel(sc_server* s, uint64_t id);
+int sc_server_stats(sc_server* s, uint64_t* photons_traced, uint64_t* bytes_in_use, uint32_t* queued,
+                    uint32_t* active, uint32_t* finished);
 
 #ifdef __cplusplus
 }

@@ -72,6 +72,27 @@ class sc_trace_desc(C.Structure):
                 ("zbuffer", C.c_void_p)]
 
 
+class sc_scene_job(C.Structure):
+    _fields_ = [("n_prims", C.c_uint32), ("n_planes", C.c_uint32), ("n_mats", C.c_uint32), ("spectral", C.c_uint32),
+                ("prims", sc_primitive * 4), ("planes", sc_plane * 16), ("mats", sc_material * 4),
+                ("cam", sc_camera), ("beam", sc_beam), ("weights", sc_vol_weights), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("n_photons", C.c_uint32), ("seed", C.c_uint32), ("max_dist", C.c_float),
+                ("opts", sc_film_options)]
+
+
+class sc_batch_tuning(C.Structure):
+    _fields_ = [("chunk_photons", C.c_uint32), ("minb", C.c_uint32), ("aggregate", C.c_uint32), ("grid", C.c_uint32)]
+
+
+class sc_server_config(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_slots", C.c_uint32), ("chunk_photons", C.c_uint32)]
+
+
+class sc_request(C.Structure):
+    _fields_ = [("job", sc_scene_job), ("frames", C.c_uint32), ("orbit_deg", C.c_float), ("orbit_target", F3),
+                ("orbit_up", F3), ("vfov_deg", C.c_float)]
+
+
 assert C.sizeof(sc_primitive) == 32 and C.sizeof(sc_material) == 16 and C.sizeof(sc_plane) == 16
 assert C.sizeof(sc_debug_photon) == 304
 
@@ -114,6 +135,8 @@ PROTOTYPES = {
     "sc_photon_film_set_scene": (_i32, [_vp, P(sc_primitive), _u32, P(sc_plane), _u32, P(sc_material), _u32,
                                         P(sc_camera), P(sc_beam)]),
     "sc_photon_film_trace_stats": (_i32, [_vp, _u32, _u32, _u32, P(_u64)]),
+    "sc_photon_film_device_buffers": (_i32, [_vp, P(_vp), P(_sz), P(_vp), P(_sz), P(_vp)]),
+    "sc_photon_film_mark_all_dirty": (_i32, [_vp]),
     "sc_trace_stats_device": (_i32, [_vp, P(sc_trace_desc), _u32, _u32, _vp, _vp]),
     "sc_tracer_create": (_i32, [_vp, P(sc_primitive), _u32, P(sc_plane), _u32, P(sc_material), _u32, _f32, _i32,
                                 _f32, P(sc_camera), _u32, _u32, _u32, _u32, P(sc_tracer_options), P(_vp)]),
@@ -133,6 +156,27 @@ PROTOTYPES = {
     "sc_atomic_film_clear_film": (_i32, [_vp]),
     "sc_atomic_film_clear_accum": (_i32, [_vp]),
     "sc_atomic_film_check_determinism": (_i32, [_vp, _u32, _u32, _u32, _u32, P(_i64)]),
+    "sc_batch_create": (_i32, [_vp, P(sc_scene_job), _u32, P(sc_batch_tuning), P(_vp)]),
+    "sc_batch_destroy": (_i32, [_vp]),
+    "sc_batch_autotune": (_i32, [_vp, P(sc_batch_tuning)]),
+    "sc_batch_set_tuning": (_i32, [_vp, P(sc_batch_tuning)]),
+    "sc_batch_get_tuning": (_i32, [_vp, P(sc_batch_tuning)]),
+    "sc_batch_update_jobs": (_i32, [_vp, P(sc_scene_job), _u32]),
+    "sc_batch_run": (_i32, [_vp, _vp]),
+    "sc_batch_run_plain": (_i32, [_vp, _vp]),
+    "sc_batch_synchronize": (_i32, [_vp]),
+    "sc_batch_read_xyz": (_i32, [_vp, _u32, P(_f32)]),
+    "sc_batch_read_all_xyz": (_i32, [_vp, P(_f32), _sz, _vp]),
+    "sc_batch_info": (_i32, [_vp, P(_u64), P(_u64), P(_u64), P(_u64)]),
+    "sc_batch_device_xyz": (_i32, [_vp, _u32, P(P(_f32))]),
+    "sc_batch_stats": (_i32, [_vp, P(_u64)]),
+    "sc_server_create": (_i32, [_vp, P(sc_server_config), P(_vp)]),
+    "sc_server_destroy": (_i32, [_vp]),
+    "sc_server_submit": (_i32, [_vp, P(sc_request), P(_u64)]),
+    "sc_server_step": (_i32, [_vp, P(_u32)]),
+    "sc_server_poll": (_i32, [_vp, P(_u64), P(_f32), _sz, P(_u32), P(_u32), P(C.c_double)]),
+    "sc_server_cancel": (_i32, [_vp, _u64]),
+    "sc_server_stats": (_i32, [_vp, P(_u64), P(_u64), P(_u32), P(_u32), P(_u32)]),
     "sc_film_bytes": (_sz, [_u32, _u32, _u32]),
     "sc_film_flag_bytes": (_sz, [_u32, _u32]),
     "sc_trace_photons_device": (_i32, [_vp, P(sc_trace_desc), _u32, _u32, _vp, _vp, _vp]),

@@ -626,6 +626,28 @@ int sc_photon_film_set_scene(sc_photon_film* f, const sc_primitive* prims, uint3
     SC_GUARD_END
 }
 
+int sc_photon_film_device_buffers(sc_photon_film* f, void** film_dev, size_t* film_bytes, void** flags_dev,
+                                  size_t* flag_bytes, void** stream) {
+    SC_GUARD_BEGIN
+    SC_REQUIRE(f, SC_E_INVALID, "null photon film");
+    if (film_dev) *film_dev = f->film.p;
+    if (film_bytes) *film_bytes = f->film.bytes();
+    if (flags_dev) *flags_dev = f->flags.p;
+    if (flag_bytes) *flag_bytes = f->flags.bytes();
+    if (stream) *stream = f->stream;
+    return SC_OK;
+    SC_GUARD_END
+}
+
+int sc_photon_film_mark_all_dirty(sc_photon_film* f) {
+    SC_GUARD_BEGIN
+    FILM_LOCK(f);
+    SC_CUDA(cudaMemsetAsync(f->flags.p, 0xFF, f->flags.bytes(), f->stream));
+    ++f->film_version;
+    return SC_OK;
+    SC_GUARD_END
+}
+
 int sc_photon_film_trace_stats(sc_photon_film* f, uint32_t base, uint32_t count, uint32_t seed, uint64_t out[4]) {
     SC_GUARD_BEGIN
     FILM_LOCK(f);

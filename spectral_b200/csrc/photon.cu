@@ -11,178 +11,11 @@
 // Splats land in a 64-bit fixed-point film with red.global.add.u64; the film is
 // tile-major (8x8 pixel tiles) and every touched tile raises a dirty flag so the
 // drain/reduce pass reads only tiles that received light.
-#include "internal.h"
+#include "photon_trace.cuh"
 
 namespace sc {
 
 namespace {
-
-constexpr float kInv4Pi = 1.0f / (4.0f * 3.14159265358979323846f);
-
-__device__ __forceinline__ void red_u64(unsigned long long* a, unsigned long long v) {
-    if (v) atomicAdd(a, v);
-}
-
-// Exact segmented sum of 64-bit values over the lanes of `peers` using three
-// 26-bit chunks (no chunk sum can overflow 32 bits for <= 32 lanes).
-__device__ __forceinline__ unsigned long long peer_sum64(unsigned peers, unsigned long long v) {
-    unsigned c0 = (unsigned)(v & 0x3FFFFFFull);
-    unsigned c1 = (unsigned)((v >> 26) & 0x3FFFFFFull);
-    unsigned c2 = (unsigned)(v >> 52);
-    unsigned s0 = __reduce_add_sync(peers, c0);
-    unsigned s1 = __reduce_add_sync(peers, c1);
-    unsigned s2 = __reduce_add_sync(peers, c2);
-    return (unsigned long long)s0 + ((unsigned long long)s1 << 26) + ((unsigned long long)s2 << 52);
-}
-
-// Dirty-tile bitmask: bits go to this CTA's shared-memory copy (flushed to the
-// global mask when the CTA finishes) or, for films whose mask does not fit,
-// straight to the global mask with a fire-and-forget red.or.
-__device__ __forceinline__ void mark_tile(const PhotonParams& p, uint32_t* smask, uint32_t tile) {
-    if (!p.flags) return;
-    const uint32_t w = tile >> 5, bit = 1u << (tile & 31u);
-    if (smask) {
-        if (!(smask[w] & bit)) atomicOr(smask + w, bit);
-    } else {
-        atomicOr(p.flags + w, bit);
-    }
-}
-
-// Deposit one haze sample.  AGG=1 merges lanes of the warp that hit the same
-// film cell before issuing the atomic.
-template <bool SPEC, int AGG>
-__device__ __forceinline__ void deposit(const PhotonParams& p, uint32_t* smask, bool ok, uint32_t px, uint32_t py,
-                                        float contrib, float cx, float cy, float cz, uint32_t bin) {
-    size_t cell = 0;
-    uint32_t tile = 0;
-    unsigned long long v0 = 0, v1 = 0, v2 = 0;
-    if (ok) {
-        tile = film_tile(px, py, p.tiles_x);
-        cell = film_cell(px, py, p.tiles_x, p.channels) + (SPEC ? bin : 0u);
-        if (SPEC) {
-            v0 = to_fixed(contrib, p.scale);
-        } else {
-            v0 = to_fixed(cx * contrib, p.scale);
-            v1 = to_fixed(cy * contrib, p.scale);
-            v2 = to_fixed(cz * contrib, p.scale);
-        }
-    }
-    if (AGG == 0) {
-        if (!ok) return;
-        mark_tile(p, smask, tile);
-        red_u64(p.film + cell, v0);
-        if (!SPEC) { red_u64(p.film + cell + 1, v1); red_u64(p.film + cell + 2, v2); }
-        return;
-    }
-    const unsigned mask = __activemask();
-    const uint32_t key = ok ? (uint32_t)cell : 0xFFFFFFFFu;
-    const unsigned peers = __match_any_sync(mask, key);
-    if (!ok) return;
-    const unsigned lane = threadIdx.x & 31u;
-    if (peers != (1u << lane)) {
-        v0 = peer_sum64(peers, v0);
-        if (!SPEC) { v1 = peer_sum64(peers, v1); v2 = peer_sum64(peers, v2); }
-        if ((int)lane != __ffs(peers) - 1) return;
-    }
-    mark_tile(p, smask, tile);
-    red_u64(p.film + cell, v0);
-    if (!SPEC) { red_u64(p.film + cell + 1, v1); red_u64(p.film + cell + 2, v2); }
-}
-
-__device__ __forceinline__ void record_pair(sc_debug_photon* rec, uint32_t pair, f3 o, f3 d) {
-    if (pair >= 9u) return;
-    float* q = rec->states[2 * pair];
-    q[0] = o.x; q[1] = o.y; q[2] = o.z; q[3] = 0.0f;
-    q = rec->states[2 * pair + 1];
-    q[0] = d.x; q[1] = d.y; q[2] = d.z; q[3] = 0.0f;
-}
-
-// Work counters of one photon (instrumented launches only): segments traced,
-// haze samples that land in frame (= film splats), dielectric/diffuse scatters.
-struct PhotonCounts { uint32_t segments, splats, scatters; };
-
-template <bool SPEC, int AGG, bool DEBUG, bool COUNT = false>
-__device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneView& S, const float* cmf,
-                                             uint32_t idx, uint32_t* smask, PhotonCounts* cnt = nullptr) {
-    Rng r = Rng::make(idx, p.seed);
-    const float r1 = r.f32();
-    const float r2 = r.f32();
-    f3 o = add(add(p.corner, mul(p.bu, r1)), mul(p.bv, r2));
-    const float lambda = p.lambda_min + p.lambda_range * r.f32();
-    float cx = 0.f, cy = 0.f, cz = 0.f;
-    uint32_t bin = 0;
-    if (!DEBUG) {
-        if (SPEC) {
-            float fb = (lambda - p.bin_min) * p.bin_inv_width;
-            int bi = (int)fb;
-            bin = fb < 0.0f ? 0u : (bi >= (int)p.bins ? p.bins - 1u : (uint32_t)bi);
-        } else {
-            cx = tab_sample(cmf, lambda);
-            cy = tab_sample(cmf + kTableN, lambda);
-            cz = tab_sample(cmf + 2 * kTableN, lambda);
-        }
-    }
-    f3 d = p.bdir;
-    float power = 1.0f;
-    sc_debug_photon* rec = nullptr;
-    uint32_t pairs = 1;
-    if (DEBUG) {
-        rec = p.debug + idx;
-        rec->lambda = lambda;
-        rec->pad0 = rec->pad1 = 0u;
-        record_pair(rec, 0, o, d);
-    }
-    for (uint32_t b = 0; b < p.max_bounces; ++b) {
-        Hit h;
-        uint32_t mi = 0;
-        const bool any = scene_hit(S, o, d, h, mi);
-        const float seg = any ? h.t : p.max_dist;
-        if (COUNT) ++cnt->segments;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const float dist = r.f32() * seg;
-            if (DEBUG) continue;
-            const f3 q = add(o, mul(d, dist));
-            float s, t;
-            bool ok = project(p.proj, q, s, t);
-            uint32_t px = 0, py = 0;
-            float contrib = 0.0f;
-            if (ok) {
-                px = min((uint32_t)(s * (float)p.width), p.width - 1u);
-                py = min((uint32_t)((1.0f - t) * (float)p.height), p.height - 1u);
-                if (p.estimator == 0u) {
-                    const f3 to = sub(p.proj.o, q);
-                    const float dd = fmaxf(length(to), 1e-3f);
-                    if (p.zbuf && !(dd < p.zbuf[py * p.width + px])) {
-                        ok = false;
-                    } else {
-                        // g == 0: phase_hg is exactly 1/(4 pi) (pow(1, 1.5) == 1), so
-                        // the direction to the camera is not needed.
-                        const float phase = p.g == 0.0f ? kInv4Pi : phase_hg(p.g, dot(d, vdiv(to, dd)));
-                        const float trans = expf(-p.sigma_t * dd);
-                        contrib = power * p.sigma_s * phase * trans / (dd * dd) * seg / 4.0f;
-                    }
-                } else {
-                    contrib = power * p.sigma_s * seg / 4.0f * kInv4Pi;
-                }
-            }
-            if (COUNT) { if (ok) ++cnt->splats; continue; }
-            deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, cx, cy, cz, bin);
-        }
-        if (!any) break;
-        const sc_material& m = S.mats[mi];
-        const float nh = m.kind == 1u ? glass_n(m.glass, p.spectral ? lambda : 550.0f) : 1.0f;
-        f3 nd;
-        float w;
-        if (COUNT) ++cnt->scatters;
-        scatter(m, d, h, nh, r, nd, w);
-        power *= w;
-        o = h.point;
-        d = nd;
-        if (DEBUG) { record_pair(rec, pairs, o, d); ++pairs; }
-    }
-    if (DEBUG) rec->num_states = pairs < 9u ? pairs : 9u;
-}
 
 // Stage the scene records and the CMF table in shared memory; when `mask_words`
 // is non-zero a zeroed dirty-tile bitmask of that many words follows them.

@@ -1,0 +1,169 @@
+"""Serving loop: continuous batching of render requests (sc_server_* ABI).
+
+``Server`` wraps the C object; ``poisson_requests`` draws a seeded request
+stream (Poisson arrivals; prism scenes; photons per frame log-uniform; a share
+of progressive orbit sessions); ``run_stream`` replays a stream in real time
+and returns latency percentiles and throughput.
+"""
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+from .batch import prism_job
+from .scenes import Pcg
+
+ORBIT_TARGET = (0.6, -0.4, 0.0)
+
+
+class Server:
+    def __init__(self, ctx, budget_bytes=40 << 30, max_slots=256, chunk_photons=2048):
+        self.h = C.c_void_p()
+        cfg = _lib.sc_server_config(int(budget_bytes), int(max_slots), int(chunk_photons))
+        check(lib.sc_server_create(ctx.h, C.byref(cfg), C.byref(self.h)))
+        self._dims = {}
+
+    def submit(self, job, frames=1, orbit_deg=0.0, target=ORBIT_TARGET, up=(0.0, 1.0, 0.0), vfov=42.0):
+        r = _lib.sc_request()
+        r.job, r.frames, r.orbit_deg = job, int(frames), float(orbit_deg)
+        r.orbit_target, r.orbit_up, r.vfov_deg = _lib.F3(*target), _lib.F3(*up), float(vfov)
+        rid = C.c_uint64()
+        check(lib.sc_server_submit(self.h, C.byref(r), C.byref(rid)))
+        self._dims[rid.value] = 3 * job.width * job.height
+        return rid.value
+
+    def step(self):
+        a = C.c_uint32()
+        check(lib.sc_server_step(self.h, C.byref(a)))
+        return a.value
+
+    def poll(self, want_image=True):
+        """(id, xyz or None, (t_submit, t_admit, t_first_frame, t_done)) or None."""
+        rid, w, h = C.c_uint64(), C.c_uint32(), C.c_uint32()
+        times = (C.c_double * 4)()
+        # the largest possible image of any request still outstanding
+        cap = max(self._dims.values()) if (want_image and self._dims) else 0
+        buf = np.empty(cap, np.float32) if cap else None
+        rc = lib.sc_server_poll(self.h, C.byref(rid), buf.ctypes.data_as(C.POINTER(C.c_float)) if cap else None,
+                                cap, C.byref(w), C.byref(h), times)
+        if rc == _lib.SC_E_STATE:
+            return None
+        check(rc)
+        n = self._dims.pop(rid.value, 0)
+        return rid.value, (buf[:n].copy() if cap else None), tuple(times)
+
+    def cancel(self, rid):
+        check(lib.sc_server_cancel(self.h, int(rid)))
+        self._dims.pop(rid, None)
+
+    def stats(self):
+        p, b = C.c_uint64(), C.c_uint64()
+        q, a, f = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib.sc_server_stats(self.h, C.byref(p), C.byref(b), C.byref(q), C.byref(a), C.byref(f)))
+        return dict(photons=p.value, bytes_in_use=b.value, queued=q.value, active=a.value, finished=f.value)
+
+    def close(self):
+        if self.h:
+            lib.sc_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def poisson_requests(rate=200.0, seconds=60.0, seed=0x5E7E, session_share=0.3, frames=(16, 128),
+                     photons=(2 ** 16, 2 ** 20), side=(128, 1024), bins=32, orbit_deg=2.0):
+    """Seeded request stream: list of (arrival_s, job, frames, orbit_deg)."""
+    g = Pcg(0, seed)
+    out, t, i = [], 0.0, 0
+    while True:
+        t += -math.log(1.0 - g.f()) / rate
+        if t >= seconds:
+            break
+        r = Pcg(i, seed ^ 0x9E3779B9)
+        glass = (0, 1, 3)[r.u32() % 3]
+        apex, inc = r.uniform(30.0, 75.0), r.uniform(30.0, 60.0)
+        n = int(round(r.log_uniform(*photons)))
+        s = int(round(r.log_uniform(*side)))
+        sig = r.uniform(0.01, 0.1)
+        sess = r.f() < session_share
+        nf = (frames[0] + r.u32() % (frames[1] - frames[0] + 1)) if sess else 1
+        job = prism_job(glass, apex, inc, n, s, s, sig, sig, 0.0, (seed * 2654435761 + i) & 0xFFFFFFFF, bins,
+                        380.0, 780.0)
+        out.append((t, job, nf, orbit_deg if sess else 0.0))
+        i += 1
+    return out
+
+
+def run_stream(server, stream, time_scale=1.0, idle_sleep=2e-4):
+    """Replay `stream` in real time against `server`; returns a metrics dict."""
+    t0 = time.perf_counter()
+    k, done, lat, ttff = 0, 0, [], []
+    pending = {}
+    steps, photons0 = 0, server.stats()["photons"]
+    while done < len(stream):
+        now = time.perf_counter() - t0
+        while k < len(stream) and stream[k][0] * time_scale <= now:
+            _, job, nf, orbit = stream[k]
+            rid = server.submit(job, nf, orbit)
+            pending[rid] = nf
+            k += 1
+        st = server.stats()
+        if st["queued"] or st["active"]:
+            server.step()
+            steps += 1
+        elif k < len(stream):
+            time.sleep(min(idle_sleep, max(0.0, stream[k][0] * time_scale - now)))
+        while True:
+            r = server.poll(want_image=False)
+            if r is None:
+                break
+            rid, _, (ts, ta, tf, td) = r
+            lat.append(td - ts)
+            ttff.append(tf - ts)
+            pending.pop(rid, None)
+            done += 1
+    wall = time.perf_counter() - t0
+    photons = server.stats()["photons"] - photons0
+    lat, ttff = np.array(lat), np.array(ttff)
+    return dict(requests=len(stream), wall_s=wall, steps=steps, photons=photons, photons_per_s=photons / wall,
+                p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
+                p50_first_frame_ms=float(np.percentile(ttff, 50) * 1e3),
+                p99_first_frame_ms=float(np.percentile(ttff, 99) * 1e3))
+
+
+def main():
+    """Replay the seeded request stream (Poisson arrivals) with continuous
+    batching and with one request at a time; print one JSON line."""
+    import argparse
+    import json
+    from . import GpuContext
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--seconds", type=float, default=60.0)
+    ap.add_argument("--budget-gb", type=float, default=40.0)
+    ap.add_argument("--seed", type=int, default=0x5E7E)
+    ap.add_argument("--skip-serial", action="store_true")
+    a = ap.parse_args()
+    ctx = GpuContext(0)
+    stream = poisson_requests(a.rate, a.seconds, a.seed)
+    out = {"requests": len(stream), "rate_per_s": a.rate, "seconds": a.seconds, "budget_gb": a.budget_gb,
+           "sessions": sum(1 for s in stream if s[2] > 1), "frames": sum(s[2] for s in stream)}
+    srv = Server(ctx, budget_bytes=int(a.budget_gb * (1 << 30)))
+    out["continuous_batching"] = run_stream(srv, stream)
+    srv.close()
+    if not a.skip_serial:
+        srv = Server(ctx, budget_bytes=int(a.budget_gb * (1 << 30)), max_slots=1)
+        out["one_request_at_a_time"] = run_stream(srv, stream)
+        srv.close()
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

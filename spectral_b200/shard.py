@@ -1,0 +1,66 @@
+"""Multi-GPU sharding of one scene's photons (one process per GPU).
+
+Photon i is keyed by its global index (its RNG stream is PathRng(i, seed)), so
+a scene's photons split into contiguous index ranges, one per rank, with no
+communication while tracing.  Each rank's 64-bit fixed-point film then holds
+the exact sum of its photons' splats, and ONE all-reduce (sum) of the int64
+films over NCCL (NVLink / NVSwitch) gives the film of the whole range,
+bit-identical to a single-GPU trace and independent of the number of ranks or
+the reduction order.  Batches and serving shard by whole scenes / requests and
+need no collective at all.
+"""
+import ctypes as C
+
+from ._lib import check, lib
+
+
+def photon_range(rank, world, n_photons, base=0):
+    """Contiguous [begin, end) of photon indices owned by `rank`."""
+    if not (0 <= rank < world):
+        raise ValueError("rank %d outside world %d" % (rank, world))
+    begin = base + (n_photons * rank) // world
+    end = base + (n_photons * (rank + 1)) // world
+    return begin, end
+
+
+class _CudaArray:
+    """__cuda_array_interface__ view of a device buffer (no copy)."""
+
+    def __init__(self, ptr, nbytes, typestr, itemsize, stream):
+        self.__cuda_array_interface__ = {"shape": (nbytes // itemsize,), "typestr": typestr,
+                                         "data": (ptr, False), "version": 3, "strides": None,
+                                         "stream": stream or 1}
+
+
+def film_tensor(film):
+    """int64 torch tensor aliasing a GpuPhotonFilm's device film (tile-major cells)."""
+    import torch
+    fp, fb, gp, gb, st = C.c_void_p(), C.c_size_t(), C.c_void_p(), C.c_size_t(), C.c_void_p()
+    check(lib.sc_photon_film_device_buffers(film.h, C.byref(fp), C.byref(fb), C.byref(gp), C.byref(gb),
+                                            C.byref(st)))
+    return torch.as_tensor(_CudaArray(fp.value, fb.value, "<i8", 8, st.value), device="cuda")
+
+
+def allreduce_film_(tensor, group=None):
+    """Sum an int64 film tensor over every rank in place (exact; any backend)."""
+    import torch.distributed as dist
+    if tensor.dtype.is_floating_point:
+        raise TypeError("films are int64 fixed point; a float all-reduce would not be exact")
+    dist.all_reduce(tensor, op=dist.ReduceOp.SUM, group=group)
+    return tensor
+
+
+def trace_sharded(film, n_photons, seed, group=None):
+    """Trace this rank's share of photons [0, n_photons) into `film`, then sum the
+    films of all ranks into every rank's film (NCCL all-reduce on int64)."""
+    import torch
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    b, e = photon_range(rank, world, n_photons)
+    film.dispatch_photons(b, e, seed)
+    t = film_tensor(film)
+    check(lib.sc_ctx_synchronize(film.ctx.h))
+    allreduce_film_(t, group)
+    torch.cuda.synchronize()
+    check(lib.sc_photon_film_mark_all_dirty(film.h))
+    return film

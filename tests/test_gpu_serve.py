@@ -1,0 +1,118 @@
+"""Serving loop (continuous batching): a request's image is the same alone and
+in any mix of concurrent requests (bit-identical: its photons are keyed by its
+own index), single renders and orbit frames match the CPU oracle, admission
+respects the device-memory budget, and a real-time Poisson stream completes."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+import spectral_b200 as sb
+from spectral_b200 import _lib
+from spectral_b200.batch import prism_job
+from spectral_b200.serve import ORBIT_TARGET, Server, poisson_requests, run_stream
+
+from helpers import rel_l1
+
+pytestmark = pytest.mark.gpu
+
+
+def job(i, n=20_000, side=48, bins=16):
+    return prism_job((0, 1, 3)[i % 3], 40.0 + 7 * i, 35.0 + 3 * i, n + 1000 * i, side + 8 * (i % 3),
+                     side + 8 * (i % 3), 0.03 + 0.01 * i, 0.03 + 0.01 * i, 0.0, 1000 + i, bins, 380.0, 780.0)
+
+
+def drain(server):
+    out = {}
+    for _ in range(10_000):
+        st = server.stats()
+        if not (st["queued"] or st["active"]):
+            break
+        server.step()
+    while True:
+        r = server.poll()
+        if r is None:
+            return out
+        out[r[0]] = r[1]
+
+
+def oracle_image(j, photon_begin, photon_end, cam=None):
+    sc = oracle.OScene(bytes(j.prims)[:32 * j.n_prims], j.n_prims, bytes(j.planes)[:16 * j.n_planes], j.n_planes,
+                       bytes(j.mats)[:16 * j.n_mats], j.n_mats, 0.0)
+    oc = oracle.or_camera.from_buffer_copy(bytes(cam if cam is not None else j.cam))
+    ob = oracle.or_beam.from_buffer_copy(bytes(j.beam))
+    o = j.opts
+    p = oracle.vol_params(j.width, j.height, j.seed, j.weights.sigma_s, j.weights.sigma_t, j.weights.g, j.max_dist,
+                          o.max_bounces, o.lambda_min, o.lambda_max, bins=o.bins)
+    _, _, fs = oracle.render_point(sc, oc, ob, p, photon_begin, photon_end, f32=False, xyz=False, spec=True)
+    w = oracle.bin_weights(o.bins, o.lambda_min, o.lambda_max).astype(np.float64)
+    return (fs.reshape(-1, o.bins).astype(np.float64) @ w.T).reshape(-1) * 2.0 ** -32
+
+
+def orbit_camera(j, frame, deg):
+    a = deg * frame * math.pi / 180.0
+    ox, oy, oz = j.cam.origin
+    tx, ty, tz = ORBIT_TARGET
+    # f32 differences, rotation in double, rounded to f32 (as the server does)
+    dx, dz = float(np.float32(ox) - np.float32(tx)), float(np.float32(oz) - np.float32(tz))
+    o = (float(np.float32(float(np.float32(tx)) + dx * math.cos(a) + dz * math.sin(a))), float(oy),
+         float(np.float32(float(np.float32(tz)) - dx * math.sin(a) + dz * math.cos(a))))
+    return sb.Camera.look_at(o, ORBIT_TARGET, (0, 1, 0), 42.0, float(np.float32(j.width) / np.float32(j.height))).c
+
+
+def test_same_alone_and_in_the_mix(ctx):
+    jobs = [job(i) for i in range(6)]
+    alone = {}
+    for i, j in enumerate(jobs):
+        s = Server(ctx, budget_bytes=1 << 30)
+        rid = s.submit(j, frames=3 if i % 2 else 1, orbit_deg=2.0 if i % 2 else 0.0)
+        alone[i] = drain(s)[rid]
+        s.close()
+    s = Server(ctx, budget_bytes=1 << 30)
+    ids = {}
+    for i, j in enumerate(jobs):
+        ids[s.submit(j, frames=3 if i % 2 else 1, orbit_deg=2.0 if i % 2 else 0.0)] = i
+        if i == 2:
+            s.step()  # later arrivals join while earlier ones are on the device
+    mixed = drain(s)
+    assert len(mixed) == len(jobs)
+    for rid, img in mixed.items():
+        assert img.tobytes() == alone[ids[rid]].tobytes(), ids[rid]
+    # single renders match the CPU oracle; orbit sessions return their last frame
+    for i, j in enumerate(jobs):
+        if i % 2 == 0:
+            exp = oracle_image(j, 0, j.n_photons)
+        else:
+            exp = oracle_image(j, 2 * j.n_photons, 3 * j.n_photons, orbit_camera(j, 2, 2.0))
+        assert exp.sum() > 0 and rel_l1(alone[i], exp) < 1e-6, i
+
+
+def test_budget_admission_and_cancel(ctx):
+    small = job(0, side=64, bins=32)
+    per = 64 // 8 * (64 // 8) * 64 * 32 * 8  # film bytes of one request
+    s = Server(ctx, budget_bytes=int(per * 2.5), max_slots=8)
+    big = job(1, side=512, bins=64)
+    with pytest.raises(_lib.SpectralError) as e:
+        s.submit(big)
+    assert e.value.code == _lib.SC_E_NOMEM
+    ids = [s.submit(small, frames=2) for _ in range(4)]
+    s.step()
+    st = s.stats()
+    assert st["active"] == 2 and st["queued"] == 2 and st["bytes_in_use"] <= int(per * 2.5)
+    s.cancel(ids[3])
+    s.cancel(ids[0])
+    got = drain(s)
+    assert sorted(got) == sorted(ids[1:3]) and s.stats()["bytes_in_use"] == 0
+    with pytest.raises(_lib.SpectralError):
+        s.cancel(12345)
+
+
+def test_realtime_stream_completes(ctx):
+    stream = poisson_requests(rate=60.0, seconds=1.0, seed=7, frames=(2, 6), photons=(2 ** 12, 2 ** 15),
+                              side=(32, 128), bins=16)
+    s = Server(ctx, budget_bytes=2 << 30)
+    m = run_stream(s, stream)
+    assert m["requests"] == len(stream) > 10
+    assert 0 < m["p50_ms"] <= m["p99_ms"] and m["photons"] > 0
+    assert s.stats()["bytes_in_use"] == 0

@@ -1,0 +1,78 @@
+"""Multi-process path on CPU (gloo, world size 2): photon-range sharding plus the
+exact int64 film all-reduce reproduce the single-process film bit for bit.
+The per-rank films come from the CPU oracle standing in for each rank's GPU."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from spectral_b200.shard import allreduce_film_, photon_range
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _scene():
+    import oracle
+    from helpers import obeam, ocam, oscene
+    import spectral_b200 as sb
+    scene, beam, cam = sb.dsotm_scene(1.0)
+    return oscene(scene), obeam(beam), ocam(cam), oracle.vol_params(48, 40, 9, 0.5, 0.06, 0.5, 14.0, bins=16)
+
+
+def _worker(rank, world, port, n, out_path):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    import oracle
+    osc, ob, oc, p = _scene()
+    b, e = photon_range(rank, world, n)
+    _, _, fs = oracle.render_point(osc, oc, ob, p, b, e, f32=False, xyz=False, spec=True)
+    t = torch.from_numpy(fs)
+    allreduce_film_(t)
+    if rank == 0:
+        np.save(out_path, t.numpy())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_photon_range_partitions():
+    for world in (1, 2, 3, 8):
+        for n in (0, 1, 7, 1000, 2 ** 20 + 3):
+            ranges = [photon_range(r, world, n, base=5) for r in range(world)]
+            assert ranges[0][0] == 5 and ranges[-1][1] == 5 + n
+            assert all(ranges[i][1] == ranges[i + 1][0] for i in range(world - 1))
+    with pytest.raises(ValueError):
+        photon_range(2, 2, 10)
+
+
+def test_two_rank_film_reduce_is_exact(tmp_path):
+    n = 6000
+    out = str(tmp_path / "film.npy")
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, n, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    import oracle
+    osc, ob, oc, p = _scene()
+    _, _, whole = oracle.render_point(osc, oc, ob, p, 0, n, f32=False, xyz=False, spec=True)
+    assert (np.load(out) == whole).all() and whole.sum() > 0
+
+
+def test_float_films_are_refused():
+    with pytest.raises(TypeError):
+        allreduce_film_(torch.zeros(4, dtype=torch.float32))
