@@ -243,6 +243,28 @@ int sc_sensor_reduce_device(sc_ctx* ctx, uint32_t width, uint32_t height, uint32
                             void* film_dev, uint32_t* flags_dev, float* xyz_dev, int drain,
                             void* stream);
 
+/* ---- allocation-free render (no counterpart in the reference) ----------
+ * For callers that cannot allocate device memory: hosts whose framework owns
+ * all device memory through its own pool (a raw cudaMalloc would bypass it and
+ * cudaFree synchronises the whole device) and render loops that must never
+ * block on an allocation.  Traces photons [photon_base, photon_base+count) of
+ * the scene in `desc` (scene records in device memory, as for
+ * sc_trace_photons_device) and writes the f32 XYZ image (3*w*h floats) to the
+ * caller's device buffer `xyz_dev` on `stream`.  It calls no cudaMalloc /
+ * cudaFree: its scratch (64-bit film, tile mask, sensor table, bin weights)
+ * lives in static device arrays that every GPU loading this library holds
+ * until the process exits.  Limit: (width padded to 8) * (height padded to 8)
+ * * channels <= SC_NOALLOC_MAX_FILM_CELLS (16 MiB of int64 cells; e.g.
+ * 640x360 XYZ, or 256x256 with 32 bins); larger films return SC_E_LIMIT.
+ * The first call on a device looks up the arrays' device addresses (once per
+ * device); make that first call before any stream capture.  Every call
+ * clears the scratch it reads, but all calls share it: calls that overlap on
+ * the GPU (other streams, other threads) race and must be serialised. */
+#define SC_NOALLOC_MAX_FILM_CELLS (1u << 21)
+#define SC_NOALLOC_MAX_MASK_WORDS 4096u
+int sc_trace_xyz_noalloc(const float* tables_5x71, const sc_trace_desc* desc, uint32_t photon_base,
+                         uint32_t count, float* xyz_dev, void* stream);
+
 /* ---- batched uneven workload (no counterpart in the reference) ----------
  * Many independent scenes with different photon budgets, film sizes and bins
  * traced by ONE persistent launch (warps steal photon chunks, largest scene

@@ -177,6 +177,7 @@ PROTOTYPES = {
     "sc_server_poll": (_i32, [_vp, P(_u64), P(_f32), _sz, P(_u32), P(_u32), P(C.c_double)]),
     "sc_server_cancel": (_i32, [_vp, _u64]),
     "sc_server_stats": (_i32, [_vp, P(_u64), P(_u64), P(_u32), P(_u32), P(_u32)]),
+    "sc_trace_xyz_noalloc": (_i32, [P(_f32), P(sc_trace_desc), _u32, _u32, _vp, _vp]),
     "sc_film_bytes": (_sz, [_u32, _u32, _u32]),
     "sc_film_flag_bytes": (_sz, [_u32, _u32]),
     "sc_trace_photons_device": (_i32, [_vp, P(sc_trace_desc), _u32, _u32, _vp, _vp, _vp]),
