@@ -214,6 +214,26 @@ int sc_atomic_film_clear_accum(sc_atomic_film* f);
 int sc_atomic_film_check_determinism(sc_ctx* ctx, uint32_t width, uint32_t height, uint32_t seed,
                                      uint32_t n_splats, int64_t* first_diff);
 
+/* ---- screen caustics and z-buffer (spectral-core/src/lighttrace.rs) ----- */
+/* Screen rectangle corner + s*u + r*v, s and r in [0,1) (lighttrace.rs:27-34). */
+typedef struct { float corner[3], u[3], v[3]; } sc_screen;
+/* lighttrace::trace (lighttrace.rs:157-166): photons [0, n_photons) from the
+ * beam, wavelengths uniform over [lambda_min, lambda_max) (opts; NULL = the
+ * visible band, 8 bounces), bilinear XYZ deposit into Screen::sum.  out_sum:
+ * 3*width*height floats, row 0 at the top (r = 1). */
+int sc_lighttrace(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, const sc_plane* planes,
+                  uint32_t n_planes, const sc_material* mats, uint32_t n_mats, const sc_screen* screen,
+                  uint32_t width, uint32_t height, const sc_beam* beam, uint32_t n_photons, uint32_t seed,
+                  const sc_film_options* opts, float* out_sum);
+/* Z-buffer of spectral-core/examples/prism_on_plane.rs:125-160: per pixel the
+ * ray distance of the nearer of the scene hit and the floor rectangle hit
+ * (floor may be NULL) along the primary ray through the pixel centre, +INF
+ * where nothing is hit.  out: width*height floats, the zbuffer input of
+ * sc_photon_film_create. */
+int sc_scene_zbuffer(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, const sc_plane* planes,
+                     uint32_t n_planes, const sc_material* mats, uint32_t n_mats, const sc_screen* floor,
+                     const sc_camera* cam, uint32_t width, uint32_t height, float* out);
+
 /* ---- device-pointer entry points (zero-copy; caller owns device memory) -- */
 /* One plain launch of the forward photon + haze kernel over photons
  * [photon_base, photon_base+count) into a device film the caller allocated
@@ -287,8 +307,11 @@ typedef struct {
     sc_film_options opts;                           /* bins must be >= 1 */
 } sc_scene_job;
 /* Tuning knobs, 0 = default: photons per work chunk (queue granularity),
- * register bound (minimum CTAs per SM, 4 or 5), warp-aggregated splats, grid. */
-typedef struct { uint32_t chunk_photons, minb, aggregate, grid; } sc_batch_tuning;
+ * register bound (minimum CTAs per SM, 4 or 5), warp-aggregated splats, grid,
+ * and per_photon = 1 to run each photon's haze samples in its own lane instead
+ * of the default warp-split transport (segments buffered per warp, samples
+ * processed as one converged list). */
+typedef struct { uint32_t chunk_photons, minb, aggregate, grid, per_photon; } sc_batch_tuning;
 int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs,
                     const sc_batch_tuning* tuning, sc_batch** out);
 int sc_batch_destroy(sc_batch* b);

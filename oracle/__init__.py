@@ -109,6 +109,7 @@ for name, res, args in [
     ("or_simulate_photon_fixed", _u32, [P(or_scene), P(or_beam), P(or_vol_params), _u32, _f32, _u32, P(_f32)]),
     ("or_mean_landing", _u32, [P(or_scene), P(_f32), P(or_beam), _f32, _u32, _u32, P(_f32)]),
     ("or_surface_rim", None, [P(or_scene), P(or_camera), _u32, _u32, P(_f32)]),
+    ("or_scene_zbuffer", None, [P(or_scene), P(_f32), P(or_camera), _u32, _u32, P(_f32)]),
     ("or_synthetic_splat", None, [_u32, _u32, _u32, _u32, P(_u32)]),
     ("or_gather_tonemap", None, [P(_f32), P(_f32), _u32, _u32, _f32, _f32, _f32, P(C.c_uint8)]),
 ]:

@@ -639,6 +639,34 @@ void or_lighttrace(const or_scene* sc, const float scr[9], uint32_t W, uint32_t 
     }
 }
 
+/* Z-buffer pass of examples/prism_on_plane.rs:125-160: t of the nearer of the
+ * scene hit and the floor Screen hit (screen_coords, lighttrace.rs:42-62). */
+void or_scene_zbuffer(const or_scene* sc, const float* floor9, const or_camera* cam, uint32_t W, uint32_t H,
+                      float* out) {
+    v3 fc = {0, 0, 0}, fu = fc, fv = fc, fn = fc;
+    if (floor9) { fc = L(floor9); fu = L(floor9 + 3); fv = L(floor9 + 6); fn = normalize(cross(fu, fv)); }
+    for (uint32_t py = 0; py < H; ++py)
+        for (uint32_t px = 0; px < W; ++px) {
+            float s = ((float)px + 0.5f) / (float)W;
+            float t = 1.0f - ((float)py + 0.5f) / (float)H;
+            v3 o = L(cam->origin), d = primary_dir(cam, s, t);
+            hit_t h; uint32_t mi;
+            float t_scene = scene_hit(sc, o, d, &h, &mi) ? h.t : INFINITY, t_floor = INFINITY;
+            if (floor9) {
+                float denom = dot(d, fn);
+                if (!(fabsf(denom) < 1e-8f)) {
+                    float tt = dot(sub(fc, o), fn) / denom;
+                    if (!(tt <= 1e-4f)) {
+                        v3 rel = sub(add(o, mul(d, tt)), fc);
+                        float ss = dot(rel, fu) / dot(fu, fu), rr = dot(rel, fv) / dot(fv, fv);
+                        if (ss >= 0.0f && ss < 1.0f && rr >= 0.0f && rr < 1.0f) t_floor = tt;
+                    }
+                }
+            }
+            out[(size_t)py * W + px] = t_scene < t_floor ? t_scene : t_floor;
+        }
+}
+
 /* ------------------------------------------------------------------------ */
 /* tracer.rs:44-111, spectrum.rs:20-32, scene.rs:44-50                      */
 /* ------------------------------------------------------------------------ */

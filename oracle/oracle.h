@@ -145,6 +145,9 @@ uint32_t or_mean_landing(const or_scene* sc, const float screen_cuv[9], const or
 
 /* Surface rim pass (vol_photons.rs:1517-1538). out: 3*w*h. */
 void or_surface_rim(const or_scene* sc, const or_camera* cam, uint32_t w, uint32_t h, float* out);
+/* prism_on_plane.rs:125-160 z-buffer; floor9 (corner,u,v) may be NULL. */
+void or_scene_zbuffer(const or_scene* sc, const float* floor9, const or_camera* cam, uint32_t w, uint32_t h,
+                      float* out);
 
 /* Synthetic atomic-film splat (spectral-gpu/src/shaders/vol_splat.wgsl:58-79), u32 film. */
 void or_synthetic_splat(uint32_t w, uint32_t h, uint32_t seed, uint32_t n_splats, uint32_t* film);

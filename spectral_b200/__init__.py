@@ -431,3 +431,44 @@ def check_determinism(ctx, width, height, seed, n_splats):
     check(lib.sc_atomic_film_check_determinism(ctx.h, int(width), int(height), int(seed), int(n_splats),
                                                C.byref(d)))
     return None if d.value < 0 else d.value
+
+
+class Screen:
+    """lighttrace::Screen (spectral-core/src/lighttrace.rs:14-112): a receiving
+    rectangle corner + s*u + r*v of width x height texels whose ``sum`` holds
+    the deposited XYZ (row 0 at r = 1), filled on the GPU by ``trace``."""
+
+    def __init__(self, corner, u, v, width, height):
+        self.corner, self.u, self.v = tuple(map(float, corner)), tuple(map(float, u)), tuple(map(float, v))
+        self.width, self.height = int(width), int(height)
+        self.sum = np.zeros((self.width * self.height, 3), np.float32)
+
+    def c(self):
+        return _lib.sc_screen(_f3(self.corner), _f3(self.u), _f3(self.v))
+
+    def scaled(self, scale):
+        return self.sum * np.float32(scale)
+
+
+def trace(ctx, scene, screen, beam, n, seed, lambda_min=380.0, lambda_max=730.0, max_bounces=8, scale_log2=32):
+    """lighttrace::trace (lighttrace.rs:157-166): photons 0..n from the beam,
+    splatted bilinearly into ``screen.sum`` (accumulated, like the reference)."""
+    prims, np_, planes, npl, mats, nm = scene.arrays()
+    opts = _lib.sc_film_options(0, float(lambda_min), float(lambda_max), int(max_bounces), int(scale_log2), 0)
+    out = np.zeros(3 * screen.width * screen.height, np.float32)
+    check(lib.sc_lighttrace(ctx.h, prims, np_, planes, npl, mats, nm, C.byref(screen.c()), screen.width,
+                            screen.height, C.byref(beam.c), int(n), int(seed), C.byref(opts), _fptr(out)))
+    screen.sum += out.reshape(-1, 3)
+    return screen
+
+
+def scene_zbuffer(ctx, scene, camera, width, height, floor=None):
+    """The z-buffer pass of spectral-core/examples/prism_on_plane.rs:125-160:
+    per pixel the distance to the nearer of the scene and the ``floor`` Screen
+    along the primary ray, +INF where nothing is hit (width*height floats)."""
+    prims, np_, planes, npl, mats, nm = scene.arrays()
+    out = np.zeros(int(width) * int(height), np.float32)
+    check(lib.sc_scene_zbuffer(ctx.h, prims, np_, planes, npl, mats, nm,
+                               C.byref(floor.c()) if floor is not None else None, C.byref(camera.c), int(width),
+                               int(height), _fptr(out)))
+    return out

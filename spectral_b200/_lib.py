@@ -45,6 +45,10 @@ class sc_camera(C.Structure):
     _fields_ = [("origin", F3), ("lower_left", F3), ("horizontal", F3), ("vertical", F3)]
 
 
+class sc_screen(C.Structure):
+    _fields_ = [("corner", F3), ("u", F3), ("v", F3)]
+
+
 class sc_vol_weights(C.Structure):
     _fields_ = [("sigma_s", C.c_float), ("sigma_t", C.c_float), ("g", C.c_float)]
 
@@ -81,7 +85,8 @@ class sc_scene_job(C.Structure):
 
 
 class sc_batch_tuning(C.Structure):
-    _fields_ = [("chunk_photons", C.c_uint32), ("minb", C.c_uint32), ("aggregate", C.c_uint32), ("grid", C.c_uint32)]
+    _fields_ = [("chunk_photons", C.c_uint32), ("minb", C.c_uint32), ("aggregate", C.c_uint32), ("grid", C.c_uint32),
+                ("per_photon", C.c_uint32)]
 
 
 class sc_server_config(C.Structure):
@@ -156,6 +161,10 @@ PROTOTYPES = {
     "sc_atomic_film_clear_film": (_i32, [_vp]),
     "sc_atomic_film_clear_accum": (_i32, [_vp]),
     "sc_atomic_film_check_determinism": (_i32, [_vp, _u32, _u32, _u32, _u32, P(_i64)]),
+    "sc_lighttrace": (_i32, [_vp, P(sc_primitive), _u32, P(sc_plane), _u32, P(sc_material), _u32, P(sc_screen),
+                             _u32, _u32, P(sc_beam), _u32, _u32, P(sc_film_options), P(_f32)]),
+    "sc_scene_zbuffer": (_i32, [_vp, P(sc_primitive), _u32, P(sc_plane), _u32, P(sc_material), _u32, P(sc_screen),
+                                P(sc_camera), _u32, _u32, P(_f32)]),
     "sc_batch_create": (_i32, [_vp, P(sc_scene_job), _u32, P(sc_batch_tuning), P(_vp)]),
     "sc_batch_destroy": (_i32, [_vp]),
     "sc_batch_autotune": (_i32, [_vp, P(sc_batch_tuning)]),

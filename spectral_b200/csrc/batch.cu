@@ -31,7 +31,7 @@ __device__ __forceinline__ void flush_mask(uint32_t* mask, uint32_t words, uint3
     __syncwarp();
 }
 
-template <int AGG, int MINB>
+template <int AGG, int MINB, bool SPLIT>
 __global__ void __launch_bounds__(256, MINB) batch_kernel(const BatchJobDev* __restrict__ jobs,
                                                           const WorkItem* __restrict__ items, uint32_t n_items,
                                                           uint32_t* counter, const float* __restrict__ cmf_g,
@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(const BatchJobDev* __r
     float* cmf = reinterpret_cast<float*>(smem);
     WarpSlot* slots = reinterpret_cast<WarpSlot*>(smem + kCmfBytes16);
     uint32_t* masks = reinterpret_cast<uint32_t*>(slots + blockDim.x / 32);
+    WarpSplitSmem* split = reinterpret_cast<WarpSplitSmem*>(masks + (blockDim.x / 32) * mask_words_max);
     for (uint32_t i = threadIdx.x; i < 3u * kTableN; i += blockDim.x) cmf[i] = cmf_g[i];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     uint32_t* mask = masks + warp * mask_words_max;
@@ -68,8 +69,14 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(const BatchJobDev* __r
         }
         SceneView S;
         S.prims = slot.prims; S.planes = slot.planes; S.mats = slot.mats; S.n_prims = slot.p.n_prims;
-        for (uint32_t i = lane; i < item.count; i += 32u)
-            trace_photon<true, AGG, false>(slot.p, S, cmf, item.begin + i, cur_words ? mask : nullptr);
+        if (SPLIT) {
+            for (uint32_t b0 = 0; b0 < item.count; b0 += 32u)
+                trace_warp_split<true, AGG>(slot.p, S, cmf, item.begin + b0 + lane, b0 + lane < item.count,
+                                            cur_words ? mask : nullptr, split[warp]);
+        } else {
+            for (uint32_t i = lane; i < item.count; i += 32u)
+                trace_photon<true, AGG, false>(slot.p, S, cmf, item.begin + i, cur_words ? mask : nullptr);
+        }
         __syncwarp();
     }
     if (cur_words) flush_mask(mask, cur_words, cur_flags, lane);
@@ -77,36 +84,39 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(const BatchJobDev* __r
 
 using BatchFn = void (*)(const BatchJobDev*, const WorkItem*, uint32_t, uint32_t*, const float*, uint32_t);
 
-BatchFn batch_fn(int agg, int minb) {
-    if (minb >= 5) return agg ? batch_kernel<1, 5> : batch_kernel<0, 5>;
-    return agg ? batch_kernel<1, 4> : batch_kernel<0, 4>;
+template <bool SPLIT>
+BatchFn batch_fn_t(int agg, int minb) {
+    if (minb >= 5) return agg ? batch_kernel<1, 5, SPLIT> : batch_kernel<0, 5, SPLIT>;
+    return agg ? batch_kernel<1, 4, SPLIT> : batch_kernel<0, 4, SPLIT>;
 }
+BatchFn batch_fn(int agg, int minb, int split) { return split ? batch_fn_t<true>(agg, minb) : batch_fn_t<false>(agg, minb); }
 
 }  // namespace
 
 static_assert(sizeof(WarpSlot) % 16 == 0, "warp slot must be a multiple of 16 bytes");
 static_assert(sizeof(WarpSlot) == sizeof(BatchSlotImage), "slot image layout");
 
-size_t batch_smem(uint32_t mask_words_max) {
-    return kCmfBytes16 + 8 * sizeof(WarpSlot) + 8 * mask_words_max * sizeof(uint32_t);
+size_t batch_smem(uint32_t mask_words_max, int split) {
+    return kCmfBytes16 + 8 * sizeof(WarpSlot) + 8 * mask_words_max * sizeof(uint32_t) +
+           (split ? 8 * sizeof(WarpSplitSmem) : 0);
 }
 
-int batch_occupancy(int agg, int minb, uint32_t mask_words_max) {
+int batch_occupancy(int agg, int minb, int split, uint32_t mask_words_max) {
     int n = 0;
-    const void* fn = reinterpret_cast<const void*>(batch_fn(agg, minb));
-    const size_t smem = batch_smem(mask_words_max);
+    const void* fn = reinterpret_cast<const void*>(batch_fn(agg, minb, split));
+    const size_t smem = batch_smem(mask_words_max, split);
     if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, smem) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 
 cudaError_t launch_batch(const BatchJobDev* jobs, const WorkItem* items, uint32_t n_items, uint32_t* counter,
-                         const float* cmf, uint32_t mask_words_max, int agg, int minb, uint32_t grid,
+                         const float* cmf, uint32_t mask_words_max, int agg, int minb, int split, uint32_t grid,
                          cudaStream_t s) {
-    const size_t smem = batch_smem(mask_words_max);  // attribute set by batch_occupancy before capture
+    const size_t smem = batch_smem(mask_words_max, split);  // attribute set by batch_occupancy before capture
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
-    batch_fn(agg, minb)<<<grid, 256, smem, s>>>(jobs, items, n_items, counter, cmf, mask_words_max);
+    batch_fn(agg, minb, split)<<<grid, 256, smem, s>>>(jobs, items, n_items, counter, cmf, mask_words_max);
     return cudaGetLastError();
 }
 

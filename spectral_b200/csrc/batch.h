@@ -27,10 +27,10 @@ struct alignas(16) BatchJobDev {
 
 struct WorkItem { uint32_t job, begin, count; };
 
-size_t batch_smem(uint32_t mask_words_max);
-int batch_occupancy(int agg, int minb, uint32_t mask_words_max);
+size_t batch_smem(uint32_t mask_words_max, int split);
+int batch_occupancy(int agg, int minb, int split, uint32_t mask_words_max);
 cudaError_t launch_batch(const BatchJobDev* jobs, const WorkItem* items, uint32_t n_items, uint32_t* counter,
-                         const float* cmf, uint32_t mask_words_max, int agg, int minb, uint32_t grid,
+                         const float* cmf, uint32_t mask_words_max, int agg, int minb, int split, uint32_t grid,
                          cudaStream_t s);
 
 }  // namespace sc

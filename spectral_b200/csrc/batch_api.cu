@@ -140,7 +140,8 @@ struct sc_batch {
         if (n.minb == 0) n.minb = 4;
         n.minb = n.minb >= 5 ? 5 : 4;
         n.aggregate = n.aggregate ? 1 : 0;
-        const int occ = batch_occupancy((int)n.aggregate, (int)n.minb, kBatchMaskWords);
+        n.per_photon = n.per_photon ? 1 : 0;
+        const int occ = batch_occupancy((int)n.aggregate, (int)n.minb, n.per_photon ? 0 : 1, kBatchMaskWords);
         grid = n.grid ? n.grid : (uint32_t)(ctx->sms * occ);
         if (n.chunk_photons != tuning.chunk_photons || n_items == 0) {
             int rc = build_items(n.chunk_photons);
@@ -154,7 +155,7 @@ struct sc_batch {
 
     int enqueue_batch(cudaStream_t s) {
         SC_CUDA(launch_batch(d_jobs.p, d_items.p, n_items, counter.p, ctx->cmf.p, kBatchMaskWords,
-                             (int)tuning.aggregate, (int)tuning.minb, grid, s));
+                             (int)tuning.aggregate, (int)tuning.minb, tuning.per_photon ? 0 : 1, grid, s));
         SC_CUDA(launch_reduce_many(d_descs.p, (uint32_t)jobs.size(), total_tiles, true, max_channels, s));
         return SC_OK;
     }
@@ -190,7 +191,7 @@ struct sc_batch {
             p.mats = reinterpret_cast<const sc_material*>(
                 reinterpret_cast<const unsigned char*>(d_jobs.p + j) + offsetof(BatchSlotImage, mats));
             LaunchShape shape;
-            shape.block = 256; shape.aggregate = 0; shape.minb = 4;
+            shape.block = 256; shape.aggregate = 0; shape.minb = 4; shape.split = tuning.per_photon ? 0 : 1;
             const size_t smem = scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats) +
                                 (geom[j].words <= kMaxSmemMaskWords ? geom[j].words * 4u : 0u);
             shape.grid = (uint32_t)(ctx->sms * photon_occupancy_blocks(shape, true, smem));
@@ -338,10 +339,11 @@ int sc_batch_autotune(sc_batch* b, sc_batch_tuning* chosen) {
     SC_CUDA(cudaEventCreate(&e1));
     sc_batch_tuning best{};
     float best_ms = 1e30f;
+    for (uint32_t per_photon : {0u, 1u})
     for (uint32_t chunk : {512u, 2048u, 8192u})
         for (uint32_t minb : {4u, 5u})
             for (uint32_t agg : {0u, 1u}) {
-                sc_batch_tuning t{chunk, minb, agg, 0};
+                sc_batch_tuning t{chunk, minb, agg, 0, per_photon};
                 int rc = b->apply_tuning(t);
                 if (rc == SC_OK) rc = b->run(b->stream);  // warm-up (also builds the graph)
                 if (rc != SC_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
@@ -468,7 +470,8 @@ int sc_batch_stats(sc_batch* b, uint64_t out[6]) {
     SC_CUDA(cudaMemcpyAsync(c, d.p, 32, cudaMemcpyDeviceToHost, b->stream));
     // dirty tiles of one pass: trace only, count the set bits, then drain
     SC_CUDA(launch_batch(b->d_jobs.p, b->d_items.p, b->n_items, b->counter.p, b->ctx->cmf.p, kBatchMaskWords,
-                         (int)b->tuning.aggregate, (int)b->tuning.minb, b->grid, b->stream));
+                         (int)b->tuning.aggregate, (int)b->tuning.minb, b->tuning.per_photon ? 0 : 1, b->grid,
+                         b->stream));
     std::vector<uint32_t> fl(b->flags.n);
     SC_CUDA(cudaMemcpyAsync(fl.data(), b->flags.p, b->flags.bytes(), cudaMemcpyDeviceToHost, b->stream));
     SC_CUDA(cudaStreamSynchronize(b->stream));

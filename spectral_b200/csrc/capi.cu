@@ -79,6 +79,7 @@ static int default_shape(sc_ctx* ctx, bool spectral, int aggregate, size_t smem,
     s.minb = 4;
     if (const char* agg = std::getenv("SPECTRAL_CUDA_AGGREGATE")) s.aggregate = std::atoi(agg) ? 1 : 0;
     if (const char* mb = std::getenv("SPECTRAL_CUDA_MINB")) s.minb = std::atoi(mb) >= 5 ? 5 : 4;
+    if (const char* sp = std::getenv("SPECTRAL_CUDA_SPLIT")) s.split = std::atoi(sp) ? 1 : 0;
     const int per_sm = photon_occupancy_blocks(s, spectral, smem);
     s.grid = (uint32_t)(ctx->sms * per_sm);
     return SC_OK;

@@ -29,8 +29,10 @@ struct PhotonParams {
 };
 
 // Photon launch: CTAs of 256 threads, `grid` CTAs (grid-stride), warp
-// aggregation on/off, register bound (minimum CTAs per SM: 4 or 5).
-struct LaunchShape { uint32_t block, grid; int aggregate; int minb; };
+// aggregation on/off, register bound (minimum CTAs per SM: 4 or 5), and the
+// warp-split transport (segments buffered per warp, haze samples processed as
+// one converged list) on/off.
+struct LaunchShape { uint32_t block, grid; int aggregate; int minb; int split = 1; };
 
 // Dirty-tile masks up to this many 32-bit words (16 KB, 524288 tiles) are
 // accumulated in shared memory by each photon CTA.

@@ -17,6 +17,14 @@ namespace sc {
 
 namespace {
 
+// Byte offset of the warp-split buffers: after scene records, CMF table and the
+// dirty mask, rounded up to 16 bytes.
+__host__ __device__ __forceinline__ size_t split_offset(const PhotonParams& p, uint32_t mask_words) {
+    const size_t b = p.n_prims * sizeof(sc_primitive) + p.n_planes * sizeof(sc_plane) +
+                     p.n_mats * sizeof(sc_material) + 3 * kTableN * sizeof(float) + mask_words * sizeof(uint32_t);
+    return (b + 15u) & ~size_t(15);
+}
+
 // Stage the scene records and the CMF table in shared memory; when `mask_words`
 // is non-zero a zeroed dirty-tile bitmask of that many words follows them.
 __device__ __forceinline__ SceneView load_scene(const PhotonParams& p, unsigned char* smem, const float** cmf_out,
@@ -41,15 +49,24 @@ __device__ __forceinline__ SceneView load_scene(const PhotonParams& p, unsigned 
 
 // 256 threads per CTA; MINB CTAs per SM bound the registers (4: 63 registers,
 // no spills; 5: 48 registers, a few spills, more warps in flight).
-template <bool SPEC, int AGG, int MINB>
+template <bool SPEC, int AGG, int MINB, bool SPLIT>
 __global__ void __launch_bounds__(256, MINB) photon_kernel(const PhotonParams p, uint32_t mask_words) {
     extern __shared__ __align__(16) unsigned char smem[];
     const float* cmf;
     uint32_t* smask;
     const SceneView S = load_scene(p, smem, &cmf, &smask, mask_words);
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += stride)
-        trace_photon<SPEC, AGG, false>(p, S, cmf, p.photon_base + i, smask);
+    if (SPLIT) {  // warp-split transport: per-warp segment buffers after the scene
+        WarpSplitSmem* ws = reinterpret_cast<WarpSplitSmem*>(smem + split_offset(p, mask_words));
+        const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+        const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+        for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < p.photon_count; base += warps * 32u)
+            trace_warp_split<SPEC, AGG>(p, S, cmf, p.photon_base + base + lane, base + lane < p.photon_count, smask,
+                                        ws[warp]);
+    } else {
+        const uint32_t stride = gridDim.x * blockDim.x;
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += stride)
+            trace_photon<SPEC, AGG, false>(p, S, cmf, p.photon_base + i, smask);
+    }
     if (smask) {  // publish this CTA's dirty tiles
         __syncthreads();
         for (uint32_t w = threadIdx.x; w < mask_words; w += blockDim.x)
@@ -140,19 +157,27 @@ size_t scene_smem_bytes(uint32_t n_prims, uint32_t n_planes, uint32_t n_mats) {
 
 using PhotonKernelFn = void (*)(const PhotonParams, uint32_t);
 
-static PhotonKernelFn photon_fn(bool spec, int agg, int minb) {
+template <bool SPLIT>
+static PhotonKernelFn photon_fn_t(bool spec, int agg, int minb) {
     if (minb >= 5) {
-        if (spec) return agg ? photon_kernel<true, 1, 5> : photon_kernel<true, 0, 5>;
-        return agg ? photon_kernel<false, 1, 5> : photon_kernel<false, 0, 5>;
+        if (spec) return agg ? photon_kernel<true, 1, 5, SPLIT> : photon_kernel<true, 0, 5, SPLIT>;
+        return agg ? photon_kernel<false, 1, 5, SPLIT> : photon_kernel<false, 0, 5, SPLIT>;
     }
-    if (spec) return agg ? photon_kernel<true, 1, 4> : photon_kernel<true, 0, 4>;
-    return agg ? photon_kernel<false, 1, 4> : photon_kernel<false, 0, 4>;
+    if (spec) return agg ? photon_kernel<true, 1, 4, SPLIT> : photon_kernel<true, 0, 4, SPLIT>;
+    return agg ? photon_kernel<false, 1, 4, SPLIT> : photon_kernel<false, 0, 4, SPLIT>;
 }
+static PhotonKernelFn photon_fn(const LaunchShape& s, bool spec) {
+    return s.split ? photon_fn_t<true>(spec, s.aggregate, s.minb) : photon_fn_t<false>(spec, s.aggregate, s.minb);
+}
+// Shared memory beyond scene + mask: one segment buffer per warp (8 warps).
+static size_t split_bytes(const LaunchShape& s) { return s.split ? 16 + 8 * sizeof(WarpSplitSmem) : 0; }
 
 int photon_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem) {
     int n = 0;
-    const void* fn = reinterpret_cast<const void*>(photon_fn(spectral, shape.aggregate, shape.minb));
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)shape.block, smem) != cudaSuccess) return 1;
+    const void* fn = reinterpret_cast<const void*>(photon_fn(shape, spectral));
+    const size_t total = smem + split_bytes(shape);
+    if (total > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)shape.block, total) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 
@@ -166,11 +191,12 @@ uint32_t photon_mask_words(const PhotonParams& p) {
 cudaError_t launch_photons(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s) {
     if (p.photon_count == 0) return cudaSuccess;
     const uint32_t mw = photon_mask_words(p);
-    const size_t smem = scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats) + mw * sizeof(uint32_t);
+    const size_t smem = shape.split ? split_offset(p, mw) + 8 * sizeof(WarpSplitSmem)
+                                    : scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats) + mw * sizeof(uint32_t);
     const bool spec = p.channels != 3u || p.bins != 0u;
     const uint32_t need = (p.photon_count + 255u) / 256u;
     const uint32_t grid = need < shape.grid ? need : shape.grid;
-    photon_fn(spec, shape.aggregate, shape.minb)<<<grid, 256, smem, s>>>(p, mw);
+    photon_fn(shape, spec)<<<grid, 256, smem, s>>>(p, mw);
     return cudaGetLastError();
 }
 

@@ -90,6 +90,53 @@ __device__ __forceinline__ void record_pair(sc_debug_photon* rec, uint32_t pair,
 // haze samples that land in frame (= film splats), dielectric/diffuse scatters.
 struct PhotonCounts { uint32_t segments, splats, scatters; };
 
+// One point-estimator haze sample at distance `dist` along a segment
+// (spectral-core/src/volume.rs:130-150): camera projection, z-test, HG phase x
+// transmittance / d^2 x seg/4.  Returns whether the sample lands in frame;
+// `contrib`, px, py are its weight and pixel.
+__device__ __forceinline__ bool haze_sample(const PhotonParams& p, f3 o, f3 d, float dist, float seg, float power,
+                                            uint32_t& px, uint32_t& py, float& contrib) {
+    const f3 q = add(o, mul(d, dist));
+    float s, t;
+    bool ok = project(p.proj, q, s, t);
+    contrib = 0.0f;
+    px = py = 0u;
+    if (ok) {
+        px = min((uint32_t)(s * (float)p.width), p.width - 1u);
+        py = min((uint32_t)((1.0f - t) * (float)p.height), p.height - 1u);
+        if (p.estimator == 0u) {
+            const f3 to = sub(p.proj.o, q);
+            const float dd = fmaxf(length(to), 1e-3f);
+            if (p.zbuf && !(dd < p.zbuf[py * p.width + px])) {
+                ok = false;
+            } else {
+                // g == 0: phase_hg is exactly 1/(4 pi) (pow(1, 1.5) == 1), so the
+                // direction to the camera is not needed.
+                const float phase = p.g == 0.0f ? kInv4Pi : phase_hg(p.g, dot(d, vdiv(to, dd)));
+                const float trans = expf(-p.sigma_t * dd);
+                contrib = power * p.sigma_s * phase * trans / (dd * dd) * seg / 4.0f;
+            }
+        } else {
+            contrib = power * p.sigma_s * seg / 4.0f * kInv4Pi;
+        }
+    }
+    return ok;
+}
+
+// Photon-level splat payload: CMF of the photon's wavelength (XYZ film) or its bin.
+__device__ __forceinline__ void photon_payload(const PhotonParams& p, const float* cmf, float lambda, float& cx,
+                                               float& cy, float& cz, uint32_t& bin, bool spec) {
+    if (spec) {
+        float fb = (lambda - p.bin_min) * p.bin_inv_width;
+        int bi = (int)fb;
+        bin = fb < 0.0f ? 0u : (bi >= (int)p.bins ? p.bins - 1u : (uint32_t)bi);
+    } else {
+        cx = tab_sample(cmf, lambda);
+        cy = tab_sample(cmf + kTableN, lambda);
+        cz = tab_sample(cmf + 2 * kTableN, lambda);
+    }
+}
+
 template <bool SPEC, int AGG, bool DEBUG, bool COUNT = false>
 __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneView& S, const float* cmf,
                                              uint32_t idx, uint32_t* smask, PhotonCounts* cnt = nullptr) {
@@ -100,17 +147,7 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
     const float lambda = p.lambda_min + p.lambda_range * r.f32();
     float cx = 0.f, cy = 0.f, cz = 0.f;
     uint32_t bin = 0;
-    if (!DEBUG) {
-        if (SPEC) {
-            float fb = (lambda - p.bin_min) * p.bin_inv_width;
-            int bi = (int)fb;
-            bin = fb < 0.0f ? 0u : (bi >= (int)p.bins ? p.bins - 1u : (uint32_t)bi);
-        } else {
-            cx = tab_sample(cmf, lambda);
-            cy = tab_sample(cmf + kTableN, lambda);
-            cz = tab_sample(cmf + 2 * kTableN, lambda);
-        }
-    }
+    if (!DEBUG) photon_payload(p, cmf, lambda, cx, cy, cz, bin, SPEC);
     f3 d = p.bdir;
     float power = 1.0f;
     uint32_t n_glass = 0xFFFFFFFFu;
@@ -133,30 +170,9 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
         for (int k = 0; k < 4; ++k) {
             const float dist = r.f32() * seg;
             if (DEBUG) continue;
-            const f3 q = add(o, mul(d, dist));
-            float s, t;
-            bool ok = project(p.proj, q, s, t);
-            uint32_t px = 0, py = 0;
-            float contrib = 0.0f;
-            if (ok) {
-                px = min((uint32_t)(s * (float)p.width), p.width - 1u);
-                py = min((uint32_t)((1.0f - t) * (float)p.height), p.height - 1u);
-                if (p.estimator == 0u) {
-                    const f3 to = sub(p.proj.o, q);
-                    const float dd = fmaxf(length(to), 1e-3f);
-                    if (p.zbuf && !(dd < p.zbuf[py * p.width + px])) {
-                        ok = false;
-                    } else {
-                        // g == 0: phase_hg is exactly 1/(4 pi) (pow(1, 1.5) == 1), so
-                        // the direction to the camera is not needed.
-                        const float phase = p.g == 0.0f ? kInv4Pi : phase_hg(p.g, dot(d, vdiv(to, dd)));
-                        const float trans = expf(-p.sigma_t * dd);
-                        contrib = power * p.sigma_s * phase * trans / (dd * dd) * seg / 4.0f;
-                    }
-                } else {
-                    contrib = power * p.sigma_s * seg / 4.0f * kInv4Pi;
-                }
-            }
+            uint32_t px, py;
+            float contrib;
+            const bool ok = haze_sample(p, o, d, dist, seg, power, px, py, contrib);
             if (COUNT) { if (ok) ++cnt->splats; continue; }
             deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, cx, cy, cz, bin);
         }
@@ -179,6 +195,109 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
         if (DEBUG) { record_pair(rec, pairs, o, d); ++pairs; }
     }
     if (DEBUG) rec->num_states = pairs < 9u ? pairs : 9u;
+}
+
+// ---------------------------------------------------------------------------
+// Warp-split transport.  (a) Every lane traces its photon's path (intersect,
+// Fresnel / refract / TIR scatter) and appends one record per segment to the
+// warp's shared-memory segment buffer; (b) the warp then works through the 4
+// haze samples of every buffered segment as one flat list, so the expensive
+// camera connection runs converged even when the photons of a warp have
+// different numbers of segments.  PCG is counter based: sample k of a segment
+// uses draw pcg32(state_before + k + 1), exactly the draw the per-photon loop
+// makes, so paths and films are bit-identical to trace_photon's.
+struct SegRec { f3 o, d; float seg, power; uint32_t rng, lane; };
+constexpr uint32_t kWarpSegs = 96;
+struct alignas(16) WarpSplitSmem {
+    SegRec seg[kWarpSegs];
+    float4 payload[32];  // per lane: CMF x, y, z of the photon (XYZ film) or its bin in .w
+};
+static_assert(sizeof(SegRec) == 40, "segment record layout");
+
+template <bool SPEC, int AGG>
+__device__ __forceinline__ void flush_segments(const PhotonParams& p, WarpSplitSmem& ws, uint32_t n, uint32_t* smask,
+                                               uint32_t lane) {
+    __syncwarp();
+    const uint32_t total = 4u * n;
+    for (uint32_t t = lane; t < total; t += 32u) {
+        const SegRec R = ws.seg[t >> 2];
+        const float u = (float)(pcg32(R.rng + (t & 3u) + 1u) >> 8) * (1.0f / 16777216.0f);
+        uint32_t px, py;
+        float contrib;
+        const bool ok = haze_sample(p, R.o, R.d, u * R.seg, R.seg, R.power, px, py, contrib);
+        const float4 pl = ws.payload[R.lane];
+        deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, pl.x, pl.y, pl.z, __float_as_uint(pl.w));
+    }
+    __syncwarp();
+}
+
+// All 32 lanes of the warp must call this together; lanes without a photon pass
+// valid = false.
+template <bool SPEC, int AGG>
+__device__ __forceinline__ void trace_warp_split(const PhotonParams& p, const SceneView& S, const float* cmf,
+                                                 uint32_t idx, bool valid, uint32_t* smask, WarpSplitSmem& ws) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned below = (1u << lane) - 1u;
+    Rng r = Rng::make(idx, p.seed);
+    f3 o = mk(0.f, 0.f, 0.f), d = p.bdir;
+    float lambda = 0.0f, power = 1.0f;
+    if (valid) {
+        const float r1 = r.f32();
+        const float r2 = r.f32();
+        o = add(add(p.corner, mul(p.bu, r1)), mul(p.bv, r2));
+        lambda = p.lambda_min + p.lambda_range * r.f32();
+        float cx = 0.f, cy = 0.f, cz = 0.f;
+        uint32_t bin = 0;
+        photon_payload(p, cmf, lambda, cx, cy, cz, bin, SPEC);
+        ws.payload[lane] = make_float4(cx, cy, cz, __uint_as_float(bin));
+    }
+    bool alive = valid;
+    uint32_t n = 0;  // buffered segments, the same in every lane
+    uint32_t n_glass = 0xFFFFFFFFu;
+    float n_cached = 1.0f;
+    for (uint32_t b = 0; b < p.max_bounces; ++b) {
+        const unsigned m = __ballot_sync(0xffffffffu, alive);
+        if (m == 0u) break;
+        Hit h;
+        uint32_t mi = 0;
+        bool any = false;
+        float seg = 0.0f;
+        if (alive) {
+            any = scene_hit(S, o, d, h, mi);
+            seg = any ? h.t : p.max_dist;
+        }
+        const uint32_t cnt = __popc(m);
+        if (n + cnt > kWarpSegs) {
+            flush_segments<SPEC, AGG>(p, ws, n, smask, lane);
+            n = 0;
+        }
+        if (alive) {
+            SegRec& R = ws.seg[n + __popc(m & below)];
+            R.o = o; R.d = d; R.seg = seg; R.power = power; R.rng = r.state; R.lane = lane;
+            r.state += 4u;  // this segment's 4 distance draws, made by the flush
+            if (!any) {
+                alive = false;
+            } else {
+                const sc_material& mt = S.mats[mi];
+                float nh = 1.0f;
+                if (mt.kind == 1u) {
+                    if (mt.glass != n_glass) {
+                        n_cached = glass_n(mt.glass, p.spectral ? lambda : 550.0f);
+                        n_glass = mt.glass;
+                    }
+                    nh = n_cached;
+                }
+                f3 nd;
+                float w;
+                scatter(mt, d, h, nh, r, nd, w);
+                power *= w;
+                o = h.point;
+                d = nd;
+            }
+        }
+        n += cnt;
+    }
+    flush_segments<SPEC, AGG>(p, ws, n, smask, lane);
 }
 
 }  // namespace sc

@@ -223,7 +223,7 @@ struct sc_server {
         SC_CUDA(cudaMemcpyAsync(d_items.p, h_items.data(), h_items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
                                 stream));
         SC_CUDA(launch_batch(d_jobs.p, d_items.p, (uint32_t)h_items.size(), counter.p, ctx->cmf.p, kBatchMaskWords, 0,
-                             4, grid, stream));
+                             4, 1, grid, stream));
         SC_CUDA(launch_reduce_many(d_descs.p, n, tiles, true, maxc, stream));
         SC_CUDA(cudaStreamSynchronize(stream));
         const double t1 = now_s();
@@ -276,7 +276,7 @@ int sc_server_create(sc_ctx* ctx, const sc_server_config* cfg, sc_server** out) 
     if ((e = s->d_descs.alloc(s->cfg.max_slots)) != cudaSuccess) return fail(e);
     if ((e = s->counter.alloc(1)) != cudaSuccess) return fail(e);
     s->arena.reset(cfg->hbm_budget_bytes);
-    s->grid = (uint32_t)(ctx->sms * batch_occupancy(0, 4, kBatchMaskWords));
+    s->grid = (uint32_t)(ctx->sms * batch_occupancy(0, 4, 1, kBatchMaskWords));
     *out = s;
     return SC_OK;
     SC_GUARD_END

@@ -14,7 +14,7 @@ import math
 
 import numpy as np
 
-from . import BK7, FUSED_SILICA, SF11, WATER, Beam, Camera, Dielectric, Scene
+from . import BK7, FUSED_SILICA, SF11, WATER, Beam, Camera, Dielectric, Scene, Screen
 
 
 def prism_planes(apex_deg, side, depth):
@@ -53,6 +53,25 @@ def prism_workload(width=640, height=360, glass=SF11, apex_deg=60.0, side=1.0, i
     beam = prism_beam(apex_deg, side, incidence_deg, beam_width)
     cam = Camera.look_at((0.6, -0.4, 6.0), (0.6, -0.4, 0.0), (0.0, 1.0, 0.0), 42.0, width / height)
     return scene, beam, cam
+
+
+def wedge_planes(apex_deg, size, depth):
+    """ConvexSolid::wedge (spectral-core/src/geom.rs:110-121) in f32 trig."""
+    a = np.float32(apex_deg) * np.float32(np.float32(math.pi) / np.float32(180.0))
+    return [((-1.0, 0.0, 0.0), -size), ((float(np.cos(a)), float(np.sin(a)), 0.0), -size), ((0.0, -1.0, 0.0), -size),
+            ((0.0, 0.0, 1.0), -depth / 2.0), ((0.0, 0.0, -1.0), -depth / 2.0)]
+
+
+def prism_on_plane(width=800, height=600, floor_texels=512):
+    """The floor, SF11 wedge, beam and oblique camera of
+    spectral-core/examples/prism_on_plane.rs:77-119: returns
+    (scene, floor Screen, beam, camera)."""
+    floor = Screen((-5.0, -1.0, -5.0), (0.0, 0.0, 10.0), (14.0, 0.0, 0.0), floor_texels, floor_texels)
+    scene = Scene(background=0.0)
+    scene.add_solid(wedge_planes(30.0, 1.0, 2.0), Dielectric(SF11))
+    beam = Beam((-3.0, 0.55, -0.75), (0.0, 0.0, 1.5), (0.0, 0.12, 0.0), (1.0, 0.0, 0.0))
+    cam = Camera.look_at((0.0, 4.5, 9.0), (4.0, -1.2, 0.0), (0.0, 1.0, 0.0), 50.0, width / height)
+    return scene, floor, beam, cam
 
 
 def rainbow_workload(width=1920, height=1080, beam_width=2.2):

@@ -65,7 +65,7 @@ def test_autotune_and_tunings_agree(ctx):
     ref = b.read_all_xyz().copy()
     chosen = b.autotune()
     assert chosen["chunk_photons"] in (512, 2048, 8192) and chosen["minb"] in (4, 5)
-    for t in [(64, 4, 0), (1024, 5, 1), (32, 4, 1)]:
+    for t in [(64, 4, 0, 0, 0), (1024, 5, 1, 0, 0), (32, 4, 1, 0, 1), (96, 5, 0, 0, 1), (4096, 4, 0, 7, 0)]:
         b.set_tuning(*t)
         b.run()
         assert b.read_all_xyz().tobytes() == ref.tobytes(), t

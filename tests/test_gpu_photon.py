@@ -148,15 +148,21 @@ def test_forward_gpu_determinism_and_chunking(ctx):
     assert a.accum().tobytes() == c.accum().tobytes()
 
 
-@pytest.mark.parametrize("aggregate", [0, 1])
-def test_warp_aggregated_splats_identical(ctx, aggregate, monkeypatch):
+@pytest.mark.parametrize("aggregate,split,minb", [(0, 0, 4), (1, 0, 4), (0, 1, 4), (1, 1, 5), (0, 1, 5)])
+@pytest.mark.parametrize("bins", [0, 24])
+def test_launch_variants_give_identical_films(ctx, aggregate, split, minb, bins, monkeypatch):
+    """Warp-aggregated atomics, the warp-split transport and the register bound
+    are pure scheduling choices: every variant writes the same film bits."""
     monkeypatch.setenv("SPECTRAL_CUDA_AGGREGATE", str(aggregate))
-    f, *_ = dsotm_film(ctx, 96, 96, 50_000, 3)
+    monkeypatch.setenv("SPECTRAL_CUDA_SPLIT", str(split))
+    monkeypatch.setenv("SPECTRAL_CUDA_MINB", str(minb))
+    f, *_ = dsotm_film(ctx, 96, 80, 50_000, 3, bins=bins, max_bounces=5)
     f.trace_and_resolve(50_000, 3)
-    monkeypatch.setenv("SPECTRAL_CUDA_AGGREGATE", "0")
-    g, *_ = dsotm_film(ctx, 96, 96, 50_000, 3)
+    for k in ("SPECTRAL_CUDA_AGGREGATE", "SPECTRAL_CUDA_SPLIT", "SPECTRAL_CUDA_MINB"):
+        monkeypatch.setenv(k, "0")
+    g, *_ = dsotm_film(ctx, 96, 80, 50_000, 3, bins=bins, max_bounces=5)
     g.trace_and_resolve(50_000, 3)
-    assert (f.read_raw() == g.read_raw()).all()
+    assert (f.read_raw() == g.read_raw()).all() and f.read_raw().sum() > 0
 
 
 @pytest.mark.parametrize("bins,band", [(64, (380.0, 730.0)), (32, (380.0, 780.0)), (7, (400.0, 700.0))])
