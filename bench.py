@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch"], default="batch")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "tracer"], default="batch")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps")
@@ -348,6 +348,171 @@ def run_gpu(args, rank, world, local_rank):
     return line
 
 
+# Camera-tracer workload (config 2): SF11 prism on a diffuse ground plane,
+# spherical D65 emitter r=0.2 at (2,3,1), 1280x720, 64 spp per step, hero comb
+# of 4 wavelengths, depth 8, Russian roulette after bounce 3.
+TRACER = dict(width=1280, height=720, spp=64, seed=0x7ACE)
+TRACER_WAVE_PATHS = 1 << 20  # paths per wavefront wave (the library's queue size)
+
+
+def run_cpu_tracer(seconds, threads=None):
+    """Path samples/s of the CPU restatement of CpuTracer (pixel-parallel, as
+    the reference's rayon loop) with the emitter / roulette extensions, on
+    whole frames at 1 spp until ~`seconds` of work."""
+    import oracle
+    from spectral_b200.scenes import tracer_workload
+    W, H = TRACER["width"], TRACER["height"]
+    scene, cam, kw = tracer_workload(W, H)
+    prims, np_, planes, npl, mats, nm = scene.arrays()
+    osc = oracle.OScene(bytes(prims), np_, bytes(planes), npl, bytes(mats), nm, scene.background)
+    oc = oracle.or_camera.from_buffer_copy(bytes(cam.c))
+    c, r, sc = kw["emitter"]
+    ext = oracle.or_tracer_ext(oracle.F3(*c), r, sc, kw["rr_start"])
+    threads = threads or os.cpu_count() or 1
+    out = np.zeros(3 * W * H, np.float32)
+    oracle.lib.or_tracer_set_ext(C.byref(ext))
+    try:
+        frames, t0 = 0, time.perf_counter()
+        while True:
+            oracle.lib.or_tracer_accumulate_mt(C.byref(osc.c), C.byref(oc), W, H, 0, TRACER["seed"], 1, frames,
+                                               kw["max_depth"], oracle.fp(out), threads)
+            frames += 1
+            dt = time.perf_counter() - t0
+            if dt >= seconds:
+                break
+    finally:
+        oracle.lib.or_tracer_set_ext(None)
+    return W * H * frames / dt, frames, dt, threads
+
+
+def run_gpu_tracer(args, rank, world, local_rank):
+    import torch
+    import spectral_b200 as sb
+    from spectral_b200 import _lib
+    from spectral_b200.scenes import tracer_workload
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ctx = sb.GpuContext(local_rank)
+    W, H, SPP = TRACER["width"], TRACER["height"], TRACER["spp"]
+    scene, cam, kw = tracer_workload(W, H)
+    seed = TRACER["seed"] + rank  # each rank: its own independent 64-spp frame
+    tr = sb.GpuTracer(ctx, scene, cam, W, H, sb.D65, seed, **kw)
+    sp = C.c_void_p()
+    _lib.check(_lib.lib.sc_tracer_stream(tr.h, C.byref(sp)))
+    st = torch.cuda.ExternalStream(sp.value, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        tr.accumulate(SPP)
+    torch.cuda.synchronize()
+    _, seg0 = tr.stats()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    with ClockSampler(uuid) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(st):
+                flush.zero_()  # evict queues and accumulators from L2 (outside the events)
+            ev[k][0].record(st)
+            tr.accumulate(SPP)
+            ev[k][1].record(st)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps)]
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    paths, seg1 = tr.stats()
+    segments = (seg1 - seg0) // args.steps
+    samples = W * H * SPP
+    value = samples * world * args.steps / (total_ms / 1e3)
+
+    # end to end through the GpuTracer-shaped ABI object with host buffers: a new
+    # camera, clear, 64 spp, mean XYZ back to the host, every step
+    host = np.empty(3 * W * H, np.float32)
+    e2e_steps = args.e2e_steps or args.steps
+
+    def e2e_step():
+        tr.set_camera(cam)
+        tr.clear_accum()
+        tr.accumulate(SPP)
+        _lib.check(_lib.lib.sc_tracer_read_xyz(tr.h, host.ctypes.data_as(C.POINTER(C.c_float))))
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = samples * world * e2e_steps / e2e_s
+    tr.close()
+    if rank != 0:
+        return None
+
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    peak_note = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    step_s = statistics.mean(step_ms) / 1e3
+    cl = clk.summary()
+    sm_mhz = cl["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp32_peak = sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+    n_planes = len(scene.planes)
+    # counted FP32 work per path segment: 14 per plane (intersection), 20 for the
+    # emitter sphere test, 60 for the shading step (Fresnel / refraction or
+    # cosine sampling, 4-lane throughput and radiance update)
+    flops = segments * (14 * n_planes + 20 + 60)
+    # wavefront queue traffic per segment: ray 24 B read by intersect, hit 20 B
+    # written and read, path state 44 B read and written by shade
+    qbytes = segments * (24 + 2 * 20 + 2 * 44)
+    waves = -(-(W * H) // max(1, TRACER_WAVE_PATHS // SPP))
+    line = {
+        "metric": "path samples/s (hero-wavelength camera tracer, 4 lanes, depth 8)",
+        "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
+        "config": {"workload": "tracer: SF11 prism on a diffuse ground (albedo 0.8), D65 sphere emitter r=0.2 at "
+                               "(2,3,1), 1280x720, 64 spp, depth 8, roulette after bounce 3",
+                   "samples_per_step": samples * world, "l2": "flushed between steps (256 MB write outside the events)",
+                   "parallelism": "independent frames per rank (own seed), no collective"},
+        "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": C.sizeof(cam.c),
+                "d2h_bytes_per_step": 3 * W * H * 4,
+                "path": "sc_tracer_set_camera + clear_accum + accumulate(64) + read_xyz (host f32 XYZ)"},
+        "gpu_launches": args.steps * waves * (2 + 2 * kw["max_depth"]),
+        "kernels": {"accumulate_ms": statistics.mean(step_ms)},
+        "roofline": {"bound": "hbm", "achieved": qbytes / step_s / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": qbytes / step_s / 1e9 / hbm, "traffic": None, "kernel": "tr_intersect + tr_shade",
+                     "peak_source": "%s hbm_gbs" % peak_note,
+                     "algorithmic": "wavefront queue bytes: 176 B per path segment, %d segments per step" % segments},
+        "roofline_fp32": {"kernel": "tr_intersect + tr_shade", "counted_flops": flops,
+                          "achieved_tflops": flops / step_s / 1e12, "peak_tflops": fp32_peak,
+                          "frac": flops / step_s / 1e12 / fp32_peak,
+                          "peak_source": "%d SMs x 128 FP32 lanes x 2 x %.0f MHz (sampled median)" % (sms, sm_mhz)},
+        "work": {"paths": samples, "segments": segments},
+        "clocks": cl,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        rate, frames, dt, th = run_cpu_tracer(args.cpu_seconds)
+        line["cpu_baseline"] = {"value": rate, "unit": "samples/s", "cores": th, "kind": "port",
+                                "sample": "%d frames of 1280x720 at 1 spp (%.1f s), %s" % (frames, dt, cpu_model())}
+    return line
+
+
 BATCH = dict(n_jobs=256, seed=0xB200, bins=32, lambda_min=380.0, lambda_max=780.0)
 
 
@@ -559,7 +724,16 @@ def main():
             return 0
         rates = []
         per_step = max(1.0, args.cpu_seconds / max(1, args.steps))
-        if args.workload == "batch":
+        if args.workload == "tracer":
+            run_cpu_tracer(0.5)
+            for _ in range(args.steps):
+                rate, frames, dt, th = run_cpu_tracer(per_step)
+                rates.append((TRACER["width"] * TRACER["height"] * frames, dt))
+            sample = "per step whole 1280x720 frames at 1 spp for ~%.1f s" % per_step
+            metric = "path samples/s (hero-wavelength camera tracer, 4 lanes, depth 8)"
+            cfg_line = {"workload": "tracer (see the GPU arm)", "samples_per_step": TRACER["width"] * TRACER["height"]
+                        * TRACER["spp"]}
+        elif args.workload == "batch":
             run_cpu_batch(0.5)
             for _ in range(args.steps):
                 rate, n_s, dt, th, sc = run_cpu_batch(per_step)
@@ -581,15 +755,16 @@ def main():
                         "film": [cfg["width"], cfg["height"], cfg["bins"]]}
         tot_n, tot_t = sum(n for n, _ in rates), sum(t for _, t in rates)
         value = tot_n / tot_t
+        unit, what = ("samples/s", "CpuTracer::accumulate") if args.workload == "tracer" else \
+            ("photons/s", "render_volumetric_scene_point")
         line = {"metric": metric, "value": value,
-                "unit": "photons/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": tot_t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32 transport", "data": "synthetic (seeded scenes)", "impl": "reference",
                 "config": cfg_line,
-                "cpu_baseline": {"value": value, "unit": "photons/s", "cores": th, "kind": "port",
-                                 "sample": sample + "; CPU restatement of spectral-core "
-                                                    "render_volumetric_scene_point, %s" % cpu_model()},
-                "e2e": {"value": value, "unit": "photons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                "cpu_baseline": {"value": value, "unit": unit, "cores": th, "kind": "port",
+                                 "sample": sample + "; CPU restatement of spectral-core %s, %s" % (what, cpu_model())},
+                "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
     if world > 1:
@@ -597,7 +772,8 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = (run_gpu_batch if args.workload == "batch" else run_gpu)(args, rank, world, local_rank)
+    line = {"batch": run_gpu_batch, "tracer": run_gpu_tracer}.get(args.workload, run_gpu)(args, rank, world,
+                                                                                          local_rank)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

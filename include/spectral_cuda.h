@@ -65,7 +65,9 @@ typedef struct {
     float lambda_max;       /* emission band end, nm (0 -> 730) */
     uint32_t max_bounces;   /* bounce loop length (0 -> 8, volume.rs:126) */
     uint32_t scale_log2;    /* fixed-point scale 2^k (0 -> 32) */
-    uint32_t estimator;     /* 0 point estimator (volume.rs:99-168), 1 legacy isotropic (volume.rs:22-85) */
+    uint32_t estimator;     /* 0 point estimator (volume.rs:99-168), 1 legacy isotropic (volume.rs:22-85),
+                               2 photon-beam estimator (volume.rs:170-329; photon films and the
+                               device-pointer trace only; deposits are small: use scale_log2 >= 40) */
 } sc_film_options;
 
 typedef struct sc_batch sc_batch;
@@ -194,6 +196,9 @@ int sc_tracer_set_camera(sc_tracer* t, const sc_camera* cam);
 /* clear_accum (lib.rs:386-389): zero the sum and the sample count. */
 int sc_tracer_clear_accum(sc_tracer* t);
 int sc_tracer_dims(sc_tracer* t, uint32_t* width, uint32_t* height);
+/* The CUDA stream (cudaStream_t) all of this tracer's work runs on, for callers
+ * that order or time their own work against it.  Owned by the tracer. */
+int sc_tracer_stream(sc_tracer* t, void** stream);
 /* paths of the last accumulate and path segments traced since creation. */
 int sc_tracer_last_stats(sc_tracer* t, uint64_t* paths, uint64_t* segments);
 

@@ -173,6 +173,14 @@ def render_point(scene, cam, beam, p, begin, end, zbuf=None, f32=True, xyz=True,
     return img, fx, fs
 
 
+def render_beam(scene, cam, beam, p, begin, end, zbuf=None):
+    """render_volumetric_scene (volume.rs:233-329), f32 XYZ image 3*w*h."""
+    img = np.zeros(3 * p.width * p.height, np.float32)
+    z = fp(np.ascontiguousarray(zbuf, np.float32)) if zbuf is not None else None
+    _lib.or_render_beam(C.byref(scene.c), C.byref(cam), C.byref(beam), C.byref(p), z, begin, end, fp(img))
+    return img
+
+
 def simulate_photon(scene, beam, p, idx, max_pairs=9):
     st = np.zeros(8 * max_pairs, np.float32)
     lam = C.c_float()

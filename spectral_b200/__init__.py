@@ -190,16 +190,24 @@ def _fptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
+POINT, ISOTROPIC, BEAM = 0, 1, 2
+
+
 class GpuPhotonFilm:
     """GpuPhotonFilm (spectral-gpu/src/vol_photons.rs:228-851) on sm_100a.
 
     Extra keyword arguments select the film beyond the reference: ``bins`` (0 =
     XYZ film, N = spectral bins), the emission band, ``max_bounces``,
-    ``scale_log2`` and ``estimator``."""
+    ``scale_log2`` (default 2^32, 2^40 for the beam estimator) and
+    ``estimator``: POINT (render_volumetric_scene_point, the GPU path of the
+    reference), ISOTROPIC (render_volumetric) or BEAM (render_volumetric_scene,
+    spectral-core/src/volume.rs:170-329)."""
 
     def __init__(self, ctx, scene, camera, beam, width, height, n_photons, seed, max_dist, weights=None,
-                 zbuffer=None, bins=0, lambda_min=380.0, lambda_max=730.0, max_bounces=8, scale_log2=32,
+                 zbuffer=None, bins=0, lambda_min=380.0, lambda_max=730.0, max_bounces=8, scale_log2=None,
                  estimator=0):
+        if scale_log2 is None:
+            scale_log2 = 40 if estimator == BEAM else 32
         self.ctx = ctx
         self.width, self.height = int(width), int(height)
         weights = weights or VolWeights()

@@ -152,6 +152,7 @@ PROTOTYPES = {
     "sc_tracer_clear_accum": (_i32, [_vp]),
     "sc_tracer_dims": (_i32, [_vp, P(_u32), P(_u32)]),
     "sc_tracer_last_stats": (_i32, [_vp, P(_u64), P(_u64)]),
+    "sc_tracer_stream": (_i32, [_vp, P(_vp)]),
     "sc_atomic_film_create": (_i32, [_vp, _u32, _u32, P(_vp)]),
     "sc_atomic_film_destroy": (_i32, [_vp]),
     "sc_atomic_film_splat": (_i32, [_vp, _u32, _u32]),

@@ -24,8 +24,8 @@ void set_error(const char* fmt, ...) {
     g_error = buf;
 }
 
-static int check_scene(uint32_t n_prims, uint32_t n_planes, uint32_t n_mats, const sc_primitive* prims,
-                       const sc_plane* planes, const sc_material* mats) {
+int check_scene(uint32_t n_prims, uint32_t n_planes, uint32_t n_mats, const sc_primitive* prims,
+                const sc_plane* planes, const sc_material* mats) {
     SC_REQUIRE(n_prims <= SC_MAX_PRIMS, SC_E_LIMIT, "scene has %u primitives (max %d)", n_prims, SC_MAX_PRIMS);
     SC_REQUIRE(n_planes <= SC_MAX_PLANES, SC_E_LIMIT, "scene has %u planes (max %d)", n_planes, SC_MAX_PLANES);
     SC_REQUIRE(n_mats <= SC_MAX_PRIMS, SC_E_LIMIT, "scene has %u materials (max %d)", n_mats, SC_MAX_PRIMS);
@@ -73,14 +73,16 @@ static size_t mask_smem(uint32_t w, uint32_t h) {
     return words <= kMaxSmemMaskWords ? words * sizeof(uint32_t) : 0;
 }
 
-static int default_shape(sc_ctx* ctx, bool spectral, int aggregate, size_t smem, LaunchShape& s) {
+static int default_shape(sc_ctx* ctx, bool spectral, int aggregate, size_t smem, LaunchShape& s,
+                         uint32_t estimator = 0) {
     s.block = 256;
     s.aggregate = aggregate;
     s.minb = 4;
     if (const char* agg = std::getenv("SPECTRAL_CUDA_AGGREGATE")) s.aggregate = std::atoi(agg) ? 1 : 0;
     if (const char* mb = std::getenv("SPECTRAL_CUDA_MINB")) s.minb = std::atoi(mb) >= 5 ? 5 : 4;
     if (const char* sp = std::getenv("SPECTRAL_CUDA_SPLIT")) s.split = std::atoi(sp) ? 1 : 0;
-    const int per_sm = photon_occupancy_blocks(s, spectral, smem);
+    const int per_sm = estimator == 2u ? beam_occupancy_blocks(s, spectral, smem)
+                                       : photon_occupancy_blocks(s, spectral, smem);
     s.grid = (uint32_t)(ctx->sms * per_sm);
     return SC_OK;
 }
@@ -140,7 +142,8 @@ struct sc_photon_film {
         if (end <= base) return SC_OK;
         DeviceGuard g(ctx->device);
         PhotonParams p = params(base, end - base, s);
-        SC_CUDA(launch_photons(p, shape, stream));
+        if (opts.estimator == 2u) SC_CUDA(launch_beam(p, shape, stream));
+        else SC_CUDA(launch_photons(p, shape, stream));
         ++film_version;
         return SC_OK;
     }
@@ -319,7 +322,7 @@ int sc_photon_film_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_pri
     SC_REQUIRE(o.lambda_max > o.lambda_min, SC_E_INVALID, "empty band [%g, %g)", o.lambda_min, o.lambda_max);
     SC_REQUIRE(o.scale_log2 <= 50u, SC_E_INVALID, "scale_log2 %u > 50", o.scale_log2);
     SC_REQUIRE(o.max_bounces <= 64u, SC_E_LIMIT, "max_bounces %u > 64", o.max_bounces);
-    SC_REQUIRE(o.estimator <= 1u, SC_E_INVALID, "estimator %u", o.estimator);
+    SC_REQUIRE(o.estimator <= 2u, SC_E_INVALID, "estimator %u", o.estimator);
     (void)background;
     sc_photon_film* f = new sc_photon_film();
     f->ctx = ctx;
@@ -362,7 +365,7 @@ int sc_photon_film_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_pri
     if ((e = cudaMemsetAsync(f->surface.p, 0, f->surface.bytes(), f->stream)) != cudaSuccess) return fail(e);
     if ((e = cudaStreamSynchronize(f->stream)) != cudaSuccess) return fail(e);
     default_shape(ctx, o.bins != 0, 0, scene_smem_bytes(n_prims, n_planes, n_mats) + mask_smem(width, height),
-                  f->shape);
+                  f->shape, o.estimator);
     *out = f;
     return SC_OK;
     SC_GUARD_END
@@ -423,6 +426,7 @@ int sc_photon_film_trace_debug(sc_photon_film* f, uint32_t n, uint32_t seed, uin
     SC_GUARD_BEGIN
     FILM_LOCK(f);
     SC_REQUIRE(out || debug_count == 0, SC_E_INVALID, "null output");
+    SC_REQUIRE(f->opts.estimator != 2u, SC_E_STATE, "trace_debug records point-estimator paths only");
     const uint32_t count = std::min(debug_count, n);
     if (debug_count) std::memset(out, 0, (size_t)debug_count * sizeof(sc_debug_photon));
     if (count == 0) return SC_OK;
@@ -653,6 +657,7 @@ int sc_photon_film_trace_stats(sc_photon_film* f, uint32_t base, uint32_t count,
     SC_GUARD_BEGIN
     FILM_LOCK(f);
     SC_REQUIRE(out, SC_E_INVALID, "null output");
+    SC_REQUIRE(f->opts.estimator != 2u, SC_E_STATE, "trace_stats counts point-estimator work only");
     DevBuf<unsigned long long> d;
     SC_CUDA(d.alloc(4));
     SC_CUDA(cudaMemsetAsync(d.p, 0, 32, f->stream));
@@ -677,7 +682,8 @@ int sc_trace_photons_device(sc_ctx* ctx, const sc_trace_desc* d, uint32_t base, 
     SC_REQUIRE(d->width > 0 && d->height > 0, SC_E_INVALID, "empty film");
     sc_film_options o;
     resolve_options(&d->opts, o);
-    SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min, SC_E_INVALID, "bad film options");
+    SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min && o.estimator <= 2u, SC_E_INVALID,
+               "bad film options");
     DeviceGuard g(ctx->device);
     sc_photon_film tmp;  // parameter builder only; owns no device memory
     tmp.ctx = ctx; tmp.geom = film_geom(d->width, d->height, o.bins ? o.bins : 3u); tmp.opts = o;
@@ -690,8 +696,9 @@ int sc_trace_photons_device(sc_ctx* ctx, const sc_trace_desc* d, uint32_t base, 
     LaunchShape shape;
     default_shape(ctx, o.bins != 0, 0,
                   scene_smem_bytes(d->n_prims, d->n_planes, d->n_mats) + (flags_dev ? mask_smem(d->width, d->height) : 0),
-                  shape);
-    SC_CUDA(launch_photons(p, shape, static_cast<cudaStream_t>(stream)));
+                  shape, o.estimator);
+    if (o.estimator == 2u) SC_CUDA(launch_beam(p, shape, static_cast<cudaStream_t>(stream)));
+    else SC_CUDA(launch_photons(p, shape, static_cast<cudaStream_t>(stream)));
     return SC_OK;
     SC_GUARD_END
 }

@@ -49,6 +49,15 @@ cudaError_t launch_photon_debug(const PhotonParams& p, cudaStream_t s);
 cudaError_t launch_photon_count(const PhotonParams& p, unsigned long long* out, uint32_t grid, cudaStream_t s);
 int photon_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem);
 
+// Photon-beam estimator (beam.cu): same transport, each segment marched in
+// deterministic steps with an energy-conserving transverse tent splat.
+cudaError_t launch_beam(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s);
+int beam_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem);
+
+// Host-side scene validation shared by every entry point that uploads a scene.
+int check_scene(uint32_t n_prims, uint32_t n_planes, uint32_t n_mats, const sc_primitive* prims,
+                const sc_plane* planes, const sc_material* mats);
+
 struct RimParams {
     sc_camera cam;
     uint32_t width, height;

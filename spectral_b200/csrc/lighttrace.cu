@@ -161,16 +161,8 @@ __global__ void __launch_bounds__(256) zbuffer_kernel(sc_camera cam, uint32_t w,
 int upload_scene(const sc_primitive* prims, uint32_t np, const sc_plane* planes, uint32_t npl,
                  const sc_material* mats, uint32_t nm, DevBuf<sc_primitive>& dp, DevBuf<sc_plane>& dpl,
                  DevBuf<sc_material>& dm) {
-    SC_REQUIRE(np <= SC_MAX_PRIMS && npl <= SC_MAX_PLANES && nm <= SC_MAX_PRIMS, SC_E_LIMIT, "scene exceeds limits");
-    SC_REQUIRE((np == 0 || prims) && (npl == 0 || planes) && (nm == 0 || mats), SC_E_INVALID, "null scene array");
-    for (uint32_t i = 0; i < np; ++i) {
-        SC_REQUIRE(prims[i].kind <= 1u && prims[i].material < nm, SC_E_INVALID, "primitive %u invalid", i);
-        if (prims[i].kind == 1u)
-            SC_REQUIRE((uint64_t)prims[i].plane_start + prims[i].plane_count <= npl, SC_E_INVALID,
-                       "primitive %u plane range", i);
-    }
-    for (uint32_t i = 0; i < nm; ++i)
-        SC_REQUIRE(mats[i].kind <= 1u && (mats[i].kind == 0u || mats[i].glass <= 3u), SC_E_INVALID, "material %u", i);
+    const int rc = check_scene(np, npl, nm, prims, planes, mats);
+    if (rc != SC_OK) return rc;
     SC_CUDA(dp.alloc(np ? np : 1));
     SC_CUDA(dpl.alloc(npl ? npl : 1));
     SC_CUDA(dm.alloc(nm ? nm : 1));

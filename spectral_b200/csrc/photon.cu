@@ -25,28 +25,6 @@ __host__ __device__ __forceinline__ size_t split_offset(const PhotonParams& p, u
     return (b + 15u) & ~size_t(15);
 }
 
-// Stage the scene records and the CMF table in shared memory; when `mask_words`
-// is non-zero a zeroed dirty-tile bitmask of that many words follows them.
-__device__ __forceinline__ SceneView load_scene(const PhotonParams& p, unsigned char* smem, const float** cmf_out,
-                                                uint32_t** mask_out = nullptr, uint32_t mask_words = 0) {
-    sc_primitive* sp = reinterpret_cast<sc_primitive*>(smem);
-    sc_plane* spl = reinterpret_cast<sc_plane*>(sp + p.n_prims);
-    sc_material* sm = reinterpret_cast<sc_material*>(spl + p.n_planes);
-    float* scmf = reinterpret_cast<float*>(sm + p.n_mats);
-    uint32_t* mask = reinterpret_cast<uint32_t*>(scmf + 3 * kTableN);
-    for (uint32_t i = threadIdx.x; i < p.n_prims; i += blockDim.x) sp[i] = p.prims[i];
-    for (uint32_t i = threadIdx.x; i < p.n_planes; i += blockDim.x) spl[i] = p.planes[i];
-    for (uint32_t i = threadIdx.x; i < p.n_mats; i += blockDim.x) sm[i] = p.mats[i];
-    for (uint32_t i = threadIdx.x; i < 3u * kTableN; i += blockDim.x) scmf[i] = p.cmf[i];
-    for (uint32_t i = threadIdx.x; i < mask_words; i += blockDim.x) mask[i] = 0u;
-    __syncthreads();
-    *cmf_out = scmf;
-    if (mask_out) *mask_out = mask_words ? mask : nullptr;
-    SceneView S;
-    S.prims = sp; S.planes = spl; S.mats = sm; S.n_prims = p.n_prims;
-    return S;
-}
-
 // 256 threads per CTA; MINB CTAs per SM bound the registers (4: 63 registers,
 // no spills; 5: 48 registers, a few spills, more warps in flight).
 template <bool SPEC, int AGG, int MINB, bool SPLIT>

@@ -231,6 +231,14 @@ int sc_tracer_clear_accum(sc_tracer* t) {
     SC_GUARD_END
 }
 
+int sc_tracer_stream(sc_tracer* t, void** stream) {
+    SC_GUARD_BEGIN
+    SC_REQUIRE(t && stream, SC_E_INVALID, "null argument");
+    *stream = t->stream;
+    return SC_OK;
+    SC_GUARD_END
+}
+
 int sc_tracer_dims(sc_tracer* t, uint32_t* w, uint32_t* h) {
     SC_GUARD_BEGIN
     SC_REQUIRE(t, SC_E_INVALID, "null tracer");

@@ -14,7 +14,7 @@ import math
 
 import numpy as np
 
-from . import BK7, FUSED_SILICA, SF11, WATER, Beam, Camera, Dielectric, Scene, Screen
+from . import BK7, FUSED_SILICA, SF11, WATER, Beam, Camera, Dielectric, Lambertian, Scene, Screen
 
 
 def prism_planes(apex_deg, side, depth):
@@ -72,6 +72,18 @@ def prism_on_plane(width=800, height=600, floor_texels=512):
     beam = Beam((-3.0, 0.55, -0.75), (0.0, 0.0, 1.5), (0.0, 0.12, 0.0), (1.0, 0.0, 0.0))
     cam = Camera.look_at((0.0, 4.5, 9.0), (4.0, -1.2, 0.0), (0.0, 1.0, 0.0), 50.0, width / height)
     return scene, floor, beam, cam
+
+
+def tracer_workload(width=1280, height=720):
+    """Camera-tracer scene: SF11 prism (apex 60, side 1) on a diffuse ground
+    half-space (albedo 0.8, y = -0.6), lit by a spherical D65 emitter of radius
+    0.2 at (2, 3, 1); Russian roulette after 3 scatters.  Returns (scene,
+    camera, tracer keyword arguments)."""
+    scene = Scene(background=0.0)
+    scene.add_solid(prism_planes(60.0, 1.0, 1.0), Dielectric(SF11))
+    scene.add_solid([((0.0, 1.0, 0.0), 0.6)], Lambertian(0.8))
+    cam = Camera.look_at((0.5, 1.5, 5.0), (0.0, -0.3, 0.0), (0.0, 1.0, 0.0), 45.0, width / height)
+    return scene, cam, dict(emitter=((2.0, 3.0, 1.0), 0.2, 40.0), rr_start=3, max_depth=8)
 
 
 def rainbow_workload(width=1920, height=1080, beam_width=2.2):
