@@ -45,7 +45,18 @@ WORKLOADS = {
     # internal bounces (6 surface interactions), sigma_s 0.02, 1920x1080x64.
     "rainbow": dict(width=1920, height=1080, bins=64, photons=1 << 26, sigma_s=0.02, sigma_t=0.02, g=0.0,
                     lambda_min=380.0, lambda_max=780.0, max_dist=8.0, max_bounces=6, seed=0x8A1B),
+    # Photon-beam estimator (render_volumetric_scene) on the Dark-Side-of-the-Moon
+    # composition of spectral-core/examples/prism_dsotm.rs: 800x800 XYZ film,
+    # sigma_s 0.5, sigma_t 0.06, g 0.5, max_dist 14, seed 0xDED; 2^18 photons
+    # per step (the example traces 50 M in total).
+    "beam": dict(width=800, height=800, bins=0, photons=1 << 18, sigma_s=0.5, sigma_t=0.06, g=0.5,
+                 lambda_min=380.0, lambda_max=730.0, max_dist=14.0, max_bounces=8, seed=0xDED, scale_log2=40,
+                 estimator=2),
 }
+
+
+METRIC_POINT = "photons/s @<=0.5% film err (forward + volumetric single scatter)"
+METRIC_BEAM = "photons/s (forward + photon-beam estimator, volumetric single scatter)"
 
 
 def parse():
@@ -54,7 +65,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "tracer"], default="batch")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "serve", "tracer"], default="batch")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps")
@@ -67,6 +78,8 @@ def build_scene(wl):
     cfg = WORKLOADS[wl]
     if wl == "prism":
         return prism_workload(cfg["width"], cfg["height"])
+    if wl == "beam":
+        return sb.dsotm_scene(cfg["width"] / cfg["height"])
     return rainbow_workload(cfg["width"], cfg["height"])
 
 
@@ -85,22 +98,38 @@ def run_cpu(wl, seconds, threads=None):
     p = oracle.vol_params(cfg["width"], cfg["height"], cfg["seed"], cfg["sigma_s"], cfg["sigma_t"], cfg["g"],
                           cfg["max_dist"], cfg["max_bounces"], cfg["lambda_min"], cfg["lambda_max"], bins=cfg["bins"])
     threads = threads or os.cpu_count() or 1
-    film = np.zeros(cfg["width"] * cfg["height"] * cfg["bins"], np.int64)
-    fp = film.ctypes.data_as(C.POINTER(C.c_int64))
+    if cfg.get("estimator", 0) == 2:
+        # render_volumetric_scene: photon ranges on all host threads (ctypes
+        # releases the GIL), one f32 image per thread as the reference's loop
+        import concurrent.futures as cf
+        imgs = [np.zeros(3 * cfg["width"] * cfg["height"], np.float32) for _ in range(threads)]
+
+        def render(n):
+            def part(i):
+                lo, hi = n * i // threads, n * (i + 1) // threads
+                oracle.lib.or_render_beam(C.byref(osc.c), C.byref(oc), C.byref(ob), C.byref(p), None, lo, hi,
+                                          oracle.fp(imgs[i]))
+            with cf.ThreadPoolExecutor(threads) as ex:
+                list(ex.map(part, range(threads)))
+    else:
+        film = np.zeros(cfg["width"] * cfg["height"] * cfg["bins"], np.int64)
+        fp = film.ctypes.data_as(C.POINTER(C.c_int64))
+
+        def render(n):
+            oracle.lib.or_render_point_mt(C.byref(osc.c), C.byref(oc), C.byref(ob), C.byref(p), None, 0, n, None,
+                                          fp, threads)
     # calibrate on a small sample, then size the timed sample to ~`seconds`
-    n = 4096
+    n = 64 if cfg.get("estimator", 0) == 2 else 4096
     while True:
         t0 = time.perf_counter()
-        oracle.lib.or_render_point_mt(C.byref(osc.c), C.byref(oc), C.byref(ob), C.byref(p), None, 0, n, None, fp,
-                                      threads)
+        render(n)
         dt = time.perf_counter() - t0
         if dt > 0.5 or n >= cfg["photons"]:
             break
         n *= 4
     n_s = int(min(cfg["photons"], max(n, n * seconds / max(dt, 1e-6))))
-    film[:] = 0
     t0 = time.perf_counter()
-    oracle.lib.or_render_point_mt(C.byref(osc.c), C.byref(oc), C.byref(ob), C.byref(p), None, 0, n_s, None, fp, threads)
+    render(n_s)
     dt = time.perf_counter() - t0
     return n_s / dt, n_s, dt, threads
 
@@ -192,6 +221,8 @@ def run_gpu(args, rank, world, local_rank):
     ctx = sb.GpuContext(local_rank)
     scene, beam, cam = build_scene(args.workload)
     W, H, B, N = cfg["width"], cfg["height"], cfg["bins"], cfg["photons"]
+    CH = B or 3  # film channels: spectral bins, or the reference's XYZ film
+    SCALE, EST = cfg.get("scale_log2", 32), cfg.get("estimator", 0)
     prims, np_, planes, npl, mats, nm = scene.arrays()
 
     def dev_bytes(obj, n):
@@ -199,11 +230,11 @@ def run_gpu(args, rank, world, local_rank):
         return t
 
     d_prims, d_planes, d_mats = dev_bytes(prims, np_), dev_bytes(planes, npl), dev_bytes(mats, nm)
-    opts = _lib.sc_film_options(B, cfg["lambda_min"], cfg["lambda_max"], cfg["max_bounces"], 32, 0)
+    opts = _lib.sc_film_options(B, cfg["lambda_min"], cfg["lambda_max"], cfg["max_bounces"], SCALE, EST)
     desc = _lib.sc_trace_desc(d_prims.data_ptr(), np_, d_planes.data_ptr(), npl, d_mats.data_ptr(), nm, cam.c, beam.c,
                               _lib.sc_vol_weights(cfg["sigma_s"], cfg["sigma_t"], cfg["g"]), W, H, cfg["seed"], 1,
                               cfg["max_dist"], opts, None)
-    film = torch.zeros(_lib.lib.sc_film_bytes(W, H, B) // 8, dtype=torch.int64, device=dev)
+    film = torch.zeros(_lib.lib.sc_film_bytes(W, H, CH) // 8, dtype=torch.int64, device=dev)
     flags = torch.zeros(_lib.lib.sc_film_flag_bytes(W, H) // 4, dtype=torch.int32, device=dev)
     xyz = torch.empty(3 * W * H, dtype=torch.float32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
@@ -216,18 +247,27 @@ def run_gpu(args, rank, world, local_rank):
                                                     C.c_void_p(flags.data_ptr()), sp))
 
     def reduce():
-        _lib.check(_lib.lib.sc_sensor_reduce_device(ctx.h, W, H, B, cfg["lambda_min"], cfg["lambda_max"], 32,
+        _lib.check(_lib.lib.sc_sensor_reduce_device(ctx.h, W, H, CH, cfg["lambda_min"], cfg["lambda_max"], SCALE,
                                                     C.c_void_p(film.data_ptr()), C.c_void_p(flags.data_ptr()),
                                                     C.c_void_p(xyz.data_ptr()), 1, sp))
 
     # algorithmic work of one launch (instrumented pass, outside the timed region)
-    stats = torch.zeros(4, dtype=torch.int64, device=dev)
+    stats = torch.zeros(5, dtype=torch.int64, device=dev)
     _lib.check(_lib.lib.sc_trace_stats_device(ctx.h, C.byref(desc), base, N, C.c_void_p(stats.data_ptr()), sp))
-    photons, segments, splats, scatters = [int(x) for x in stats.cpu()]
+    if EST == 2:  # photons, segments, march steps, in-frame steps, footprint deposits
+        photons, segments, steps, in_frame, deposits = [int(x) for x in stats.cpu()]
+        splats, scatters = deposits, 0
+    else:
+        photons, segments, splats, scatters = [int(x) for x in stats.cpu()[:4]]
 
     for _ in range(args.warmup):
         trace()
         reduce()
+    # lit tiles of one pass (the drain reads and zeroes only those)
+    trace()
+    torch.cuda.synchronize()
+    dirty_tiles = int(np.unpackbits(flags.cpu().numpy().view(np.uint8)).sum())
+    reduce()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -261,7 +301,7 @@ def run_gpu(args, rank, world, local_rank):
     pf = sb.GpuPhotonFilm(ctx, scene, cam, beam, W, H, N, cfg["seed"], cfg["max_dist"],
                           sb.VolWeights(cfg["sigma_s"], cfg["sigma_t"], cfg["g"]), bins=B,
                           lambda_min=cfg["lambda_min"], lambda_max=cfg["lambda_max"],
-                          max_bounces=cfg["max_bounces"])
+                          max_bounces=cfg["max_bounces"], scale_log2=SCALE, estimator=EST)
     host_xyz = np.empty(3 * W * H, np.float32)
     h2d = C.sizeof(prims._type_) * np_ + C.sizeof(planes._type_) * npl + C.sizeof(mats._type_) * nm + \
         C.sizeof(cam.c) + C.sizeof(beam.c)
@@ -299,26 +339,39 @@ def run_gpu(args, rank, world, local_rank):
     hbm = hbm or 6650.0
     trace_s = statistics.mean(trace_ms) / 1e3
     reduce_s = statistics.mean(reduce_ms) / 1e3
-    # dominant kernel: the photon kernel.  Algorithmic bytes = one 8-byte
-    # fixed-point payload per in-frame haze sample (its film atomic).
-    alg_bytes = splats * 8
     cl = clk.summary()
     sm_mhz = cl["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     fp32_peak = sms * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
-    # counted FP32 work (exp/pow counted as one op each): emission 20, intersect
-    # 14 per plane per segment, 60 per haze sample, 45 per scatter
-    flops = photons * 20 + segments * 14 * npl + segments * 4 * 60 + scatters * 45
-    film_bytes = W * H * B * 8
+    if EST == 2:
+        # beam kernel: 8 B per film channel per footprint pixel deposited;
+        # counted FP32 work: emission 20, intersect 14 per plane per segment,
+        # 100 per in-frame march step (two projections, weight, radius), 16
+        # per footprint pixel (two tent evaluations), 45 per scatter (segments
+        # minus photons)
+        kname = "beam_kernel"
+        alg_bytes = deposits * 8 * CH
+        alg_note = "8 B x %d channels per footprint pixel: %d deposits per launch" % (CH, deposits)
+        flops = photons * 20 + segments * 14 * npl + in_frame * 100 + deposits * 16 + (segments - photons) * 45
+    else:
+        # photon kernel: one 8-byte fixed-point payload per in-frame haze
+        # sample (its film atomic); counted FP32 work (exp/pow one op each):
+        # emission 20, intersect 14 per plane per segment, 60 per haze sample,
+        # 45 per scatter
+        kname = "photon_kernel"
+        alg_bytes = splats * 8 * (1 if B else 3)
+        alg_note = "8 B per film channel per in-frame haze sample: %d samples per launch" % splats
+        flops = photons * 20 + segments * 14 * npl + segments * 4 * 60 + scatters * 45
+    lit_bytes = dirty_tiles * 64 * CH * 8
+    workload_txt = {"prism": "SF11 prism apex 60 side 1, beam 0.02 @45deg, 2^20 photons, 640x360x64 bins",
+                    "rainbow": "water sphere r=1, beam 2.2, 2^26 photons, 1920x1080x64 bins",
+                    "beam": "photon-beam estimator, DSOTM prism scene, 2^18 photons, 800x800 XYZ film"}
     line = {
-        "metric": "photons/s @<=0.5% film err (forward + volumetric single scatter)",
+        "metric": METRIC_BEAM if EST == 2 else METRIC_POINT,
         "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 transport, int64 fixed-point film", "data": "synthetic (seeded scene)",
-        "config": {"workload": "%s: %s" % (args.workload, {"prism": "SF11 prism apex 60 side 1, beam 0.02 @45deg, "
-                                                                     "2^20 photons, 640x360x64 bins",
-                                                           "rainbow": "water sphere r=1, beam 2.2, 2^26 photons, "
-                                                                      "1920x1080x64 bins"}[args.workload]),
+        "config": {"workload": "%s: %s" % (args.workload, workload_txt[args.workload]),
                    "photons_per_step": N * world, "film": [W, H, B], "band_nm": [cfg["lambda_min"], cfg["lambda_max"]],
                    "l2": "flushed between steps (256 MB write outside the timed events)",
                    "parallelism": "photon ranges per rank, no collective"},
@@ -326,19 +379,21 @@ def run_gpu(args, rank, world, local_rank):
                 "d2h_bytes_per_step": 3 * W * H * 4,
                 "path": "sc_photon_film_set_scene + dispatch + read_accum (host f32 XYZ) + clear"},
         "gpu_launches": args.steps * 2,
-        "kernels": {"photon_ms": statistics.mean(trace_ms), "reduce_ms": statistics.mean(reduce_ms)},
+        "kernels": {"trace_ms": statistics.mean(trace_ms), "reduce_ms": statistics.mean(reduce_ms)},
         "roofline": {"bound": "hbm", "achieved": alg_bytes / trace_s / 1e9, "peak": hbm, "unit": "GB/s",
-                     "frac": alg_bytes / trace_s / 1e9 / hbm, "traffic": None, "kernel": "photon_kernel",
-                     "peak_source": "%s hbm_gbs" % peak_note,
-                     "algorithmic": "8 B per in-frame haze sample: %d samples per launch" % splats},
-        "roofline_fp32": {"kernel": "photon_kernel", "counted_flops": flops, "achieved_tflops": flops / trace_s / 1e12,
+                     "frac": alg_bytes / trace_s / 1e9 / hbm, "traffic": None, "kernel": kname,
+                     "peak_source": "%s hbm_gbs" % peak_note, "algorithmic": alg_note},
+        "roofline_fp32": {"kernel": kname, "counted_flops": flops, "achieved_tflops": flops / trace_s / 1e12,
                           "peak_tflops": fp32_peak, "frac": flops / trace_s / 1e12 / fp32_peak,
                           "peak_source": "%d SMs x 128 FP32 lanes x 2 x %.0f MHz (sampled median)" % (sms, sm_mhz)},
         "roofline_reduce": {"kernel": "reduce_kernel (drain)", "bound": "hbm",
-                            "achieved": 2 * film_bytes / reduce_s / 1e9, "peak": hbm, "unit": "GB/s",
-                            "frac": 2 * film_bytes / reduce_s / 1e9 / hbm,
-                            "algorithmic": "read + zero the whole film (dirty tiles only are touched)"},
-        "work": {"photons": photons, "segments": segments, "in_frame_samples": splats, "scatters": scatters},
+                            "achieved": (2 * lit_bytes + 12 * W * H) / reduce_s / 1e9, "peak": hbm, "unit": "GB/s",
+                            "frac": (2 * lit_bytes + 12 * W * H) / reduce_s / 1e9 / hbm,
+                            "algorithmic": "read + zero the %d lit 8x8 tiles (%d B) + 12 B XYZ per pixel"
+                                           % (dirty_tiles, lit_bytes)},
+        "work": ({"photons": photons, "segments": segments, "march_steps": steps, "in_frame_steps": in_frame,
+                  "footprint_deposits": deposits} if EST == 2 else
+                 {"photons": photons, "segments": segments, "in_frame_samples": splats, "scatters": scatters}),
         "clocks": cl,
     }
     if world == 1 and not args.no_cpu_baseline:
@@ -513,6 +568,59 @@ def run_gpu_tracer(args, rank, world, local_rank):
     return line
 
 
+# Serving workload (config 5): Poisson arrivals at 200 req/s (a 15 s window of
+# the 60 s stream by default), prism scenes of the config-4 distribution,
+# 2^16-2^20 photons per frame, 30 % orbit sessions of 16-128 frames at 2 deg
+# per frame, 40 GB HBM budget.
+SERVE = dict(rate=200.0, seconds=15.0, budget_gb=40.0, seed=0x5E7E)
+
+
+def run_gpu_serve(args, rank, world, local_rank):
+    import torch
+    import spectral_b200 as sb
+    from spectral_b200.serve import Server, poisson_requests, run_plain_stream, run_stream
+    torch.cuda.set_device(local_rank)
+    ctx = sb.GpuContext(local_rank)
+    budget = int(SERVE["budget_gb"] * (1 << 30))
+    # warm-up: a short stream of other requests through both paths
+    warm = poisson_requests(SERVE["rate"], 0.5 * max(1, args.warmup), SERVE["seed"] ^ 0xA5A5 ^ rank)
+    srv = Server(ctx, budget_bytes=budget)
+    run_stream(srv, warm, want_image=True)
+    srv.close()
+    run_plain_stream(ctx, warm[:20])
+    stream = poisson_requests(SERVE["rate"], SERVE["seconds"], SERVE["seed"] + rank)
+    srv = Server(ctx, budget_bytes=budget)
+    uuid = "GPU-" + str(torch.cuda.get_device_properties(torch.device("cuda", local_rank)).uuid)
+    with ClockSampler(uuid) as clk:
+        served = run_stream(srv, stream, want_image=True)
+    srv.close()
+    plain = run_plain_stream(ctx, stream)
+    if rank != 0:
+        return None
+    frames = sum(s[2] for s in stream)
+    in_bytes = sum(C.sizeof(s[1]) for s in stream)
+    out_bytes = sum(3 * s[1].width * s[1].height * 4 for s in stream)
+    return {
+        "metric": "served photons/s with p50/p99 request latency (continuous batching vs plain per-request launch)",
+        "value": served["photons_per_s"] * world, "unit": "photons/s", "n_gpus": world, "steps": 1,
+        "warmup": args.warmup, "ms_per_step": served["wall_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 transport, int64 fixed-point film", "data": "synthetic (seeded stream)",
+        "config": {"workload": "serve: Poisson %.0f req/s for %.0f s (%d requests, %d frames), prism scenes of the "
+                               "batch distribution, 2^16-2^20 photons per frame, 30%% orbit sessions of 16-128 "
+                               "frames at 2 deg, %.0f GB budget" % (SERVE["rate"], SERVE["seconds"], len(stream),
+                                                                     frames, SERVE["budget_gb"]),
+                   "parallelism": "own request stream per rank, no collective",
+                   "timing": "host clock over the whole stream replayed in real time (one step = the stream)"},
+        "served": served, "plain_per_request": plain,
+        "served_over_plain": served["photons_per_s"] / plain["photons_per_s"],
+        "e2e": {"value": served["photons_per_s"] * world, "unit": "photons/s", "h2d_bytes_per_step": in_bytes,
+                "d2h_bytes_per_step": out_bytes,
+                "path": "sc_server_submit per request, sc_server_step, sc_server_poll with the XYZ image to host"},
+        "gpu_launches": served["steps"],
+        "clocks": clk.summary(),
+    }
+
+
 BATCH = dict(n_jobs=256, seed=0xB200, bins=32, lambda_min=380.0, lambda_max=780.0)
 
 
@@ -523,15 +631,16 @@ def batch_jobs(rank):
                              lambda_min=BATCH["lambda_min"], lambda_max=BATCH["lambda_max"]), prism_jobs
 
 
-def run_cpu_batch(seconds, threads=None, rank=0):
-    """Photons/s of the CPU restatement over a bounded sample of the batch.
-    Scenes are rendered in parallel, one host thread per scene with its own film
-    (the CPU oracle releases the GIL), taking scenes in job order and the first
-    2^18 photons of each, until `seconds` of wall time are used."""
+def run_cpu_batch(seconds, threads=None, rank=0, jobs=None):
+    """Photons/s of the CPU restatement over a bounded sample of the batch (or
+    of `jobs`).  Scenes are rendered in parallel, one host thread per scene with
+    its own film (the CPU oracle releases the GIL), taking scenes in job order
+    and the first 2^18 photons of each, until `seconds` of wall time are used."""
     import threading
     import oracle
-    specs, prism_jobs = batch_jobs(rank)
-    jobs = prism_jobs(specs)
+    if jobs is None:
+        specs, prism_jobs = batch_jobs(rank)
+        jobs = prism_jobs(specs)
     threads = threads or os.cpu_count() or 1
     per_job = 1 << 18
     lock = threading.Lock()
@@ -724,7 +833,20 @@ def main():
             return 0
         rates = []
         per_step = max(1.0, args.cpu_seconds / max(1, args.steps))
-        if args.workload == "tracer":
+        if args.workload == "serve":
+            from spectral_b200.serve import poisson_requests
+            reqs = [r[1] for r in poisson_requests(SERVE["rate"], SERVE["seconds"], SERVE["seed"])]
+            run_cpu_batch(0.5, jobs=reqs)
+            for _ in range(args.steps):
+                rate, n_s, dt, th, sc = run_cpu_batch(per_step, jobs=reqs)
+                rates.append((n_s, dt))
+            sample = ("per step the first frame (up to 2^18 photons) of the stream's requests in arrival order, "
+                      "one host thread per request, for ~%.1f s" % per_step)
+            metric = ("served photons/s with p50/p99 request latency (continuous batching vs plain per-request "
+                      "launch)")
+            cfg_line = {"workload": "serve (see the GPU arm)", "rate_per_s": SERVE["rate"],
+                        "seconds": SERVE["seconds"]}
+        elif args.workload == "tracer":
             run_cpu_tracer(0.5)
             for _ in range(args.steps):
                 rate, frames, dt, th = run_cpu_tracer(per_step)
@@ -750,13 +872,14 @@ def main():
                 rate, n_s, dt, th = run_cpu(args.workload, per_step)
                 rates.append((n_s, dt))
             sample = "per step the first %d photons of the workload" % rates[0][0]
-            metric = "photons/s @<=0.5% film err (forward + volumetric single scatter)"
+            metric = METRIC_BEAM if args.workload == "beam" else METRIC_POINT
             cfg_line = {"workload": args.workload, "photons_per_step": cfg["photons"],
                         "film": [cfg["width"], cfg["height"], cfg["bins"]]}
         tot_n, tot_t = sum(n for n, _ in rates), sum(t for _, t in rates)
         value = tot_n / tot_t
-        unit, what = ("samples/s", "CpuTracer::accumulate") if args.workload == "tracer" else \
-            ("photons/s", "render_volumetric_scene_point")
+        unit, what = {"tracer": ("samples/s", "CpuTracer::accumulate"),
+                      "beam": ("photons/s", "render_volumetric_scene (beam estimator)")}.get(
+            args.workload, ("photons/s", "render_volumetric_scene_point"))
         line = {"metric": metric, "value": value,
                 "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": tot_t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -772,8 +895,8 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = {"batch": run_gpu_batch, "tracer": run_gpu_tracer}.get(args.workload, run_gpu)(args, rank, world,
-                                                                                          local_rank)
+    line = {"batch": run_gpu_batch, "serve": run_gpu_serve, "tracer": run_gpu_tracer}.get(
+        args.workload, run_gpu)(args, rank, world, local_rank)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

@@ -257,8 +257,11 @@ size_t sc_film_bytes(uint32_t width, uint32_t height, uint32_t channels);
 size_t sc_film_flag_bytes(uint32_t width, uint32_t height);
 int sc_trace_photons_device(sc_ctx* ctx, const sc_trace_desc* desc, uint32_t photon_base,
                             uint32_t count, void* film_dev, uint32_t* flags_dev, void* stream);
-/* Work counters (see sc_photon_film_trace_stats) for a device-pointer desc;
- * out_dev: 4 uint64 on the device, accumulated into (zero it first). */
+/* Work counters for a device-pointer desc, accumulated into out_dev (device
+ * uint64, zero it first): point / isotropic estimators 4 counters (photons,
+ * segments, in-frame haze samples, scatters; see sc_photon_film_trace_stats),
+ * beam estimator 5 (photons, segments, march steps, in-frame steps, footprint
+ * pixels deposited). */
 int sc_trace_stats_device(sc_ctx* ctx, const sc_trace_desc* desc, uint32_t photon_base, uint32_t count,
                           uint64_t* out_dev, void* stream);
 /* Sensor reduction of a device film to interleaved f32 XYZ (3*w*h, device);

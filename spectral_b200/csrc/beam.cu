@@ -16,12 +16,16 @@
 // so per-photon work varies by three orders of magnitude.  Each warp traces 32
 // photons at a time and only records segments (origin, direction, step length,
 // power, M) in a per-warp shared-memory buffer; when the buffer fills (and when
-// the 32 photons are done) the warp marches all buffered steps as one flat list
-// -- lane t takes global step t, found by a binary search over the buffer's
-// prefix sums of M -- so lanes stay busy whatever the segment lengths.  Steps
-// next to each other in the list lie ~0.5 px apart on the same segment, so the
-// lanes of a warp deposit into overlapping footprints; the optional warp
-// aggregation merges equal film cells before the 64-bit atomics.
+// the 32 photons are done) the warp marches all buffered steps as one flat list:
+// 32 steps at a time are set up one per lane (step t found by a binary search
+// over the buffer's prefix sums of M), then each in-frame step is splatted by
+// the whole warp, lanes spread over its footprint box (the tent sum is added
+// up by the step's own lane during the setup, row by row like the reference).
+// Lanes stay converged whatever the segment lengths and footprint sizes, and
+// the 32 atomics of one warp instruction hit 32 distinct pixels.  Film width
+// and height are below 2^16 (the box corner is packed into one word).
+// |d| is d2 * rsqrt(d2) (within 2 ulp) and |d| / r a multiply by 1/r, so a
+// deposit can differ from the reference's in the last few bits.
 #include "photon_trace.cuh"
 
 namespace sc {
@@ -32,12 +36,30 @@ constexpr float kBeamRadius = 0.03f;  // R_BEAM (volume.rs:172)
 constexpr uint32_t kMaxSteps = 4096u;
 
 struct BeamSeg { f3 o, d; float ds, power; uint32_t m, lane; };
+// One march step ready to splat: footprint centre and 1 / radius in pixels,
+// the step's colour (XYZ film) or weight and bin (spectral film), the footprint
+// box [x0, x0 + bw) x [y0, y0 + bh), the warp's lane layout over it (`rows` rows
+// of bw lanes per pass; lane / bw = (lane * magic) >> 16) and the tent sum,
+// all worked out one step per lane so the warp-wide splat does no division.
+struct StepRec {
+    float cx, cy, inv_r, c0, c1, c2;
+    uint32_t bin, valid;  // valid: 0 none, 1 footprint, 2 whole colour on the centre pixel
+    uint32_t x0y0;        // x0 | y0 << 16
+    uint32_t box;         // bw | bh << 8 | rows << 16 | passes << 24 (bw, bh <= 49)
+    uint32_t magic;       // ceil(2^16 / bw)
+    float inv_wsum;       // 1 / sum of the tent over the box
+};
 constexpr uint32_t kBeamSegs = 64;
 struct alignas(16) BeamWarpSmem {
     BeamSeg seg[kBeamSegs];
     uint32_t start[kBeamSegs + 4];  // exclusive prefix of m; start[kBeamSegs] = total
     float4 payload[32];             // per-lane CMF (x, y, z) and bin of its photon
+    StepRec step[32];               // 32 march steps set up for splatting
 };
+
+// Work counters of an instrumented launch: segments, march steps, steps in
+// frame (and not occluded), footprint pixels deposited.
+struct BeamCounts { unsigned long long segments, steps, in_frame, deposits; };
 
 __host__ __device__ __forceinline__ size_t beam_offset(const PhotonParams& p, uint32_t mask_words) {
     const size_t b = p.n_prims * sizeof(sc_primitive) + p.n_planes * sizeof(sc_plane) +
@@ -66,53 +88,31 @@ __device__ __forceinline__ uint32_t march_count(const PhotonParams& p, f3 o, f3 
     return m < 1u ? 1u : (m > kMaxSteps ? kMaxSteps : m);
 }
 
-// splat_transverse (volume.rs:174-218): tent footprint renormalised over the
-// covered pixels; value = col * w (XYZ film) or weight * w into the bin.
-template <bool SPEC, int AGG>
-__device__ __forceinline__ void splat_transverse(const PhotonParams& p, uint32_t* smask, float s, float t, float c0,
-                                                 float c1, float c2, float weight, uint32_t bin, float radius_px) {
-    const float cx = s * (float)p.width - 0.5f;
-    const float cy = (1.0f - t) * (float)p.height - 0.5f;
-    const float r = fmaxf(radius_px, 0.5f);
-    const int wmax = (int)p.width - 1, hmax = (int)p.height - 1;
-    const int x0 = (int)fmaxf(floorf(cx - r), 0.0f);
-    const int x1 = min(max((int)ceilf(cx + r), 0), wmax);
-    const int y0 = (int)fmaxf(floorf(cy - r), 0.0f);
-    const int y1 = min(max((int)ceilf(cy + r), 0), hmax);
-    float wsum = 0.0f;
-    for (int py = y0; py <= y1; ++py)
-        for (int px = x0; px <= x1; ++px) {
-            const float dx = (float)px - cx, dy = (float)py - cy;
-            wsum += fmaxf(1.0f - sqrtf(dx * dx + dy * dy) / r, 0.0f);
-        }
-    if (wsum <= 0.0f) {
-        const int px = min(max((int)roundf(cx), 0), wmax), py = min(max((int)roundf(cy), 0), hmax);
-        deposit<SPEC, AGG>(p, smask, true, (uint32_t)px, (uint32_t)py, SPEC ? weight : 1.0f, c0, c1, c2, bin);
-        return;
-    }
-    const float inv = 1.0f / wsum;
-    for (int py = y0; py <= y1; ++py)
-        for (int px = x0; px <= x1; ++px) {
-            const float dx = (float)px - cx, dy = (float)py - cy;
-            const float w = fmaxf(1.0f - sqrtf(dx * dx + dy * dy) / r, 0.0f) * inv;
-            deposit<SPEC, AGG>(p, smask, w > 0.0f, (uint32_t)px, (uint32_t)py, SPEC ? weight * w : w, c0, c1, c2,
-                               bin);
-        }
+// Tent weight max(1 - |d| / r, 0); the division is a multiply by 1/r (within
+// an ulp of the reference's quotient).
+__device__ __forceinline__ float tent(float dx2, float dy, float inv_r) {
+    const float d2 = dx2 + dy * dy;
+    const float d = d2 > 0.0f ? d2 * rsqrtf(d2) : 0.0f;  // |d| within 2 ulp
+    return fmaxf(1.0f - d * inv_r, 0.0f);
 }
 
-// One march step k of a buffered segment (volume.rs:268-307).
-template <bool SPEC, int AGG>
-__device__ __forceinline__ void beam_step(const PhotonParams& p, uint32_t* smask, const BeamSeg& B, float4 pay,
-                                          uint32_t k) {
+// Per-step setup (volume.rs:268-300), one lane per step: the step point, its
+// projection, z-test, camera-connection weight and projected beam radius.
+template <bool SPEC, bool COUNT>
+__device__ __forceinline__ StepRec beam_step(const PhotonParams& p, const BeamSeg& B, float4 pay, uint32_t k,
+                                             BeamCounts& cnt) {
+    StepRec R;
+    R.valid = 0u;
     const float dist = ((float)k + 0.5f) * B.ds;
     const f3 q = add(B.o, mul(B.d, dist));
     float s, t;
-    if (!project(p.proj, q, s, t)) return;
+    if (!project(p.proj, q, s, t)) return R;
     const uint32_t px = min((uint32_t)(s * (float)p.width), p.width - 1u);
     const uint32_t py = min((uint32_t)((1.0f - t) * (float)p.height), p.height - 1u);
     const f3 to = sub(p.proj.o, q);
     const float dd = fmaxf(length(to), 1e-3f);
-    if (p.zbuf && !(dd < p.zbuf[py * p.width + px])) return;
+    if (p.zbuf && !(dd < p.zbuf[py * p.width + px])) return R;
+    if (COUNT) ++cnt.in_frame;
     const f3 view = vdiv(to, dd);
     const float phase = phase_hg(p.g, dot(B.d, view));
     const float trans = expf(-p.sigma_t * dd);
@@ -125,14 +125,108 @@ __device__ __forceinline__ void beam_step(const PhotonParams& p, uint32_t* smask
         const float dpx = (s2 - s) * (float)p.width, dpy = (t2 - t) * (float)p.height;
         radius = fminf(fmaxf(sqrtf(dpx * dpx + dpy * dpy), 1.5f), 24.0f);
     }
-    float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
-    if (!SPEC) { c0 = pay.x * weight; c1 = pay.y * weight; c2 = pay.z * weight; }
-    splat_transverse<SPEC, AGG>(p, smask, s, t, c0, c1, c2, weight, __float_as_uint(pay.w), radius);
+    // splat_transverse (volume.rs:174-186): centre, radius and box in pixels
+    R.cx = s * (float)p.width - 0.5f;
+    R.cy = (1.0f - t) * (float)p.height - 0.5f;
+    const float r = fmaxf(radius, 0.5f);
+    R.inv_r = 1.0f / r;
+    const int x0 = (int)fmaxf(floorf(R.cx - r), 0.0f);
+    const int x1 = min(max((int)ceilf(R.cx + r), 0), (int)p.width - 1);
+    const int y0 = (int)fmaxf(floorf(R.cy - r), 0.0f);
+    const int y1 = min(max((int)ceilf(R.cy + r), 0), (int)p.height - 1);
+    const uint32_t bw = (uint32_t)(x1 - x0 + 1), bh = (uint32_t)(y1 - y0 + 1);
+    R.x0y0 = (uint32_t)x0 | ((uint32_t)y0 << 16);
+    const uint32_t rows = bw <= 32u ? 32u / bw : 1u;
+    R.box = bw | (bh << 8) | (rows << 16) | (((bh + rows - 1u) / rows) << 24);
+    R.magic = (65536u + bw - 1u) / bw;
+    if (SPEC) { R.c0 = weight; R.c1 = R.c2 = 0.0f; }
+    else { R.c0 = pay.x * weight; R.c1 = pay.y * weight; R.c2 = pay.z * weight; }
+    R.bin = __float_as_uint(pay.w);
+    // the tent sum over the box, row by row as the reference adds it
+    float wsum = 0.0f;
+    for (int py = y0; py <= y1; ++py) {
+        const float dy = (float)py - R.cy;
+        for (int px = x0; px <= x1; ++px) {
+            const float dx = (float)px - R.cx;
+            wsum += tent(dx * dx, dy, R.inv_r);
+        }
+    }
+    R.valid = wsum > 0.0f ? 1u : 2u;
+    R.inv_wsum = wsum > 0.0f ? 1.0f / wsum : 0.0f;
+    return R;
 }
 
-// March every step of the n buffered segments as one flat list.
-template <bool SPEC, int AGG>
-__device__ __forceinline__ void beam_flush(const PhotonParams& p, BeamWarpSmem& ws, uint32_t n, uint32_t* smask) {
+// Add one footprint pixel's share (w = tent / wsum) to the film.
+template <bool SPEC>
+__device__ __forceinline__ void deposit_pixel(const PhotonParams& p, uint32_t px, uint32_t py, const StepRec& R,
+                                              float w) {
+    unsigned long long* c = p.film + film_cell(px, py, p.tiles_x, p.channels);
+    if (SPEC) {
+        red_u64(c + R.bin, to_fixed(R.c0 * w, p.scale));
+    } else {
+        red_u64(c, to_fixed(R.c0 * w, p.scale));
+        red_u64(c + 1, to_fixed(R.c1 * w, p.scale));
+        red_u64(c + 2, to_fixed(R.c2 * w, p.scale));
+    }
+}
+
+// splat_transverse (volume.rs:174-218) by the whole warp, its tent sum already
+// known: lanes cover the footprint box (rows packed 32 / width at a time, or
+// 32-column chunks of one row for boxes wider than 32) and deposit their pixels'
+// renormalised shares; tiles under the box are marked dirty once.
+template <bool SPEC, bool COUNT>
+__device__ __forceinline__ void splat_warp(const PhotonParams& p, uint32_t* smask, const StepRec& R, uint32_t lane,
+                                           BeamCounts& cnt) {
+    const float cx = R.cx, cy = R.cy;
+    if (R.valid == 2u) {  // empty tent sum: the whole colour to the centre pixel
+        if (lane == 0) {
+            const uint32_t px = (uint32_t)min(max((int)roundf(cx), 0), (int)p.width - 1);
+            const uint32_t py = (uint32_t)min(max((int)roundf(cy), 0), (int)p.height - 1);
+            if (COUNT) { ++cnt.deposits; return; }
+            mark_tile(p, smask, film_tile(px, py, p.tiles_x));
+            deposit_pixel<SPEC>(p, px, py, R, 1.0f);
+        }
+        return;
+    }
+    const uint32_t x0y0 = R.x0y0, box = R.box;
+    const int x0 = (int)(x0y0 & 0xFFFFu), y0 = (int)(x0y0 >> 16);
+    const int bw = (int)(box & 0xFFu), bh = (int)((box >> 8) & 0xFFu), rows = (int)((box >> 16) & 0xFFu);
+    const int x1 = x0 + bw - 1, y1 = y0 + bh - 1;
+    const float inv_r = R.inv_r, inv = R.inv_wsum;
+    if (!COUNT) {  // tiles under the box: its corners' tiles when it spans <= 2 per axis
+        const int tx0 = x0 >> 3, ty0 = y0 >> 3, tx1 = x1 >> 3, ty1 = y1 >> 3;
+        if (tx1 - tx0 <= 1 && ty1 - ty0 <= 1) {
+            if (lane < 4u)
+                mark_tile(p, smask, (uint32_t)(((lane & 2u) ? ty1 : ty0) * (int)p.tiles_x + ((lane & 1u) ? tx1 : tx0)));
+        } else {
+            const int ntx = tx1 - tx0 + 1, nt = ntx * (ty1 - ty0 + 1);
+            for (int i = (int)lane; i < nt; i += 32)
+                mark_tile(p, smask, (uint32_t)((ty0 + i / ntx) * (int)p.tiles_x + tx0 + i % ntx));
+        }
+    }
+    const int lrow = bw <= 32 ? (int)((lane * R.magic) >> 16) : 0;
+    const int lcol = (int)lane - lrow * bw;
+    if (lrow >= rows) return;
+    const int chunks = bw <= 32 ? 1 : (bw + 31) / 32;
+    for (int ch = 0; ch < chunks; ++ch) {
+        const int px = x0 + ch * 32 + lcol;
+        if (px > x1) break;
+        const float dx = (float)px - cx, dx2 = dx * dx;
+        for (int py = y0 + lrow; py <= y1; py += rows) {
+            const float w = tent(dx2, (float)py - cy, inv_r) * inv;
+            if (w > 0.0f) {
+                if (COUNT) ++cnt.deposits;
+                else deposit_pixel<SPEC>(p, (uint32_t)px, (uint32_t)py, R, w);
+            }
+        }
+    }
+}
+
+// March every step of the n buffered segments as one flat list: 32 steps at a
+// time are set up one per lane, then splatted one at a time by the whole warp.
+template <bool SPEC, bool COUNT>
+__device__ __forceinline__ void beam_flush(const PhotonParams& p, BeamWarpSmem& ws, uint32_t n, uint32_t* smask,
+                                           BeamCounts& cnt) {
     const uint32_t lane = threadIdx.x & 31u;
     __syncwarp();
     const uint32_t m0 = lane < n ? ws.seg[lane].m : 0u;
@@ -149,23 +243,39 @@ __device__ __forceinline__ void beam_flush(const PhotonParams& p, BeamWarpSmem& 
     if (lane == 0) ws.start[kBeamSegs] = tot0 + tot1;
     __syncwarp();
     const uint32_t total = tot0 + tot1;
-    for (uint32_t t = lane; t < total; t += 32u) {
-        uint32_t lo = 0, hi = n;  // start[lo] <= t < start[hi]
-        while (hi - lo > 1u) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (ws.start[mid] <= t) lo = mid; else hi = mid;
+    if (COUNT && lane == 0) { cnt.segments += n; cnt.steps += total; }
+    for (uint32_t t0 = 0; t0 < total; t0 += 32u) {
+        const uint32_t t = t0 + lane;
+        StepRec R;
+        R.valid = 0u;
+        if (t < total) {
+            uint32_t lo = 0, hi = n;  // start[lo] <= t < start[hi]
+            while (hi - lo > 1u) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (ws.start[mid] <= t) lo = mid; else hi = mid;
+            }
+            const BeamSeg B = ws.seg[lo];
+            R = beam_step<SPEC, COUNT>(p, B, ws.payload[B.lane], t - ws.start[lo], cnt);
         }
-        const BeamSeg B = ws.seg[lo];
-        beam_step<SPEC, AGG>(p, smask, B, ws.payload[B.lane], t - ws.start[lo]);
+        ws.step[lane] = R;
+        unsigned todo = __ballot_sync(0xffffffffu, R.valid != 0u);
+        __syncwarp();
+        while (todo) {
+            const uint32_t j = __ffs(todo) - 1u;
+            todo &= todo - 1u;
+            const StepRec& Rj = ws.step[j];  // fields read from shared memory as used
+            splat_warp<SPEC, COUNT>(p, smask, Rj, lane, cnt);
+        }
+        __syncwarp();
     }
-    __syncwarp();
 }
 
 // 32 photons of one warp (lane = photon): transport with segments recorded,
 // then marched by beam_flush.
-template <bool SPEC, int AGG>
+template <bool SPEC, bool COUNT>
 __device__ __forceinline__ void trace_beam_warp(const PhotonParams& p, const SceneView& S, const float* cmf,
-                                                uint32_t idx, bool valid, uint32_t* smask, BeamWarpSmem& ws) {
+                                                uint32_t idx, bool valid, uint32_t* smask, BeamWarpSmem& ws,
+                                                BeamCounts& cnt) {
     const uint32_t lane = threadIdx.x & 31u;
     Rng r = Rng::make(idx, p.seed);
     const float r1 = r.f32();
@@ -186,7 +296,7 @@ __device__ __forceinline__ void trace_beam_warp(const PhotonParams& p, const Sce
         // one flush site (keeps beam_flush inlined): when the buffer cannot take
         // another 32 segments, and once when the 32 photons are done
         if (n > kBeamSegs - 32u || (!live && n)) {
-            beam_flush<SPEC, AGG>(p, ws, n, smask);
+            beam_flush<SPEC, COUNT>(p, ws, n, smask, cnt);
             n = 0;
         }
         if (!live) break;
@@ -225,8 +335,8 @@ __device__ __forceinline__ void trace_beam_warp(const PhotonParams& p, const Sce
     }
 }
 
-template <bool SPEC, int AGG>
-__global__ void __launch_bounds__(256, 4) beam_kernel(const PhotonParams p, uint32_t mask_words) {
+template <bool SPEC>
+__global__ void __launch_bounds__(256, 3) beam_kernel(const PhotonParams p, uint32_t mask_words) {
     extern __shared__ __align__(16) unsigned char smem[];
     const float* cmf;
     uint32_t* smask;
@@ -234,9 +344,10 @@ __global__ void __launch_bounds__(256, 4) beam_kernel(const PhotonParams p, uint
     BeamWarpSmem* ws = reinterpret_cast<BeamWarpSmem*>(smem + beam_offset(p, mask_words));
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    BeamCounts cnt = {0, 0, 0, 0};
     for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < p.photon_count; base += warps * 32u)
-        trace_beam_warp<SPEC, AGG>(p, S, cmf, p.photon_base + base + lane, base + lane < p.photon_count, smask,
-                                   ws[warp]);
+        trace_beam_warp<SPEC, false>(p, S, cmf, p.photon_base + base + lane, base + lane < p.photon_count, smask,
+                                          ws[warp], cnt);
     if (smask) {
         __syncthreads();
         for (uint32_t w = threadIdx.x; w < mask_words; w += blockDim.x)
@@ -244,12 +355,33 @@ __global__ void __launch_bounds__(256, 4) beam_kernel(const PhotonParams p, uint
     }
 }
 
+// Instrumented pass: same transport and march, no film writes; sums the work
+// counters into out[0..4] = photons, segments, steps, in-frame steps, deposits.
+__global__ void __launch_bounds__(256, 3) beam_count_kernel(const PhotonParams p, unsigned long long* out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const float* cmf;
+    const SceneView S = load_scene(p, smem, &cmf);
+    BeamWarpSmem* ws = reinterpret_cast<BeamWarpSmem*>(smem + beam_offset(p, 0));
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    BeamCounts cnt = {0, 0, 0, 0};
+    unsigned long long ph = 0;
+    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < p.photon_count; base += warps * 32u) {
+        trace_beam_warp<false, true>(p, S, cmf, p.photon_base + base + lane, base + lane < p.photon_count, nullptr,
+                                        ws[warp], cnt);
+        ph += base + lane < p.photon_count;
+    }
+    unsigned long long v[5] = {ph, cnt.segments, cnt.steps, cnt.in_frame, cnt.deposits};
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
+        if (lane == 0 && v[i]) atomicAdd(out + i, v[i]);
+    }
+}
+
 using BeamKernelFn = void (*)(const PhotonParams, uint32_t);
 
-BeamKernelFn beam_fn(bool spec, int agg) {
-    if (spec) return agg ? beam_kernel<true, 1> : beam_kernel<true, 0>;
-    return agg ? beam_kernel<false, 1> : beam_kernel<false, 0>;
-}
+BeamKernelFn beam_fn(bool spec) { return spec ? beam_kernel<true> : beam_kernel<false>; }
 
 size_t beam_smem(const PhotonParams& p, uint32_t mask_words) {
     return beam_offset(p, mask_words) + 8 * sizeof(BeamWarpSmem);
@@ -259,11 +391,22 @@ size_t beam_smem(const PhotonParams& p, uint32_t mask_words) {
 
 int beam_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem) {
     int n = 0;
-    const void* fn = reinterpret_cast<const void*>(beam_fn(spectral, shape.aggregate));
+    const void* fn = reinterpret_cast<const void*>(beam_fn(spectral));
     const size_t total = smem + 16 + 8 * sizeof(BeamWarpSmem);
     if (total > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)shape.block, total) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
+}
+
+cudaError_t launch_beam_count(const PhotonParams& p, unsigned long long* out, uint32_t grid, cudaStream_t s) {
+    if (p.photon_count == 0) return cudaSuccess;
+    const uint32_t need = (p.photon_count + 255u) / 256u;
+    const size_t smem = beam_smem(p, 0);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(reinterpret_cast<const void*>(beam_count_kernel),
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    beam_count_kernel<<<need < grid ? need : grid, 256, smem, s>>>(p, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_beam(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s) {
@@ -272,7 +415,7 @@ cudaError_t launch_beam(const PhotonParams& p, const LaunchShape& shape, cudaStr
     const bool spec = p.channels != 3u || p.bins != 0u;
     const uint32_t need = (p.photon_count + 255u) / 256u;
     const uint32_t grid = need < shape.grid ? need : shape.grid;
-    beam_fn(spec, shape.aggregate)<<<grid, 256, beam_smem(p, mw), s>>>(p, mw);
+    beam_fn(spec)<<<grid, 256, beam_smem(p, mw), s>>>(p, mw);
     return cudaGetLastError();
 }
 

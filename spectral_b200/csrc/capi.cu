@@ -323,6 +323,8 @@ int sc_photon_film_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_pri
     SC_REQUIRE(o.scale_log2 <= 50u, SC_E_INVALID, "scale_log2 %u > 50", o.scale_log2);
     SC_REQUIRE(o.max_bounces <= 64u, SC_E_LIMIT, "max_bounces %u > 64", o.max_bounces);
     SC_REQUIRE(o.estimator <= 2u, SC_E_INVALID, "estimator %u", o.estimator);
+    SC_REQUIRE(o.estimator != 2u || (width < 65536u && height < 65536u), SC_E_LIMIT,
+               "beam estimator films are below 65536 pixels per side");
     (void)background;
     sc_photon_film* f = new sc_photon_film();
     f->ctx = ctx;
@@ -684,6 +686,8 @@ int sc_trace_photons_device(sc_ctx* ctx, const sc_trace_desc* d, uint32_t base, 
     resolve_options(&d->opts, o);
     SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min && o.estimator <= 2u, SC_E_INVALID,
                "bad film options");
+    SC_REQUIRE(o.estimator != 2u || (d->width < 65536u && d->height < 65536u), SC_E_LIMIT,
+               "beam estimator films are below 65536 pixels per side");
     DeviceGuard g(ctx->device);
     sc_photon_film tmp;  // parameter builder only; owns no device memory
     tmp.ctx = ctx; tmp.geom = film_geom(d->width, d->height, o.bins ? o.bins : 3u); tmp.opts = o;
@@ -711,6 +715,8 @@ int sc_trace_stats_device(sc_ctx* ctx, const sc_trace_desc* d, uint32_t base, ui
                "scene exceeds limits");
     sc_film_options o;
     resolve_options(&d->opts, o);
+    SC_REQUIRE(o.estimator != 2u || (d->width < 65536u && d->height < 65536u), SC_E_LIMIT,
+               "beam estimator films are below 65536 pixels per side");
     DeviceGuard g(ctx->device);
     sc_photon_film tmp;
     tmp.ctx = ctx; tmp.geom = film_geom(d->width, d->height, o.bins ? o.bins : 3u); tmp.opts = o;
@@ -719,8 +725,12 @@ int sc_trace_stats_device(sc_ctx* ctx, const sc_trace_desc* d, uint32_t base, ui
     tmp.n_prims = d->n_prims; tmp.n_planes = d->n_planes; tmp.n_mats = d->n_mats;
     PhotonParams p = tmp.params(base, count, d->seed);
     p.prims = d->prims; p.planes = d->planes; p.mats = d->mats; p.zbuf = d->zbuffer;
-    SC_CUDA(launch_photon_count(p, reinterpret_cast<unsigned long long*>(out_dev), (uint32_t)ctx->sms * 8u,
-                                static_cast<cudaStream_t>(stream)));
+    if (o.estimator == 2u)
+        SC_CUDA(launch_beam_count(p, reinterpret_cast<unsigned long long*>(out_dev), (uint32_t)ctx->sms * 4u,
+                                  static_cast<cudaStream_t>(stream)));
+    else
+        SC_CUDA(launch_photon_count(p, reinterpret_cast<unsigned long long*>(out_dev), (uint32_t)ctx->sms * 8u,
+                                    static_cast<cudaStream_t>(stream)));
     return SC_OK;
     SC_GUARD_END
 }

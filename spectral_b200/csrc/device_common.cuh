@@ -231,6 +231,8 @@ __device__ __forceinline__ float phase_hg(float g, float cos_theta) {
 __device__ __forceinline__ unsigned long long to_fixed(float x, float scale) {
     float y = x * scale;
     if (!(y > 0.0f)) return 0ull;
+    // below 2^31 the 32-bit conversion rounds identically and is cheaper
+    if (y < 2147483648.0f) return (unsigned long long)(unsigned)__float2int_rn(y);
     y = fminf(y, 4.0e18f);
     return (unsigned long long)__float2ll_rn(y);
 }

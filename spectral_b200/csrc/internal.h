@@ -53,6 +53,8 @@ int photon_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem
 // deterministic steps with an energy-conserving transverse tent splat.
 cudaError_t launch_beam(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s);
 int beam_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem);
+// Instrumented beam pass: out[0..4] += photons, segments, steps, in-frame steps, deposits.
+cudaError_t launch_beam_count(const PhotonParams& p, unsigned long long* out, uint32_t grid, cudaStream_t s);
 
 // Host-side scene validation shared by every entry point that uploads a scene.
 int check_scene(uint32_t n_prims, uint32_t n_planes, uint32_t n_mats, const sc_primitive* prims,

@@ -101,8 +101,69 @@ def poisson_requests(rate=200.0, seconds=60.0, seed=0x5E7E, session_share=0.3, f
     return out
 
 
-def run_stream(server, stream, time_scale=1.0, idle_sleep=2e-4):
-    """Replay `stream` in real time against `server`; returns a metrics dict."""
+def orbit_camera(job, frame, deg, target=ORBIT_TARGET, up=(0.0, 1.0, 0.0), vfov=42.0):
+    """Camera of frame `frame` of an orbit session, as the server builds it: the
+    job camera's origin rotated about the vertical axis through `target` by
+    deg * frame (f32 offsets, rotation in double, rounded to f32), then
+    Camera::look_at."""
+    from . import Camera
+    if deg == 0.0 or frame == 0:
+        return job.cam
+    a = deg * frame * math.pi / 180.0
+    ox, oy, oz = job.cam.origin
+    tx, _, tz = target
+    dx, dz = float(np.float32(ox) - np.float32(tx)), float(np.float32(oz) - np.float32(tz))
+    o = (float(np.float32(float(np.float32(tx)) + dx * math.cos(a) + dz * math.sin(a))), float(oy),
+         float(np.float32(float(np.float32(tz)) - dx * math.sin(a) + dz * math.cos(a))))
+    return Camera.look_at(o, target, up, vfov, float(np.float32(job.width) / np.float32(job.height))).c
+
+
+def run_plain_stream(ctx, stream, time_scale=1.0):
+    """The same stream served the plain way, one request at a time in arrival
+    order, each through its own GpuPhotonFilm-shaped object: create the film,
+    per frame set the camera, trace the frame's photon range, read the XYZ image
+    back to the host and clear; destroy.  Returns the metrics of run_stream."""
+    t0 = time.perf_counter()
+    lat, ttff, photons = [], [], 0
+    for arrival, job, nf, orbit in stream:
+        now = time.perf_counter() - t0
+        if now < arrival * time_scale:
+            time.sleep(arrival * time_scale - now)
+        f = C.c_void_p()
+        host = np.empty(3 * job.width * job.height, np.float32)
+        check(lib.sc_photon_film_create(ctx.h, job.prims, job.n_prims, job.planes, job.n_planes, job.mats,
+                                        job.n_mats, 0.0, C.byref(job.cam), C.byref(job.beam), job.width, job.height,
+                                        job.n_photons, job.seed, job.max_dist, C.byref(job.weights), None,
+                                        C.byref(job.opts), C.byref(f)))
+        try:
+            check(lib.sc_photon_film_set_spectral(f, int(job.spectral)))
+            n = job.n_photons
+            for fr in range(nf):
+                if orbit:
+                    cam = orbit_camera(job, fr, orbit)
+                    check(lib.sc_photon_film_set_camera(f, C.byref(cam)))
+                check(lib.sc_photon_film_dispatch(f, fr * n, (fr + 1) * n, job.seed))
+                check(lib.sc_photon_film_read_accum(f, host.ctypes.data_as(C.POINTER(C.c_float))))
+                check(lib.sc_photon_film_clear(f))
+                if fr == 0:
+                    ttff.append(time.perf_counter() - t0 - arrival * time_scale)
+                photons += n
+        finally:
+            lib.sc_photon_film_destroy(f)
+        lat.append(time.perf_counter() - t0 - arrival * time_scale)
+    wall = time.perf_counter() - t0
+    lat, ttff = np.array(lat), np.array(ttff)
+    return dict(requests=len(stream), wall_s=wall, steps=len(stream), photons=photons, photons_per_s=photons / wall,
+                p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
+                p50_first_frame_ms=float(np.percentile(ttff, 50) * 1e3),
+                p99_first_frame_ms=float(np.percentile(ttff, 99) * 1e3))
+
+
+def run_stream(server, stream, time_scale=1.0, idle_sleep=2e-4, want_image=False):
+    """Replay `stream` in real time against `server`; returns a metrics dict.
+    Latencies come from the server's own timestamps (submit to last frame
+    done), or with `want_image` from the host clock (arrival to the XYZ image
+    in host memory)."""
     t0 = time.perf_counter()
     k, done, lat, ttff = 0, 0, [], []
     pending = {}
@@ -110,9 +171,9 @@ def run_stream(server, stream, time_scale=1.0, idle_sleep=2e-4):
     while done < len(stream):
         now = time.perf_counter() - t0
         while k < len(stream) and stream[k][0] * time_scale <= now:
-            _, job, nf, orbit = stream[k]
+            arrival, job, nf, orbit = stream[k]
             rid = server.submit(job, nf, orbit)
-            pending[rid] = nf
+            pending[rid] = arrival * time_scale
             k += 1
         st = server.stats()
         if st["queued"] or st["active"]:
@@ -121,13 +182,13 @@ def run_stream(server, stream, time_scale=1.0, idle_sleep=2e-4):
         elif k < len(stream):
             time.sleep(min(idle_sleep, max(0.0, stream[k][0] * time_scale - now)))
         while True:
-            r = server.poll(want_image=False)
+            r = server.poll(want_image=want_image)
             if r is None:
                 break
             rid, _, (ts, ta, tf, td) = r
-            lat.append(td - ts)
+            arrived = pending.pop(rid, None)
+            lat.append(time.perf_counter() - t0 - arrived if want_image else td - ts)
             ttff.append(tf - ts)
-            pending.pop(rid, None)
             done += 1
     wall = time.perf_counter() - t0
     photons = server.stats()["photons"] - photons0

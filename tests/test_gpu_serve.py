@@ -11,7 +11,7 @@ import oracle
 import spectral_b200 as sb
 from spectral_b200 import _lib
 from spectral_b200.batch import prism_job
-from spectral_b200.serve import ORBIT_TARGET, Server, poisson_requests, run_stream
+from spectral_b200.serve import ORBIT_TARGET, Server, orbit_camera, poisson_requests, run_plain_stream, run_stream
 
 from helpers import rel_l1
 
@@ -48,17 +48,6 @@ def oracle_image(j, photon_begin, photon_end, cam=None):
     _, _, fs = oracle.render_point(sc, oc, ob, p, photon_begin, photon_end, f32=False, xyz=False, spec=True)
     w = oracle.bin_weights(o.bins, o.lambda_min, o.lambda_max).astype(np.float64)
     return (fs.reshape(-1, o.bins).astype(np.float64) @ w.T).reshape(-1) * 2.0 ** -32
-
-
-def orbit_camera(j, frame, deg):
-    a = deg * frame * math.pi / 180.0
-    ox, oy, oz = j.cam.origin
-    tx, ty, tz = ORBIT_TARGET
-    # f32 differences, rotation in double, rounded to f32 (as the server does)
-    dx, dz = float(np.float32(ox) - np.float32(tx)), float(np.float32(oz) - np.float32(tz))
-    o = (float(np.float32(float(np.float32(tx)) + dx * math.cos(a) + dz * math.sin(a))), float(oy),
-         float(np.float32(float(np.float32(tz)) - dx * math.sin(a) + dz * math.cos(a))))
-    return sb.Camera.look_at(o, ORBIT_TARGET, (0, 1, 0), 42.0, float(np.float32(j.width) / np.float32(j.height))).c
 
 
 def test_same_alone_and_in_the_mix(ctx):
@@ -116,3 +105,7 @@ def test_realtime_stream_completes(ctx):
     assert m["requests"] == len(stream) > 10
     assert 0 < m["p50_ms"] <= m["p99_ms"] and m["photons"] > 0
     assert s.stats()["bytes_in_use"] == 0
+    # the plain per-request path renders the same frames (same photon total)
+    plain = run_plain_stream(ctx, stream)
+    assert plain["requests"] == len(stream) and plain["photons"] == m["photons"]
+    assert 0 < plain["p50_ms"] <= plain["p99_ms"]
