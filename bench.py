@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps")
+    ap.add_argument("--photons", type=int, default=0,
+                    help="photons per step for prism/rainbow/beam (0: the workload's; smaller for profiling)")
     return ap.parse_args()
 
 
@@ -215,7 +217,9 @@ def run_gpu(args, rank, world, local_rank):
     dist = None
     if world > 1:
         import torch.distributed as dist
-    cfg = WORKLOADS[args.workload]
+    cfg = dict(WORKLOADS[args.workload])
+    if args.photons:
+        cfg["photons"] = args.photons
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     ctx = sb.GpuContext(local_rank)
@@ -371,7 +375,8 @@ def run_gpu(args, rank, world, local_rank):
         "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 transport, int64 fixed-point film", "data": "synthetic (seeded scene)",
-        "config": {"workload": "%s: %s" % (args.workload, workload_txt[args.workload]),
+        "config": {"workload": "%s: %s%s" % (args.workload, workload_txt[args.workload],
+                                             " [photons per step overridden: %d]" % N if args.photons else ""),
                    "photons_per_step": N * world, "film": [W, H, B], "band_nm": [cfg["lambda_min"], cfg["lambda_max"]],
                    "l2": "flushed between steps (256 MB write outside the timed events)",
                    "parallelism": "photon ranges per rank, no collective"},

@@ -74,9 +74,13 @@ __device__ __forceinline__ void comb_xyz(const TracerSmem& s, float u, float tp,
     out[0] = x; out[1] = y; out[2] = z;
 }
 
+// Paths of a wave are numbered sample-major (path i = sample s of wave pixel j
+// with i = s * n_pixels + j): neighbouring threads trace neighbouring pixels,
+// and the per-pixel sums read the results coalesced.
 __global__ void __launch_bounds__(256) tr_generate(const TracerParams* __restrict__ gp, uint32_t first_pixel,
-                                                   uint32_t n_paths, uint32_t spp, const uint32_t* __restrict__ base,
-                                                   RayQueue q, uint32_t* counts, float* result) {
+                                                   uint32_t n_pixels, uint32_t n_paths,
+                                                   const uint32_t* __restrict__ base, RayQueue q, uint32_t* counts,
+                                                   float* result) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         counts[0] = n_paths;
@@ -84,7 +88,7 @@ __global__ void __launch_bounds__(256) tr_generate(const TracerParams* __restric
     }
     if (i >= n_paths) return;
     const uint32_t W = gp->width, H = gp->height;
-    const uint32_t pixel = first_pixel + i / spp, s = i % spp;
+    const uint32_t s = i / n_pixels, pixel = first_pixel + (i - s * n_pixels);
     const uint32_t px = pixel % W, py = pixel / W;
     Rng r = Rng::make(mix2(pixel, *base + s), gp->seed);
     const float fs = ((float)px + r.f32()) / (float)W;
@@ -101,8 +105,9 @@ __global__ void __launch_bounds__(256) tr_intersect(const TracerParams* __restri
                                                     const uint32_t* __restrict__ counts, HitQueue hq) {
     __shared__ TracerSmem s;
     extern __shared__ __align__(16) unsigned char dyn[];
-    const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
     const uint32_t n = counts[bounce];
+    if (blockIdx.x * blockDim.x >= n) return;  // nothing queued for this CTA (late bounces)
+    const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const f3 o = mk(q.ox[i], q.oy[i], q.oz[i]), d = mk(q.dx[i], q.dy[i], q.dz[i]);
         Hit h;
@@ -132,8 +137,9 @@ __global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __
     __shared__ float st_f[8][kShadeThreads];      // staged survivors: ox oy oz dx dy dz tp u
     __shared__ uint32_t st_u[3][kShadeThreads];   // rng id flags
     extern __shared__ __align__(16) unsigned char dyn[];
-    const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
     const uint32_t n = counts[bounce];
+    if (blockIdx.x * blockDim.x >= n) return;  // nothing queued for this CTA (late bounces)
+    const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     for (uint32_t tile = blockIdx.x * blockDim.x; tile < n; tile += gridDim.x * blockDim.x) {
         const uint32_t i = tile + threadIdx.x;
@@ -226,8 +232,10 @@ __global__ void __launch_bounds__(256) tr_accumulate(uint32_t first_pixel, uint3
     }
     if (j >= n_pixels) return;
     float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
-    const float* r = result + (size_t)j * spp * 3u;
-    for (uint32_t s = 0; s < spp; ++s) { a0 += r[3 * s]; a1 += r[3 * s + 1]; a2 += r[3 * s + 2]; }
+    for (uint32_t s = 0; s < spp; ++s) {
+        const float* r = result + 3u * ((size_t)s * n_pixels + j);
+        a0 += r[0]; a1 += r[1]; a2 += r[2];
+    }
     float* o = sum + 3u * (size_t)(first_pixel + j);
     o[0] += a0; o[1] += a1; o[2] += a2;
 }
@@ -247,7 +255,7 @@ int tracer_grid(int sms) {
 cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch& L, uint32_t first_pixel,
                                uint32_t n_pixels, cudaStream_t st) {
     const uint32_t n_paths = n_pixels * L.spp;
-    tr_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(d_params, first_pixel, n_paths, L.spp, L.d_base, L.qa,
+    tr_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(d_params, first_pixel, n_pixels, n_paths, L.d_base, L.qa,
                                                        L.counts, L.result);
     const size_t dyn = tracer_dyn_smem(L.n_planes);
     for (uint32_t b = 0; b < L.max_depth; ++b) {
