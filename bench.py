@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps")
+    ap.add_argument("--scenes", type=int, default=0,
+                    help="scenes of the batch workload (0: 256; the first N of the same seeded draw)")
     ap.add_argument("--photons", type=int, default=0,
                     help="photons per step for prism/rainbow/beam (0: the workload's; smaller for profiling)")
     return ap.parse_args()
@@ -97,8 +99,10 @@ def run_cpu(wl, seconds, threads=None):
     osc = oracle.OScene(bytes(prims), np_, bytes(planes), npl, bytes(mats), nm, scene.background)
     ob = oracle.or_beam.from_buffer_copy(bytes(beam.c))
     oc = oracle.or_camera.from_buffer_copy(bytes(cam.c))
+    # the reference's XYZ film (per-thread int64 XYZ films merged exactly): a
+    # 64-bin film per host thread would cost more to clear and merge than to trace
     p = oracle.vol_params(cfg["width"], cfg["height"], cfg["seed"], cfg["sigma_s"], cfg["sigma_t"], cfg["g"],
-                          cfg["max_dist"], cfg["max_bounces"], cfg["lambda_min"], cfg["lambda_max"], bins=cfg["bins"])
+                          cfg["max_dist"], cfg["max_bounces"], cfg["lambda_min"], cfg["lambda_max"], bins=0)
     threads = threads or os.cpu_count() or 1
     if cfg.get("estimator", 0) == 2:
         # render_volumetric_scene: photon ranges on all host threads (ctypes
@@ -114,12 +118,12 @@ def run_cpu(wl, seconds, threads=None):
             with cf.ThreadPoolExecutor(threads) as ex:
                 list(ex.map(part, range(threads)))
     else:
-        film = np.zeros(cfg["width"] * cfg["height"] * cfg["bins"], np.int64)
+        film = np.zeros(cfg["width"] * cfg["height"] * 3, np.int64)
         fp = film.ctypes.data_as(C.POINTER(C.c_int64))
 
         def render(n):
-            oracle.lib.or_render_point_mt(C.byref(osc.c), C.byref(oc), C.byref(ob), C.byref(p), None, 0, n, None,
-                                          fp, threads)
+            oracle.lib.or_render_point_mt(C.byref(osc.c), C.byref(oc), C.byref(ob), C.byref(p), None, 0, n, fp,
+                                          None, threads)
     # calibrate on a small sample, then size the timed sample to ~`seconds`
     n = 64 if cfg.get("estimator", 0) == 2 else 4096
     while True:
@@ -278,7 +282,7 @@ def run_gpu(args, rank, world, local_rank):
     torch.cuda.synchronize()
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
-    with ClockSampler(uuid) as clk:
+    with ClockSampler(uuid) as clk, torch.cuda.nvtx.range("timed"):  # nvtx range for ncu --nvtx-include
         for k in range(args.steps):
             flush.zero_()  # evict the film from L2 between steps (outside the events)
             ev[k][0].record(stream)
@@ -473,7 +477,7 @@ def run_gpu_tracer(args, rank, world, local_rank):
     torch.cuda.synchronize()
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
     uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
-    with ClockSampler(uuid) as clk:
+    with ClockSampler(uuid) as clk, torch.cuda.nvtx.range("timed"):  # nvtx range for ncu --nvtx-include
         for k in range(args.steps):
             with torch.cuda.stream(st):
                 flush.zero_()  # evict queues and accumulators from L2 (outside the events)
@@ -596,7 +600,7 @@ def run_gpu_serve(args, rank, world, local_rank):
     stream = poisson_requests(SERVE["rate"], SERVE["seconds"], SERVE["seed"] + rank)
     srv = Server(ctx, budget_bytes=budget)
     uuid = "GPU-" + str(torch.cuda.get_device_properties(torch.device("cuda", local_rank)).uuid)
-    with ClockSampler(uuid) as clk:
+    with ClockSampler(uuid) as clk, torch.cuda.nvtx.range("timed"):  # nvtx range for ncu --nvtx-include
         served = run_stream(srv, stream, want_image=True)
     srv.close()
     plain = run_plain_stream(ctx, stream)
@@ -629,10 +633,10 @@ def run_gpu_serve(args, rank, world, local_rank):
 BATCH = dict(n_jobs=256, seed=0xB200, bins=32, lambda_min=380.0, lambda_max=780.0)
 
 
-def batch_jobs(rank):
+def batch_jobs(rank, n_jobs=0):
     from spectral_b200.batch import prism_jobs
     from spectral_b200.scenes import random_prism_jobs
-    return random_prism_jobs(BATCH["n_jobs"], seed=BATCH["seed"] + rank, bins=BATCH["bins"],
+    return random_prism_jobs(n_jobs or BATCH["n_jobs"], seed=BATCH["seed"] + rank, bins=BATCH["bins"],
                              lambda_min=BATCH["lambda_min"], lambda_max=BATCH["lambda_max"]), prism_jobs
 
 
@@ -694,7 +698,7 @@ def run_gpu_batch(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     ctx = sb.GpuContext(local_rank)
-    specs, prism_jobs = batch_jobs(rank)  # weak scaling: every rank renders its own 256 scenes
+    specs, prism_jobs = batch_jobs(rank, args.scenes)  # weak scaling: every rank renders its own scenes
     jobs = prism_jobs(specs)
     b = Batch(ctx, jobs)
     tuning = b.autotune()  # untimed: picks chunk size, register bound, splat aggregation
@@ -719,7 +723,7 @@ def run_gpu_batch(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
-    with ClockSampler(uuid) as clk:
+    with ClockSampler(uuid) as clk, torch.cuda.nvtx.range("timed"):  # nvtx range for ncu --nvtx-include
         ms = timed(b.run, args.steps)
     if dist:
         dist.barrier()
@@ -787,14 +791,16 @@ def run_gpu_batch(args, rank, world, local_rank):
         "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 transport, int64 fixed-point films", "data": "synthetic (PCG-seeded scene batch)",
-        "config": {"workload": "batch: 256 prism scenes, glass {BK7,SF11,fused silica}, apex U(30,75), incidence "
+        "config": {"workload": "batch: %d prism scenes, glass {BK7,SF11,fused silica}, apex U(30,75), incidence "
                                "U(30,60), photons log-U(2^14,2^22), square film side log-U(128,1024), 32 bins, "
-                               "sigma_s U(0.01,0.1); one persistent graph-captured launch + one drain/reduce",
+                               "sigma_s U(0.01,0.1); one persistent graph-captured launch + one drain/reduce"
+                               % len(jobs),
                    "photons_per_step": b.total_photons * world, "scenes_per_rank": len(jobs),
                    "film_gb_per_rank": film_gb, "l2": "films (%.1f GB) far larger than L2" % film_gb,
                    "autotuned": tuning, "parallelism": "scene batch per rank, no collective"},
         "plain": {"value": plain_value, "unit": "photons/s", "ms_per_step": sum(plain_ms) / len(plain_ms),
-                  "what": "the same 256 scenes as plain per-scene launches (trace + drain/reduce each), one GPU"},
+                  "what": "the same %d scenes as plain per-scene launches (trace + drain/reduce each), one GPU"
+                          % len(jobs)},
         "plain_api": {"value": b.total_photons / plain_api_s, "unit": "photons/s", "s_per_step": plain_api_s,
                       "what": "per scene: GpuPhotonFilm create + trace_and_resolve + accum (host XYZ) + destroy"},
         "batched_over_plain": value / world / plain_value,

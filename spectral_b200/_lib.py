@@ -203,7 +203,7 @@ class SpectralError(RuntimeError):
 
 def load():
     if not os.path.exists(LIB_PATH):
-        raise ImportError("spectral_cuda library not built: %s (run python -m spectral_b200.build)" % LIB_PATH)
+        raise ImportError("spectral_cuda library not built: %s (run python spectral_b200/build.py)" % LIB_PATH)
     lib = C.CDLL(LIB_PATH)
     for name, (res, args) in PROTOTYPES.items():
         fn = getattr(lib, name)

@@ -32,9 +32,23 @@ __device__ __forceinline__ void reduce_tile(const ReduceParams& p, uint32_t tile
     ulonglong2* src = reinterpret_cast<ulonglong2*>(p.film + (size_t)tile * kTilePixels * C);
     ulonglong2* dst = reinterpret_cast<ulonglong2*>(sm);
     const uint32_t n2 = kTilePixels * C / 2u;
-    for (uint32_t i = tid; i < n2; i += blockDim.x) {
-        dst[i] = __ldcs(src + i);
-        if (drain) __stcs(src + i, make_ulonglong2(0ull, 0ull));
+    // up to 8 independent 16-byte loads in flight per thread (a 64-bin tile is
+    // 8 per thread), then the shared-memory copy and the drain's zero stores
+    for (uint32_t i0 = tid; i0 < n2; i0 += 8u * blockDim.x) {
+        ulonglong2 v[8];
+#pragma unroll
+        for (uint32_t k = 0; k < 8u; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            if (i < n2) v[k] = __ldcs(src + i);
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < 8u; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            if (i < n2) {
+                dst[i] = v[k];
+                if (drain) __stcs(src + i, make_ulonglong2(0ull, 0ull));
+            }
+        }
     }
     __syncthreads();
     if (C == 3u) {
