@@ -170,6 +170,94 @@ __device__ __forceinline__ void deposit_pixel(const PhotonParams& p, uint32_t px
     }
 }
 
+// Dirty bits of the tiles under a footprint box: its corners' tiles when it
+// spans at most 2 tiles per axis, else every tile.
+__device__ __forceinline__ void mark_box(const PhotonParams& p, uint32_t* smask, int x0, int y0, int x1, int y1,
+                                         uint32_t lane) {
+    const int tx0 = x0 >> 3, ty0 = y0 >> 3, tx1 = x1 >> 3, ty1 = y1 >> 3;
+    if (tx1 - tx0 <= 1 && ty1 - ty0 <= 1) {
+        if (lane < 4u)
+            mark_tile(p, smask, (uint32_t)(((lane & 2u) ? ty1 : ty0) * (int)p.tiles_x + ((lane & 1u) ? tx1 : tx0)));
+    } else {
+        const int ntx = tx1 - tx0 + 1, nt = ntx * (ty1 - ty0 + 1);
+        for (int i = (int)lane; i < nt; i += 32)
+            mark_tile(p, smask, (uint32_t)((ty0 + i / ntx) * (int)p.tiles_x + tx0 + i % ntx));
+    }
+}
+
+// Consecutive march steps often share a footprint box (steps are ~0.5 px apart,
+// a box moves every pixel).  Over such a run each lane keeps its pixels'
+// fixed-point sums in registers and issues one atomic per cell at the end of
+// the run: the same integers reach the film, with fewer atomics.  Runs cover
+// boxes up to 32 wide and 2 passes (footprint radius up to ~7 px).
+struct BoxRun {
+    uint32_t x0y0, box, bin;  // key; box == 0: no open run
+    unsigned long long acc[2][3];
+};
+
+template <bool SPEC>
+__device__ __forceinline__ void run_flush(const PhotonParams& p, BoxRun& run, uint32_t lane) {
+    if (run.box == 0u) return;
+    const int x0 = (int)(run.x0y0 & 0xFFFFu), y0 = (int)(run.x0y0 >> 16);
+    const int bw = (int)(run.box & 0xFFu), bh = (int)((run.box >> 8) & 0xFFu), rows = (int)((run.box >> 16) & 0xFFu);
+    const int lrow = (int)lane / bw, lcol = (int)lane - lrow * bw;
+    if (lrow < rows) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int py = y0 + lrow + k * rows;
+            if (py < y0 + bh) {
+                unsigned long long* c = p.film + film_cell((uint32_t)(x0 + lcol), (uint32_t)py, p.tiles_x, p.channels);
+                if (SPEC) {
+                    red_u64(c + run.bin, run.acc[k][0]);
+                } else {
+                    red_u64(c, run.acc[k][0]);
+                    red_u64(c + 1, run.acc[k][1]);
+                    red_u64(c + 2, run.acc[k][2]);
+                }
+            }
+        }
+    }
+    run.box = 0u;
+}
+
+// Whether a step can join a run (a footprint of at most 2 passes of <= 32 lanes).
+__device__ __forceinline__ bool runnable(const StepRec& R) {
+    return R.valid == 1u && (R.box & 0xFFu) <= 32u && (R.box >> 24) <= 2u;
+}
+
+template <bool SPEC>
+__device__ __forceinline__ void run_add(const PhotonParams& p, uint32_t* smask, BoxRun& run, const StepRec& R,
+                                        uint32_t lane) {
+    const uint32_t bin = SPEC ? R.bin : 0u;
+    if (R.x0y0 != run.x0y0 || R.box != run.box || bin != run.bin) {
+        run_flush<SPEC>(p, run, lane);
+        run.x0y0 = R.x0y0; run.box = R.box; run.bin = bin;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) run.acc[k][0] = run.acc[k][1] = run.acc[k][2] = 0ull;
+        const int x0 = (int)(R.x0y0 & 0xFFFFu), y0 = (int)(R.x0y0 >> 16);
+        mark_box(p, smask, x0, y0, x0 + (int)(R.box & 0xFFu) - 1, y0 + (int)((R.box >> 8) & 0xFFu) - 1, lane);
+    }
+    const int x0 = (int)(R.x0y0 & 0xFFFFu), y0 = (int)(R.x0y0 >> 16);
+    const int bw = (int)(R.box & 0xFFu), bh = (int)((R.box >> 8) & 0xFFu), rows = (int)((R.box >> 16) & 0xFFu);
+    const int lrow = (int)((lane * R.magic) >> 16), lcol = (int)lane - lrow * bw;
+    if (lrow >= rows) return;
+    const float dx = (float)(x0 + lcol) - R.cx, dx2 = dx * dx, inv_r = R.inv_r, inv = R.inv_wsum;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int py = y0 + lrow + k * rows;
+        if (py < y0 + bh) {
+            const float w = tent(dx2, (float)py - R.cy, inv_r) * inv;
+            if (w > 0.0f) {
+                run.acc[k][0] += to_fixed(R.c0 * w, p.scale);
+                if (!SPEC) {
+                    run.acc[k][1] += to_fixed(R.c1 * w, p.scale);
+                    run.acc[k][2] += to_fixed(R.c2 * w, p.scale);
+                }
+            }
+        }
+    }
+}
+
 // splat_transverse (volume.rs:174-218) by the whole warp, its tent sum already
 // known: lanes cover the footprint box (rows packed 32 / width at a time, or
 // 32-column chunks of one row for boxes wider than 32) and deposit their pixels'
@@ -193,17 +281,7 @@ __device__ __forceinline__ void splat_warp(const PhotonParams& p, uint32_t* smas
     const int bw = (int)(box & 0xFFu), bh = (int)((box >> 8) & 0xFFu), rows = (int)((box >> 16) & 0xFFu);
     const int x1 = x0 + bw - 1, y1 = y0 + bh - 1;
     const float inv_r = R.inv_r, inv = R.inv_wsum;
-    if (!COUNT) {  // tiles under the box: its corners' tiles when it spans <= 2 per axis
-        const int tx0 = x0 >> 3, ty0 = y0 >> 3, tx1 = x1 >> 3, ty1 = y1 >> 3;
-        if (tx1 - tx0 <= 1 && ty1 - ty0 <= 1) {
-            if (lane < 4u)
-                mark_tile(p, smask, (uint32_t)(((lane & 2u) ? ty1 : ty0) * (int)p.tiles_x + ((lane & 1u) ? tx1 : tx0)));
-        } else {
-            const int ntx = tx1 - tx0 + 1, nt = ntx * (ty1 - ty0 + 1);
-            for (int i = (int)lane; i < nt; i += 32)
-                mark_tile(p, smask, (uint32_t)((ty0 + i / ntx) * (int)p.tiles_x + tx0 + i % ntx));
-        }
-    }
+    if (!COUNT) mark_box(p, smask, x0, y0, x1, y1, lane);
     const int lrow = bw <= 32 ? (int)((lane * R.magic) >> 16) : 0;
     const int lcol = (int)lane - lrow * bw;
     if (lrow >= rows) return;
@@ -260,12 +338,20 @@ __device__ __forceinline__ void beam_flush(const PhotonParams& p, BeamWarpSmem& 
         ws.step[lane] = R;
         unsigned todo = __ballot_sync(0xffffffffu, R.valid != 0u);
         __syncwarp();
+        BoxRun run;
+        run.box = 0u;
         while (todo) {
             const uint32_t j = __ffs(todo) - 1u;
             todo &= todo - 1u;
             const StepRec& Rj = ws.step[j];  // fields read from shared memory as used
-            splat_warp<SPEC, COUNT>(p, smask, Rj, lane, cnt);
+            if (!COUNT && runnable(Rj)) {
+                run_add<SPEC>(p, smask, run, Rj, lane);
+            } else {
+                if (!COUNT) run_flush<SPEC>(p, run, lane);
+                splat_warp<SPEC, COUNT>(p, smask, Rj, lane, cnt);
+            }
         }
+        if (!COUNT) run_flush<SPEC>(p, run, lane);
         __syncwarp();
     }
 }

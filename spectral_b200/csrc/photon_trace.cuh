@@ -229,7 +229,7 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
 // uses draw pcg32(state_before + k + 1), exactly the draw the per-photon loop
 // makes, so paths and films are bit-identical to trace_photon's.
 struct SegRec { f3 o, d; float seg, power; uint32_t rng, lane; };
-constexpr uint32_t kWarpSegs = 96;
+constexpr uint32_t kWarpSegs = 64;
 struct alignas(16) WarpSplitSmem {
     SegRec seg[kWarpSegs];
     float4 payload[32];  // per lane: CMF x, y, z of the photon (XYZ film) or its bin in .w
@@ -277,8 +277,15 @@ __device__ __forceinline__ void trace_warp_split(const PhotonParams& p, const Sc
     uint32_t n = 0;  // buffered segments, the same in every lane
     uint32_t n_glass = 0xFFFFFFFFu;
     float n_cached = 1.0f;
-    for (uint32_t b = 0; b < p.max_bounces; ++b) {
-        const unsigned m = __ballot_sync(0xffffffffu, alive);
+    for (uint32_t b = 0;; ++b) {
+        const unsigned m = b < p.max_bounces ? __ballot_sync(0xffffffffu, alive) : 0u;
+        const uint32_t cnt = __popc(m);
+        // one flush site (keeps the inlined haze code single): when this bounce's
+        // segments do not fit, and once when every photon is done
+        if (n + cnt > kWarpSegs || (m == 0u && n)) {
+            flush_segments<SPEC, AGG>(p, ws, n, smask, lane);
+            n = 0;
+        }
         if (m == 0u) break;
         Hit h;
         uint32_t mi = 0;
@@ -287,11 +294,6 @@ __device__ __forceinline__ void trace_warp_split(const PhotonParams& p, const Sc
         if (alive) {
             any = scene_hit(S, o, d, h, mi);
             seg = any ? h.t : p.max_dist;
-        }
-        const uint32_t cnt = __popc(m);
-        if (n + cnt > kWarpSegs) {
-            flush_segments<SPEC, AGG>(p, ws, n, smask, lane);
-            n = 0;
         }
         if (alive) {
             SegRec& R = ws.seg[n + __popc(m & below)];
@@ -319,7 +321,6 @@ __device__ __forceinline__ void trace_warp_split(const PhotonParams& p, const Sc
         }
         n += cnt;
     }
-    flush_segments<SPEC, AGG>(p, ws, n, smask, lane);
 }
 
 }  // namespace sc
