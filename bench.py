@@ -1,24 +1,29 @@
 #!/usr/bin/env python
-"""Benchmark of the forward photon + volumetric single-scatter pass on B200.
+"""Benchmarks of the B200 spectral forward / volumetric / camera-tracer path.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
-                    [--workload prism|rainbow]
+                    [--workload batch|prism|rainbow|tracer|beam|serve]
 
-One step = one pass of the hot path over one batch: trace the workload's
-photons into the 64-bit spectral film, then the sensor reduction drains the
-film into an f32 XYZ image.  Prints one JSON line (rank 0).
+Prints one JSON line (rank 0).  Workloads (seeded synthetic scenes):
 
-* value: photons/s with the scene resident in HBM (device-pointer ABI on the
-  timing stream; L2 flushed between steps; max over ranks; weak scaling, each
-  rank traces its own photon index range, no data-path collective);
-* e2e: the same metric through the GpuPhotonFilm-shaped ABI object with host
-  buffers: scene upload, trace, sensor reduce, XYZ read back, film clear;
-* roofline of the dominant kernel (the photon kernel), cpu_baseline from the
-  CPU restatement of the reference's point estimator (oracle) on this host.
+* batch (default): 256 uneven prism scenes (glass, apex, incidence, photons
+  2^14-2^22, film side 128-1024, 32 bins) in one persistent graph-captured
+  launch plus one drain/reduce; compared with plain per-scene launches and
+  with the per-scene film-object API.
+* prism: one SF11 prism, 2^20 photons, 640x360x64-bin film.
+* rainbow: a water sphere in a wide beam, 2^26 photons, 1920x1080x64 bins.
+* tracer: the hero-wavelength camera tracer, 1280x720, 64 spp.
+* beam: the photon-beam estimator on the DSOTM scene, 800x800.
+* serve: a Poisson request stream replayed against the continuous-batching
+  server and against plain per-request launches (latency p50/p99).
 
-``--impl reference`` times the reference's CPU path (the oracle restatement of
-spectral-core's render_volumetric_scene_point, all host threads) on the same
-workload; the reference itself is Rust + wgpu and cannot be built or run here.
+value is device-timed (CUDA events on the launching stream, max over ranks,
+weak scaling: every rank renders its own work, no data-path collective); e2e
+is the same metric through the public ABI with host buffers; roofline and
+cpu_baseline as described in each line.  ``--impl reference`` times the
+reference's CPU path (the oracle restatement of spectral-core, all host
+threads) on the same workload; the reference itself is Rust + wgpu and cannot
+be built or run here.
 """
 import argparse
 import ctypes as C
@@ -134,10 +139,15 @@ def run_cpu(wl, seconds, threads=None):
             break
         n *= 4
     n_s = int(min(cfg["photons"], max(n, n * seconds / max(dt, 1e-6))))
-    t0 = time.perf_counter()
-    render(n_s)
-    dt = time.perf_counter() - t0
-    return n_s / dt, n_s, dt, threads
+    # a whole step that ends early is repeated until ~`seconds` of work
+    done, t0 = 0, time.perf_counter()
+    while True:
+        render(n_s)
+        done += n_s
+        dt = time.perf_counter() - t0
+        if dt >= 0.8 * seconds or n_s < cfg["photons"]:
+            break
+    return done / dt, done, dt, threads
 
 
 def cpu_model():
@@ -408,7 +418,8 @@ def run_gpu(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         rate, n_s, dt, th = run_cpu(args.workload, args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": "photons/s", "cores": th, "kind": "port",
-                                "sample": "first %d photons of the workload (%.1f s), %s" % (n_s, dt, cpu_model())}
+                                "sample": "%d photons of the workload from photon 0 (whole steps repeated), %.1f s, %s"
+                                          % (n_s, dt, cpu_model())}
     return line
 
 
@@ -416,7 +427,7 @@ def run_gpu(args, rank, world, local_rank):
 # spherical D65 emitter r=0.2 at (2,3,1), 1280x720, 64 spp per step, hero comb
 # of 4 wavelengths, depth 8, Russian roulette after bounce 3.
 TRACER = dict(width=1280, height=720, spp=64, seed=0x7ACE)
-TRACER_WAVE_PATHS = 1 << 20  # paths per wavefront wave (the library's queue size)
+TRACER_WAVE_PATHS = 1 << 19  # paths per wavefront wave (the library's queue size per chain)
 
 
 def run_cpu_tracer(seconds, threads=None):
@@ -755,12 +766,14 @@ def run_gpu_batch(args, rank, world, local_rank):
 
     # end to end: new job table each step (host -> device), one pass, every
     # scene's XYZ image back to pinned host memory
+    # (the copy of pass k runs on the batch's copy stream while pass k+1 traces)
     host = torch.empty(b.xyz_floats, dtype=torch.float32, pin_memory=True).numpy()
     e2e_steps = args.e2e_steps or max(3, args.steps // 2)
     for _ in range(1):
         b.update_jobs(jobs)
         b.run(sp)
-        b.read_all_xyz(host, sp)
+        b.read_all_xyz_async(host)
+    b.synchronize()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -768,7 +781,8 @@ def run_gpu_batch(args, rank, world, local_rank):
     for _ in range(e2e_steps):
         b.update_jobs(jobs)
         b.run(sp)
-        b.read_all_xyz(host, sp)
+        b.read_all_xyz_async(host)
+    b.synchronize()
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if dist:
@@ -806,7 +820,8 @@ def run_gpu_batch(args, rank, world, local_rank):
         "batched_over_plain": value / world / plain_value,
         "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": b.job_table_bytes,
                 "d2h_bytes_per_step": b.xyz_floats * 4,
-                "path": "sc_batch_update_jobs + sc_batch_run + sc_batch_read_all_xyz (pinned host)"},
+                "path": "sc_batch_update_jobs + sc_batch_run + sc_batch_read_all_xyz_async (pinned host; the "
+                        "copy of a pass overlaps the next pass's tracing), all steps synchronised at the end"},
         "gpu_launches": args.steps * 2,
         "work": stats,
         "roofline": {"bound": "hbm", "kernel": "batch_kernel + reduce_many (one pass)",
@@ -882,7 +897,7 @@ def main():
             for _ in range(args.steps):
                 rate, n_s, dt, th = run_cpu(args.workload, per_step)
                 rates.append((n_s, dt))
-            sample = "per step the first %d photons of the workload" % rates[0][0]
+            sample = "per step %d photons from photon 0 (the whole workload repeated when shorter)" % rates[0][0]
             metric = METRIC_BEAM if args.workload == "beam" else METRIC_POINT
             cfg_line = {"workload": args.workload, "photons_per_step": cfg["photons"],
                         "film": [cfg["width"], cfg["height"], cfg["bins"]]}

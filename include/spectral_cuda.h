@@ -338,6 +338,12 @@ int sc_batch_synchronize(sc_batch* b);
 int sc_batch_read_xyz(sc_batch* b, uint32_t job, float* out);
 /* All jobs' XYZ images concatenated in job order (sum of 3*w*h floats). */
 int sc_batch_read_all_xyz(sc_batch* b, float* out, size_t capacity, void* stream);
+/* The same copy without waiting for it: ordered after the last pass, on
+ * `stream` (NULL: the batch's own copy stream).  The next pass traces while the
+ * copy runs and starts its drain only after the copy ends, and the next
+ * sc_batch_update_jobs waits for the last pass; `out` must stay valid (and
+ * should be pinned) until sc_batch_synchronize or the stream is synchronised. */
+int sc_batch_read_all_xyz_async(sc_batch* b, float* out, size_t capacity, void* stream);
 /* job_table_bytes: bytes uploaded host -> device by sc_batch_update_jobs. */
 int sc_batch_info(sc_batch* b, uint64_t* total_photons, uint64_t* film_bytes, uint64_t* xyz_floats,
                   uint64_t* job_table_bytes);

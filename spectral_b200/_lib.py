@@ -177,6 +177,7 @@ PROTOTYPES = {
     "sc_batch_synchronize": (_i32, [_vp]),
     "sc_batch_read_xyz": (_i32, [_vp, _u32, P(_f32)]),
     "sc_batch_read_all_xyz": (_i32, [_vp, P(_f32), _sz, _vp]),
+    "sc_batch_read_all_xyz_async": (_i32, [_vp, P(_f32), _sz, _vp]),
     "sc_batch_info": (_i32, [_vp, P(_u64), P(_u64), P(_u64), P(_u64)]),
     "sc_batch_device_xyz": (_i32, [_vp, _u32, P(P(_f32))]),
     "sc_batch_stats": (_i32, [_vp, P(_u64)]),

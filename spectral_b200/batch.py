@@ -95,6 +95,13 @@ class Batch:
                                         C.c_void_p(stream) if stream else None))
         return out
 
+    def read_all_xyz_async(self, out, stream=None):
+        """Start copying every image into `out` (pinned, kept alive by the
+        caller) without waiting; the next pass overlaps the copy."""
+        check(lib.sc_batch_read_all_xyz_async(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size,
+                                              C.c_void_p(stream) if stream else None))
+        return out
+
     def stats(self):
         out = (C.c_uint64 * 6)()
         check(lib.sc_batch_stats(self.h, out))

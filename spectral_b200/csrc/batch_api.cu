@@ -48,6 +48,13 @@ int check_job(const sc_scene_job& j, uint32_t i) {
 struct sc_batch {
     sc_ctx* ctx = nullptr;
     cudaStream_t stream = nullptr;
+    // Pipelined read-back: `ran` is recorded after every pass, `copied` after
+    // every asynchronous image copy.  Job uploads wait for the last pass, a
+    // pass's drain (which rewrites the images) waits for the last copy, and a
+    // copy waits for the last pass, so the copy of pass k overlaps the tracing
+    // of pass k + 1.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ran = nullptr, copied = nullptr;
     std::mutex mu;
     std::vector<sc_scene_job> jobs;
     std::vector<JobGeom> geom;
@@ -110,6 +117,7 @@ struct sc_batch {
             d.flags = flags.p + flag_off[j];
             d.mask_words = geom[j].words;
         }
+        SC_CUDA(cudaStreamWaitEvent(stream, ran, 0));  // the previous pass still reads the table
         SC_CUDA(cudaMemcpyAsync(d_jobs.p, h_jobs.data(), h_jobs.size() * sizeof(BatchJobDev), cudaMemcpyHostToDevice,
                                 stream));
         return SC_OK;
@@ -156,6 +164,8 @@ struct sc_batch {
     int enqueue_batch(cudaStream_t s) {
         SC_CUDA(launch_batch(d_jobs.p, d_items.p, n_items, counter.p, ctx->cmf.p, kBatchMaskWords,
                              (int)tuning.aggregate, (int)tuning.minb, tuning.per_photon ? 0 : 1, grid, s));
+        // the drain rewrites the images: wait for the last asynchronous copy of them
+        SC_CUDA(cudaStreamWaitEvent(s, copied, cudaEventWaitExternal));
         SC_CUDA(launch_reduce_many(d_descs.p, (uint32_t)jobs.size(), total_tiles, true, max_channels, s));
         return SC_OK;
     }
@@ -178,10 +188,12 @@ struct sc_batch {
             graph_stream = s;
         }
         SC_CUDA(cudaGraphLaunch(graph, s));
+        SC_CUDA(cudaEventRecord(ran, s));
         return SC_OK;
     }
 
     int run_plain(cudaStream_t s) {
+        SC_CUDA(cudaStreamWaitEvent(s, copied, 0));  // the drains rewrite the images
         for (uint32_t j = 0; j < jobs.size(); ++j) {
             PhotonParams p = job_params(j);
             p.prims = reinterpret_cast<const sc_primitive*>(
@@ -203,6 +215,7 @@ struct sc_batch {
             r.inv_scale = std::ldexp(1.0, -(int)(jobs[j].opts.scale_log2 ? jobs[j].opts.scale_log2 : 32u));
             SC_CUDA(launch_reduce(r, true, s));
         }
+        SC_CUDA(cudaEventRecord(ran, s));
         return SC_OK;
     }
 };
@@ -240,11 +253,19 @@ int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs, cons
     auto fail = [&](cudaError_t e) {
         set_error("batch setup failed: %s", cudaGetErrorString(e));
         if (b->stream) cudaStreamDestroy(b->stream);
+        if (b->copy_stream) cudaStreamDestroy(b->copy_stream);
+        if (b->ran) cudaEventDestroy(b->ran);
+        if (b->copied) cudaEventDestroy(b->copied);
         delete b;
         return e == cudaErrorMemoryAllocation ? SC_E_NOMEM : SC_E_CUDA;
     };
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(e);
+    if ((e = cudaStreamCreateWithFlags(&b->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreateWithFlags(&b->ran, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventRecord(b->ran, b->stream)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventRecord(b->copied, b->stream)) != cudaSuccess) return fail(e);
     if ((e = b->films.alloc(cells)) != cudaSuccess) return fail(e);
     if ((e = b->flags.alloc(words)) != cudaSuccess) return fail(e);
     if ((e = b->xyz.alloc(3 * px)) != cudaSuccess) return fail(e);
@@ -281,6 +302,9 @@ int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs, cons
     if (rc != SC_OK) {
         std::string msg = sc_last_error();
         if (b->stream) cudaStreamDestroy(b->stream);
+        if (b->copy_stream) cudaStreamDestroy(b->copy_stream);
+        if (b->ran) cudaEventDestroy(b->ran);
+        if (b->copied) cudaEventDestroy(b->copied);
         delete b;
         set_error("%s", msg.c_str());
         return rc;
@@ -297,10 +321,14 @@ int sc_batch_destroy(sc_batch* b) {
         DeviceGuard g(b->ctx->device);
         if (b->stream) cudaStreamSynchronize(b->stream);
         if (b->graph_stream) cudaStreamSynchronize(b->graph_stream);
+        if (b->copy_stream) cudaStreamSynchronize(b->copy_stream);
         b->drop_graph();
         b->films.reset(); b->flags.reset(); b->xyz.reset(); b->binw.reset(); b->d_jobs.reset(); b->d_items.reset();
         b->d_descs.reset(); b->counter.reset();
         if (b->stream) cudaStreamDestroy(b->stream);
+        if (b->copy_stream) cudaStreamDestroy(b->copy_stream);
+        if (b->ran) cudaEventDestroy(b->ran);
+        if (b->copied) cudaEventDestroy(b->copied);
     }
     delete b;
     return SC_OK;
@@ -413,6 +441,7 @@ int sc_batch_synchronize(sc_batch* b) {
     BATCH_LOCK(b);
     SC_CUDA(cudaStreamSynchronize(b->stream));
     if (b->graph_stream) SC_CUDA(cudaStreamSynchronize(b->graph_stream));
+    SC_CUDA(cudaStreamSynchronize(b->copy_stream));
     return SC_OK;
     SC_GUARD_END
 }
@@ -433,8 +462,21 @@ int sc_batch_read_all_xyz(sc_batch* b, float* out, size_t capacity, void* stream
     BATCH_LOCK(b);
     SC_REQUIRE(out && capacity >= b->xyz.n, SC_E_INVALID, "output holds %zu floats, need %zu", capacity, b->xyz.n);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+    SC_CUDA(cudaStreamWaitEvent(s, b->ran, 0));
     SC_CUDA(cudaMemcpyAsync(out, b->xyz.p, b->xyz.bytes(), cudaMemcpyDeviceToHost, s));
     SC_CUDA(cudaStreamSynchronize(s));
+    return SC_OK;
+    SC_GUARD_END
+}
+
+int sc_batch_read_all_xyz_async(sc_batch* b, float* out, size_t capacity, void* stream) {
+    SC_GUARD_BEGIN
+    BATCH_LOCK(b);
+    SC_REQUIRE(out && capacity >= b->xyz.n, SC_E_INVALID, "output holds %zu floats, need %zu", capacity, b->xyz.n);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->copy_stream;
+    SC_CUDA(cudaStreamWaitEvent(s, b->ran, 0));
+    SC_CUDA(cudaMemcpyAsync(out, b->xyz.p, b->xyz.bytes(), cudaMemcpyDeviceToHost, s));
+    SC_CUDA(cudaEventRecord(b->copied, s));
     return SC_OK;
     SC_GUARD_END
 }

@@ -15,48 +15,76 @@ constexpr int kReduceThreads = 256;
 // reduced per pixel: XYZ film -> value / 2^scale; spectral film -> sum over bins
 // of count * bin-averaged CMF (f64 accumulation, fixed order per pixel).
 // Tiles whose dirty flag is clear are never read: their pixels are written as 0.
-__device__ __forceinline__ void reduce_tile(const ReduceParams& p, uint32_t tile, bool drain,
-                                            unsigned long long* sm, double* part) {
-    const uint32_t C = p.channels;
-    const uint32_t tx = tile % p.tiles_x, ty = tile / p.tiles_x;
-    const bool dirty = p.flags == nullptr || (p.flags[tile >> 5] >> (tile & 31u)) & 1u;
-    const uint32_t tid = threadIdx.x;
-    if (!dirty) {
-        for (uint32_t i = tid; i < kTilePixels * 3u; i += blockDim.x) {
-            const uint32_t l = i / 3u, c = i % 3u;
-            const uint32_t px = tx * 8u + (l & 7u), py = ty * 8u + (l >> 3);
-            if (px < p.width && py < p.height) p.xyz[((size_t)py * p.width + px) * 3u + c] = 0.0f;
-        }
-        return;
+//
+// Software pipeline: a CTA walks its tiles keeping the next tile's first
+// 8 x 256 16-byte vectors (a whole tile up to 64 channels) in registers, so
+// those loads are in flight while the current tile is reduced out of shared
+// memory.
+struct TileRef {
+    ReduceParams p;
+    uint32_t tile;
+    bool valid, dirty;
+};
+
+__device__ __forceinline__ TileRef tile_ref(const ReduceParams& p, uint32_t tile, bool valid) {
+    TileRef t;
+    t.p = p;
+    t.tile = tile;
+    t.valid = valid;
+    t.dirty = valid && (p.flags == nullptr || ((p.flags[tile >> 5] >> (tile & 31u)) & 1u));
+    return t;
+}
+
+constexpr uint32_t kPrefetch = 8;  // 16-byte vectors per thread held across a tile
+
+__device__ __forceinline__ void prefetch_tile(const TileRef& t, ulonglong2 (&v)[kPrefetch]) {
+    if (!t.dirty) return;
+    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(t.p.film + (size_t)t.tile * kTilePixels * t.p.channels);
+    const uint32_t n2 = kTilePixels * t.p.channels / 2u;
+#pragma unroll
+    for (uint32_t k = 0; k < kPrefetch; ++k) {
+        const uint32_t i = threadIdx.x + k * blockDim.x;
+        if (i < n2) v[k] = __ldcs(src + i);
     }
-    ulonglong2* src = reinterpret_cast<ulonglong2*>(p.film + (size_t)tile * kTilePixels * C);
+}
+
+// Registers (and any vectors beyond them) into shared memory; zero the film
+// behind the copy when draining.
+__device__ __forceinline__ void stage_tile(const TileRef& t, const ulonglong2 (&v)[kPrefetch], bool drain,
+                                           unsigned long long* sm) {
+    if (!t.dirty) return;
+    ulonglong2* src = reinterpret_cast<ulonglong2*>(t.p.film + (size_t)t.tile * kTilePixels * t.p.channels);
     ulonglong2* dst = reinterpret_cast<ulonglong2*>(sm);
-    const uint32_t n2 = kTilePixels * C / 2u;
-    // up to 8 independent 16-byte loads in flight per thread (a 64-bin tile is
-    // 8 per thread), then the shared-memory copy and the drain's zero stores
-    for (uint32_t i0 = tid; i0 < n2; i0 += 8u * blockDim.x) {
-        ulonglong2 v[8];
+    const uint32_t n2 = kTilePixels * t.p.channels / 2u;
+    const ulonglong2 zero = make_ulonglong2(0ull, 0ull);
 #pragma unroll
-        for (uint32_t k = 0; k < 8u; ++k) {
-            const uint32_t i = i0 + k * blockDim.x;
-            if (i < n2) v[k] = __ldcs(src + i);
-        }
-#pragma unroll
-        for (uint32_t k = 0; k < 8u; ++k) {
-            const uint32_t i = i0 + k * blockDim.x;
-            if (i < n2) {
-                dst[i] = v[k];
-                if (drain) __stcs(src + i, make_ulonglong2(0ull, 0ull));
-            }
+    for (uint32_t k = 0; k < kPrefetch; ++k) {
+        const uint32_t i = threadIdx.x + k * blockDim.x;
+        if (i < n2) {
+            dst[i] = v[k];
+            if (drain) __stcs(src + i, zero);
         }
     }
-    __syncthreads();
-    if (C == 3u) {
+    for (uint32_t i = threadIdx.x + kPrefetch * blockDim.x; i < n2; i += blockDim.x) {  // > 64 channels
+        dst[i] = __ldcs(src + i);
+        if (drain) __stcs(src + i, zero);
+    }
+}
+
+// Per-pixel reduction of a staged tile (or zeros for a clean one).
+__device__ __forceinline__ void reduce_staged(const TileRef& t, bool drain, const unsigned long long* sm,
+                                              double* part) {
+    const ReduceParams& p = t.p;
+    const uint32_t C = p.channels, tile = t.tile;
+    const uint32_t tx = tile % p.tiles_x, ty = tile / p.tiles_x;
+    const uint32_t tid = threadIdx.x;
+    if (!t.dirty || C == 3u) {
         for (uint32_t i = tid; i < kTilePixels * 3u; i += blockDim.x) {
             const uint32_t l = i / 3u, c = i % 3u;
             const uint32_t px = tx * 8u + (l & 7u), py = ty * 8u + (l >> 3);
             if (px < p.width && py < p.height)
-                p.xyz[((size_t)py * p.width + px) * 3u + c] = (float)((double)(long long)sm[i] * p.inv_scale);
+                p.xyz[((size_t)py * p.width + px) * 3u + c] =
+                    t.dirty ? (float)((double)(long long)sm[i] * p.inv_scale) : 0.0f;
         }
     } else {
         // 4 threads per pixel, each a contiguous quarter of the bins; partials
@@ -88,40 +116,68 @@ __device__ __forceinline__ void reduce_tile(const ReduceParams& p, uint32_t tile
             }
         }
     }
-    if (drain && p.flags && tid == 0) atomicAnd(p.flags + (tile >> 5), ~(1u << (tile & 31u)));
-    __syncthreads();
+    if (drain && t.dirty && p.flags && tid == 0) atomicAnd(p.flags + (tile >> 5), ~(1u << (tile & 31u)));
+}
+
+// The pipelined walk over this CTA's tiles; `at(k)` gives its k-th tile.
+template <bool DRAIN, class At>
+__device__ __forceinline__ void reduce_walk(At at, unsigned long long* sm, double* part) {
+    ulonglong2 v[kPrefetch];
+    TileRef cur = at(0u);
+    prefetch_tile(cur, v);
+    for (uint32_t k = 0; cur.valid; ++k) {
+        stage_tile(cur, v, DRAIN, sm);
+        __syncthreads();
+        const TileRef nxt = at(k + 1u);
+        prefetch_tile(nxt, v);  // in flight while this tile is reduced
+        reduce_staged(cur, DRAIN, sm, part);
+        __syncthreads();
+        cur = nxt;
+    }
 }
 
 template <bool DRAIN>
-__global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const ReduceParams p) {
+__global__ void __launch_bounds__(kReduceThreads, 3) reduce_kernel(const ReduceParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
     double* part = reinterpret_cast<double*>(smem);
     unsigned long long* sm = reinterpret_cast<unsigned long long*>(smem + 4 * 64 * 3 * sizeof(double));
     const uint32_t ntiles = p.tiles_x * p.tiles_y;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) reduce_tile(p, tile, DRAIN, sm, part);
+    reduce_walk<DRAIN>(
+        [&](uint32_t k) {
+            const uint32_t tile = blockIdx.x + k * gridDim.x;
+            return tile_ref(p, tile < ntiles ? tile : 0u, tile < ntiles);
+        },
+        sm, part);
 }
 
 // Many films in one persistent launch: global tile index -> (film, tile) by a
 // binary search over the films' tile prefix.
 template <bool DRAIN>
-__global__ void __launch_bounds__(kReduceThreads) reduce_many_kernel(const FilmDesc* __restrict__ descs, uint32_t n_films,
+__global__ void __launch_bounds__(kReduceThreads, 3) reduce_many_kernel(const FilmDesc* __restrict__ descs, uint32_t n_films,
                                                                      uint32_t total_tiles) {
     extern __shared__ __align__(16) unsigned char smem[];
     double* part = reinterpret_cast<double*>(smem);
     unsigned long long* sm = reinterpret_cast<unsigned long long*>(smem + 4 * 64 * 3 * sizeof(double));
-    for (uint32_t g = blockIdx.x; g < total_tiles; g += gridDim.x) {
-        uint32_t lo = 0, hi = n_films;
-        while (hi - lo > 1u) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (descs[mid].tile_begin <= g) lo = mid; else hi = mid;
-        }
-        const FilmDesc& d = descs[lo];
-        ReduceParams p;
-        p.film = d.film; p.flags = d.flags; p.xyz = d.xyz; p.width = d.width; p.height = d.height;
-        p.tiles_x = d.tiles_x; p.tiles_y = d.tiles_y; p.channels = d.channels; p.binw = d.binw;
-        p.inv_scale = d.inv_scale;
-        reduce_tile(p, g - d.tile_begin, DRAIN, sm, part);
-    }
+    reduce_walk<DRAIN>(
+        [&](uint32_t k) {
+            const uint32_t g = blockIdx.x + k * gridDim.x;
+            ReduceParams p;
+            if (g >= total_tiles) {
+                p = ReduceParams{};
+                return tile_ref(p, 0u, false);
+            }
+            uint32_t lo = 0, hi = n_films;
+            while (hi - lo > 1u) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (descs[mid].tile_begin <= g) lo = mid; else hi = mid;
+            }
+            const FilmDesc& d = descs[lo];
+            p.film = d.film; p.flags = d.flags; p.xyz = d.xyz; p.width = d.width; p.height = d.height;
+            p.tiles_x = d.tiles_x; p.tiles_y = d.tiles_y; p.channels = d.channels; p.binw = d.binw;
+            p.inv_scale = d.inv_scale;
+            return tile_ref(p, g - d.tile_begin, true);
+        },
+        sm, part);
 }
 
 __global__ void composite_max_y_kernel(const float* __restrict__ xyz, const float* __restrict__ surface,

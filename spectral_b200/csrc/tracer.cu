@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(256) tr_accumulate(uint32_t first_pixel, uint3
     if (j == 0) {
         unsigned long long t = 0;
         for (uint32_t b = 0; b < max_depth; ++b) t += counts[b];
-        *segments += t;
+        atomicAdd(segments, t);  // both wave chains add here
     }
     if (j >= n_pixels) return;
     float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;

@@ -9,12 +9,17 @@
 using namespace sc;
 
 namespace {
-constexpr uint32_t kWavePaths = 1u << 20;  // queues of one wave stay resident in L2
+// Waves run on two chains (two streams, two queue sets), so one wave's short
+// late-bounce launches overlap the next wave's full-width ones; the queues of
+// both chains together (2 x 2^19 paths) stay resident in L2.
+constexpr uint32_t kChains = 2;
+constexpr uint32_t kWavePaths = 1u << 19;  // paths per wave and chain
 }
 
 struct sc_tracer {
     sc_ctx* ctx = nullptr;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr, stream2 = nullptr;  // chain 0 (the tracer's stream), chain 1
+    cudaEvent_t fork = nullptr, join = nullptr;
     std::mutex mu;
     uint32_t w = 0, h = 0, samples = 0;
     TracerParams hp{};
@@ -28,7 +33,7 @@ struct sc_tracer {
     DevBuf<unsigned long long> segments;
     DevBuf<uint32_t> qbuf_u;
     uint32_t wave_cap = 0;  // paths per wave the queues are sized for
-    TracerLaunch L{};
+    TracerLaunch L[kChains]{};
     cudaGraphExec_t graph = nullptr;
     uint32_t graph_spp = 0;
     uint64_t last_paths = 0, last_segments = 0;
@@ -46,22 +51,28 @@ struct sc_tracer {
         if (paths <= wave_cap) return SC_OK;
         drop_graph();
         const size_t n = paths;
-        SC_CUDA(qbuf.alloc(n * 8 * 2 + n * 4 + 3 * n));    // 2 ray queues x 8 floats, hits 4 floats, result 3
-        SC_CUDA(qbuf_u.alloc(n * 3 * 2 + n));               // 2 ray queues x 3 u32, hit info
+        // per chain: 2 ray queues x 8 floats, hits 4 floats, result 3; 2 ray queues x 3 u32, hit info
+        SC_CUDA(qbuf.alloc(kChains * (n * 8 * 2 + n * 4 + 3 * n)));
+        SC_CUDA(qbuf_u.alloc(kChains * (n * 3 * 2 + n)));
         float* f = qbuf.p;
         uint32_t* u = qbuf_u.p;
-        RayQueue* qs[2] = {&L.qa, &L.qb};
-        for (RayQueue* q : qs) {
-            q->ox = f; q->oy = f + n; q->oz = f + 2 * n; q->dx = f + 3 * n; q->dy = f + 4 * n; q->dz = f + 5 * n;
-            q->tp = f + 6 * n; q->u = f + 7 * n;
-            f += 8 * n;
-            q->rng = u; q->id = u + n; q->flags = u + 2 * n;
-            u += 3 * n;
+        for (uint32_t c = 0; c < kChains; ++c) {
+            TracerLaunch& Lc = L[c];
+            RayQueue* qs[2] = {&Lc.qa, &Lc.qb};
+            for (RayQueue* q : qs) {
+                q->ox = f; q->oy = f + n; q->oz = f + 2 * n; q->dx = f + 3 * n; q->dy = f + 4 * n;
+                q->dz = f + 5 * n; q->tp = f + 6 * n; q->u = f + 7 * n;
+                f += 8 * n;
+                q->rng = u; q->id = u + n; q->flags = u + 2 * n;
+                u += 3 * n;
+            }
+            Lc.hits.t = f; Lc.hits.nx = f + n; Lc.hits.ny = f + 2 * n; Lc.hits.nz = f + 3 * n;
+            f += 4 * n;
+            Lc.result = f;
+            f += 3 * n;
+            Lc.hits.info = u;
+            u += n;
         }
-        L.hits.t = f; L.hits.nx = f + n; L.hits.ny = f + 2 * n; L.hits.nz = f + 3 * n;
-        f += 4 * n;
-        L.result = f;
-        L.hits.info = u;
         wave_cap = paths;
         return SC_OK;
     }
@@ -70,15 +81,23 @@ struct sc_tracer {
         const uint32_t px_per_wave = std::max(1u, kWavePaths / spp);
         int rc = ensure_queues(std::min(npx, px_per_wave) * spp);
         if (rc != SC_OK) return rc;
-        L.spp = spp;
+        for (uint32_t c = 0; c < kChains; ++c) L[c].spp = spp;
         SC_CUDA(cudaMemcpyAsync(base.p, &samples, 4, cudaMemcpyHostToDevice, stream));
         if (!graph || graph_spp != spp) {
             drop_graph();
             cudaGraph_t g = nullptr;
             SC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-            cudaError_t e = cudaSuccess;
-            for (uint32_t first = 0; first < npx && e == cudaSuccess; first += px_per_wave)
-                e = launch_tracer_wave(params.p, L, first, std::min(px_per_wave, npx - first), stream);
+            // fork chain 1 off the tracer's stream, alternate waves, join it back
+            cudaError_t e = cudaEventRecord(fork, stream);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(stream2, fork, 0);
+            uint32_t wave = 0;
+            for (uint32_t first = 0; first < npx && e == cudaSuccess; first += px_per_wave, ++wave) {
+                const uint32_t c = wave % kChains;
+                e = launch_tracer_wave(params.p, L[c], first, std::min(px_per_wave, npx - first),
+                                       c ? stream2 : stream);
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(join, stream2);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, join, 0);
             cudaError_t e2 = cudaStreamEndCapture(stream, &g);
             if (e == cudaSuccess) e = e2;
             if (e == cudaSuccess) e = cudaGraphInstantiate(&graph, g, 0);
@@ -131,18 +150,24 @@ int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, c
     auto fail = [&](cudaError_t e) {
         set_error("tracer setup failed: %s", cudaGetErrorString(e));
         if (t->stream) cudaStreamDestroy(t->stream);
+        if (t->stream2) cudaStreamDestroy(t->stream2);
+        if (t->fork) cudaEventDestroy(t->fork);
+        if (t->join) cudaEventDestroy(t->join);
         delete t;
         return e == cudaErrorMemoryAllocation ? SC_E_NOMEM : SC_E_CUDA;
     };
     cudaError_t e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(e);
+    if ((e = cudaStreamCreateWithFlags(&t->stream2, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreateWithFlags(&t->fork, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreateWithFlags(&t->join, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
     if ((e = t->params.alloc(1)) != cudaSuccess) return fail(e);
     if ((e = t->tables.alloc(5 * kTableN)) != cudaSuccess) return fail(e);
     if ((e = t->prims.alloc(std::max(1u, n_prims))) != cudaSuccess) return fail(e);
     if ((e = t->planes.alloc(std::max(1u, n_planes))) != cudaSuccess) return fail(e);
     if ((e = t->mats.alloc(std::max(1u, n_mats))) != cudaSuccess) return fail(e);
     if ((e = t->sum.alloc(3ull * width * height)) != cudaSuccess) return fail(e);
-    if ((e = t->counts.alloc(o.max_depth + 1)) != cudaSuccess) return fail(e);
+    if ((e = t->counts.alloc(kChains * (o.max_depth + 1))) != cudaSuccess) return fail(e);
     if ((e = t->base.alloc(1)) != cudaSuccess) return fail(e);
     if ((e = t->segments.alloc(1)) != cudaSuccess) return fail(e);
     cudaMemcpy(t->tables.p, ctx->tables, 5 * kTableN * sizeof(float), cudaMemcpyHostToDevice);
@@ -159,9 +184,12 @@ int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, c
     hp.prims = t->prims.p; hp.planes = t->planes.p; hp.mats = t->mats.p;
     hp.n_prims = n_prims; hp.n_planes = n_planes; hp.n_mats = n_mats;
     hp.tables = t->tables.p;
-    TracerLaunch& L = t->L;
-    L.counts = t->counts.p; L.sum = t->sum.p; L.d_base = t->base.p; L.segments = t->segments.p;
-    L.max_depth = o.max_depth; L.n_planes = n_planes; L.grid = (uint32_t)tracer_grid(ctx->sms);
+    for (uint32_t c = 0; c < kChains; ++c) {
+        TracerLaunch& L = t->L[c];
+        L.counts = t->counts.p + c * (o.max_depth + 1); L.sum = t->sum.p; L.d_base = t->base.p;
+        L.segments = t->segments.p;
+        L.max_depth = o.max_depth; L.n_planes = n_planes; L.grid = (uint32_t)tracer_grid(ctx->sms);
+    }
     if ((e = cudaMemcpy(t->params.p, &hp, sizeof hp, cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e);
     *out = t;
@@ -180,6 +208,9 @@ int sc_tracer_destroy(sc_tracer* t) {
         t->sum.reset(); t->result.reset(); t->qbuf.reset(); t->qbuf_u.reset(); t->counts.reset(); t->base.reset();
         t->segments.reset();
         if (t->stream) cudaStreamDestroy(t->stream);
+        if (t->stream2) cudaStreamDestroy(t->stream2);
+        if (t->fork) cudaEventDestroy(t->fork);
+        if (t->join) cudaEventDestroy(t->join);
     }
     delete t;
     return SC_OK;

@@ -99,3 +99,30 @@ def test_update_jobs_and_errors(ctx):
     with pytest.raises(_lib.SpectralError) as e:
         Batch(ctx, bad)
     assert e.value.code == _lib.SC_E_LIMIT
+
+
+def test_async_readback_overlaps_next_pass(ctx):
+    """The asynchronous image copy of pass k runs while pass k+1 traces; the
+    next job upload waits for pass k and the next drain for the copy, so each
+    buffer holds exactly its own pass's images."""
+    import torch
+    specs = small_specs(6, seed=21)
+    jobs1 = prism_jobs(specs)
+    for s in specs:
+        s["seed"] ^= 0x5A5A5A
+    jobs2 = prism_jobs(specs)
+    b = Batch(ctx, jobs1)
+    b.run()
+    ref1 = b.read_all_xyz().copy()
+    b.update_jobs(jobs2)
+    b.run()
+    ref2 = b.read_all_xyz().copy()
+    assert ref1.tobytes() != ref2.tobytes()
+    bufs = [torch.empty(b.xyz_floats, dtype=torch.float32, pin_memory=True).numpy() for _ in range(4)]
+    for k in range(4):  # back to back, no host wait between passes
+        b.update_jobs(jobs1 if k % 2 == 0 else jobs2)
+        b.run()
+        b.read_all_xyz_async(bufs[k])
+    b.synchronize()
+    for k in range(4):
+        assert bufs[k].tobytes() == (ref1 if k % 2 == 0 else ref2).tobytes(), k
