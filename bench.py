@@ -320,7 +320,7 @@ def run_gpu(args, rank, world, local_rank):
                           sb.VolWeights(cfg["sigma_s"], cfg["sigma_t"], cfg["g"]), bins=B,
                           lambda_min=cfg["lambda_min"], lambda_max=cfg["lambda_max"],
                           max_bounces=cfg["max_bounces"], scale_log2=SCALE, estimator=EST)
-    host_xyz = np.empty(3 * W * H, np.float32)
+    host_xyz = torch.empty(3 * W * H, dtype=torch.float32, pin_memory=True).numpy()  # pinned read-back buffer
     h2d = C.sizeof(prims._type_) * np_ + C.sizeof(planes._type_) * npl + C.sizeof(mats._type_) * nm + \
         C.sizeof(cam.c) + C.sizeof(beam.c)
 
@@ -512,7 +512,7 @@ def run_gpu_tracer(args, rank, world, local_rank):
 
     # end to end through the GpuTracer-shaped ABI object with host buffers: a new
     # camera, clear, 64 spp, mean XYZ back to the host, every step
-    host = np.empty(3 * W * H, np.float32)
+    host = torch.empty(3 * W * H, dtype=torch.float32, pin_memory=True).numpy()  # pinned read-back buffer
     e2e_steps = args.e2e_steps or args.steps
 
     def e2e_step():
