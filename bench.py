@@ -615,6 +615,15 @@ def run_gpu_serve(args, rank, world, local_rank):
         served = run_stream(srv, stream, want_image=True)
     srv.close()
     plain = run_plain_stream(ctx, stream)
+    total_rate = served["photons_per_s"]
+    if world > 1:  # every rank served its own stream: total photons over the longest replay
+        import torch.distributed as dist
+        dev = torch.device("cuda", local_rank)
+        ph = torch.tensor([float(served["photons"])], dtype=torch.float64, device=dev)
+        wall = torch.tensor([served["wall_s"]], dtype=torch.float64, device=dev)
+        dist.all_reduce(ph, op=dist.ReduceOp.SUM)
+        dist.all_reduce(wall, op=dist.ReduceOp.MAX)
+        total_rate = float(ph.item()) / float(wall.item())
     if rank != 0:
         return None
     frames = sum(s[2] for s in stream)
@@ -622,7 +631,7 @@ def run_gpu_serve(args, rank, world, local_rank):
     out_bytes = sum(3 * s[1].width * s[1].height * 4 for s in stream)
     return {
         "metric": "served photons/s with p50/p99 request latency (continuous batching vs plain per-request launch)",
-        "value": served["photons_per_s"] * world, "unit": "photons/s", "n_gpus": world, "steps": 1,
+        "value": total_rate, "unit": "photons/s", "n_gpus": world, "steps": 1,
         "warmup": args.warmup, "ms_per_step": served["wall_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 transport, int64 fixed-point film", "data": "synthetic (seeded stream)",
         "config": {"workload": "serve: Poisson %.0f req/s for %.0f s (%d requests, %d frames), prism scenes of the "
@@ -633,7 +642,7 @@ def run_gpu_serve(args, rank, world, local_rank):
                    "timing": "host clock over the whole stream replayed in real time (one step = the stream)"},
         "served": served, "plain_per_request": plain,
         "served_over_plain": served["photons_per_s"] / plain["photons_per_s"],
-        "e2e": {"value": served["photons_per_s"] * world, "unit": "photons/s", "h2d_bytes_per_step": in_bytes,
+        "e2e": {"value": total_rate, "unit": "photons/s", "h2d_bytes_per_step": in_bytes,
                 "d2h_bytes_per_step": out_bytes,
                 "path": "sc_server_submit per request, sc_server_step, sc_server_poll with the XYZ image to host"},
         "gpu_launches": served["steps"],
@@ -755,13 +764,16 @@ def run_gpu_batch(args, rank, world, local_rank):
         f.accum()
         f.close()
     plain_api_s = time.perf_counter() - t0
-    # kernel split of one batched pass: persistent trace vs drain/reduce (same tuning)
     total_ms = sum(ms)
+    job_photons = b.total_photons  # photons of all ranks' batches (each rank draws its own scenes)
     if dist:
         t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = b.total_photons * world * args.steps / (total_ms / 1e3)
+        t = torch.tensor([b.total_photons], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        job_photons = float(t.item())
+    value = job_photons * args.steps / (total_ms / 1e3)
     plain_value = b.total_photons * len(plain_ms) / (sum(plain_ms) / 1e3)
 
     # end to end: new job table each step (host -> device), one pass, every
@@ -789,11 +801,10 @@ def run_gpu_batch(args, rank, world, local_rank):
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = b.total_photons * world * e2e_steps / e2e_s
+    e2e_value = job_photons * e2e_steps / e2e_s
     if rank != 0:
         return None
 
-    # per-kernel split: time the persistent trace kernel alone once more
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs") or 6650.0
     peak_note = "measured" if peaks.get("hbm_gbs") else "fallback"
@@ -809,7 +820,7 @@ def run_gpu_batch(args, rank, world, local_rank):
                                "U(30,60), photons log-U(2^14,2^22), square film side log-U(128,1024), 32 bins, "
                                "sigma_s U(0.01,0.1); one persistent graph-captured launch + one drain/reduce"
                                % len(jobs),
-                   "photons_per_step": b.total_photons * world, "scenes_per_rank": len(jobs),
+                   "photons_per_step": int(job_photons), "scenes_per_rank": len(jobs),
                    "film_gb_per_rank": film_gb, "l2": "films (%.1f GB) far larger than L2" % film_gb,
                    "autotuned": tuning, "parallelism": "scene batch per rank, no collective"},
         "plain": {"value": plain_value, "unit": "photons/s", "ms_per_step": sum(plain_ms) / len(plain_ms),
@@ -817,7 +828,8 @@ def run_gpu_batch(args, rank, world, local_rank):
                           % len(jobs)},
         "plain_api": {"value": b.total_photons / plain_api_s, "unit": "photons/s", "s_per_step": plain_api_s,
                       "what": "per scene: GpuPhotonFilm create + trace_and_resolve + accum (host XYZ) + destroy"},
-        "batched_over_plain": value / world / plain_value,
+        "batched_over_plain": value / job_photons * b.total_photons / plain_value,
+        "batched_e2e_over_plain_api": e2e_value / job_photons * b.total_photons / (b.total_photons / plain_api_s),
         "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": b.job_table_bytes,
                 "d2h_bytes_per_step": b.xyz_floats * 4,
                 "path": "sc_batch_update_jobs + sc_batch_run + sc_batch_read_all_xyz_async (pinned host; the "
