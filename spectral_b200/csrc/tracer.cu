@@ -23,6 +23,7 @@ namespace sc {
 namespace {
 
 constexpr int kShadeThreads = 256;
+constexpr uint32_t kWaveBounces = 2;  // bounces run as compacted wavefront stages; the rest by tr_tail
 constexpr float kLambdaMin = 380.0f, kLambdaRange = 350.0f;
 
 struct TracerSmem {
@@ -101,6 +102,76 @@ __global__ void __launch_bounds__(256) tr_generate(const TracerParams* __restric
     result[3 * i] = 0.0f; result[3 * i + 1] = 0.0f; result[3 * i + 2] = 0.0f;
 }
 
+// Nearest hit of one ray: scene records and the optional emitter sphere.
+// info = material | front_face << 16 | kind << 24 (0 miss, 1 surface, 2 emitter).
+__device__ __forceinline__ void trace_hit(const TracerSmem& s, const SceneView& S, f3 o, f3 d, float& t, f3& n,
+                                          uint32_t& info) {
+    Hit h;
+    uint32_t mi = 0;
+    const bool any = scene_hit(S, o, d, h, mi);
+    uint32_t kind = any ? 1u : 0u;
+    t = any ? h.t : __int_as_float(0x7f800000);
+    if (s.p.em_radius > 0.0f) {
+        sc_primitive em;
+        em.center[0] = s.p.em_center.x; em.center[1] = s.p.em_center.y; em.center[2] = s.p.em_center.z;
+        em.radius = s.p.em_radius;
+        Hit he;
+        if (sphere_hit(em, o, d, 1e-3f, t, he)) { kind = 2u; t = he.t; }
+    }
+    n = h.normal;
+    info = mi | (((any && h.front_face) ? 1u : 0u) << 16) | (kind << 24);
+}
+
+// State of one path between bounces (the ray queue's fields).
+struct PathState {
+    f3 o, d;
+    float tp, u;
+    uint32_t rs, id, flags;  // RNG state, path id, valid lanes | depth << 8
+};
+
+// Shade one path at `bounce` given its hit: background / emission ends the
+// path (its XYZ goes to result[id]); a surface scatters it (Fresnel / refract /
+// TIR or Lambertian, dispersion collapse, Russian roulette).  Returns whether
+// the path continues.
+__device__ __forceinline__ bool shade_path(const TracerSmem& s, const SceneView& S, uint32_t bounce, PathState& P,
+                                           float t, f3 n, uint32_t info, float* result) {
+    const uint32_t kind = info >> 24;
+    uint32_t valid = P.flags & 0xFFu;
+    if (kind != 1u) {
+        float e;
+        if (kind == 0u) e = s.p.background + ((s.p.has_horizon && P.d.y > 0.0f) ? s.p.horizon : 0.0f);
+        else e = s.p.em_scale;
+        float xyz[3];
+        comb_xyz(s, P.u, P.tp, valid, e, xyz);
+        result[3 * P.id] = xyz[0]; result[3 * P.id + 1] = xyz[1]; result[3 * P.id + 2] = xyz[2];
+        return false;
+    }
+    const sc_material& m = S.mats[info & 0xFFFFu];
+    Hit h;
+    h.t = t;
+    h.point = add(P.o, mul(P.d, t));
+    h.normal = n;
+    h.front_face = ((info >> 16) & 1u) != 0u;
+    const float nh = m.kind == 1u ? glass_n(m.glass, lane_lambda(P.u, 0)) : 1.0f;
+    Rng r;
+    r.state = P.rs;
+    f3 nd;
+    float w;
+    scatter(m, P.d, h, nh, r, nd, w);
+    P.tp *= w;
+    if (m.kind == 1u && valid > 1u) valid = 1u;
+    const uint32_t depth = bounce + 1u;
+    bool survive = depth < s.p.max_depth;
+    if (s.p.rr_start && depth >= s.p.rr_start) {
+        const float qv = fminf(P.tp, 0.95f);
+        if (!(r.f32() < qv)) survive = false;
+        else P.tp = P.tp / qv;
+    }
+    P.o = h.point; P.d = nd; P.rs = r.state;
+    P.flags = valid | (depth << 8);
+    return survive;
+}
+
 __global__ void __launch_bounds__(256) tr_intersect(const TracerParams* __restrict__ gp, uint32_t bounce, RayQueue q,
                                                     const uint32_t* __restrict__ counts, HitQueue hq) {
     __shared__ TracerSmem s;
@@ -110,21 +181,13 @@ __global__ void __launch_bounds__(256) tr_intersect(const TracerParams* __restri
     const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const f3 o = mk(q.ox[i], q.oy[i], q.oz[i]), d = mk(q.dx[i], q.dy[i], q.dz[i]);
-        Hit h;
-        uint32_t mi = 0;
-        const bool any = scene_hit(S, o, d, h, mi);
-        uint32_t kind = any ? 1u : 0u;
-        float t = any ? h.t : __int_as_float(0x7f800000);
-        if (s.p.em_radius > 0.0f) {
-            sc_primitive em;
-            em.center[0] = s.p.em_center.x; em.center[1] = s.p.em_center.y; em.center[2] = s.p.em_center.z;
-            em.radius = s.p.em_radius;
-            Hit he;
-            if (sphere_hit(em, o, d, 1e-3f, t, he)) { kind = 2u; t = he.t; }
-        }
+        float t;
+        f3 nrm;
+        uint32_t info;
+        trace_hit(s, S, o, d, t, nrm, info);
         hq.t[i] = t;
-        if (kind == 1u) { hq.nx[i] = h.normal.x; hq.ny[i] = h.normal.y; hq.nz[i] = h.normal.z; }
-        hq.info[i] = mi | (((any && h.front_face) ? 1u : 0u) << 16) | (kind << 24);
+        if ((info >> 24) == 1u) { hq.nx[i] = nrm.x; hq.ny[i] = nrm.y; hq.nz[i] = nrm.z; }
+        hq.info[i] = info;
     }
 }
 
@@ -144,49 +207,21 @@ __global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __
     for (uint32_t tile = blockIdx.x * blockDim.x; tile < n; tile += gridDim.x * blockDim.x) {
         const uint32_t i = tile + threadIdx.x;
         bool survive = false;
-        f3 o, d;
-        float tp = 0.0f, u = 0.0f;
-        uint32_t rs = 0, id = 0, flags = 0;
+        PathState P;
+        P.o = P.d = mk(0.0f, 0.0f, 0.0f);
+        P.tp = P.u = 0.0f;
+        P.rs = P.id = P.flags = 0u;
         if (i < n) {
-            o = mk(q.ox[i], q.oy[i], q.oz[i]);
-            d = mk(q.dx[i], q.dy[i], q.dz[i]);
-            tp = q.tp[i]; u = q.u[i]; rs = q.rng[i]; id = q.id[i]; flags = q.flags[i];
+            P.o = mk(q.ox[i], q.oy[i], q.oz[i]);
+            P.d = mk(q.dx[i], q.dy[i], q.dz[i]);
+            P.tp = q.tp[i]; P.u = q.u[i]; P.rs = q.rng[i]; P.id = q.id[i]; P.flags = q.flags[i];
             const uint32_t info = hq.info[i];
-            const uint32_t kind = info >> 24;
-            uint32_t valid = flags & 0xFFu;
-            if (kind != 1u) {
-                float e;
-                if (kind == 0u) e = s.p.background + ((s.p.has_horizon && d.y > 0.0f) ? s.p.horizon : 0.0f);
-                else e = s.p.em_scale;
-                float xyz[3];
-                comb_xyz(s, u, tp, valid, e, xyz);
-                result[3 * id] = xyz[0]; result[3 * id + 1] = xyz[1]; result[3 * id + 2] = xyz[2];
-            } else {
-                const sc_material& m = S.mats[info & 0xFFFFu];
-                Hit h;
-                h.t = hq.t[i];
-                h.point = add(o, mul(d, h.t));
-                h.normal = mk(hq.nx[i], hq.ny[i], hq.nz[i]);
-                h.front_face = ((info >> 16) & 1u) != 0u;
-                const float nh = m.kind == 1u ? glass_n(m.glass, lane_lambda(u, 0)) : 1.0f;
-                Rng r;
-                r.state = rs;
-                f3 nd;
-                float w;
-                scatter(m, d, h, nh, r, nd, w);
-                tp *= w;
-                if (m.kind == 1u && valid > 1u) valid = 1u;
-                const uint32_t depth = bounce + 1u;
-                survive = depth < s.p.max_depth;
-                if (s.p.rr_start && depth >= s.p.rr_start) {
-                    const float qv = fminf(tp, 0.95f);
-                    if (!(r.f32() < qv)) survive = false;
-                    else tp = tp / qv;
-                }
-                o = h.point; d = nd; rs = r.state;
-                flags = valid | (depth << 8);
-            }
+            const f3 nrm = (info >> 24) == 1u ? mk(hq.nx[i], hq.ny[i], hq.nz[i]) : mk(0.0f, 0.0f, 0.0f);
+            survive = shade_path(s, S, bounce, P, hq.t[i], nrm, info, result);
         }
+        const f3 o = P.o, d = P.d;
+        const float tp = P.tp, u = P.u;
+        const uint32_t rs = P.rs, id = P.id, flags = P.flags;
         // block-level compaction: ballot per warp, prefix over warps, one atomic
         const unsigned ball = __ballot_sync(0xffffffffu, survive);
         const uint32_t rank = __popc(ball & ((1u << lane) - 1u));
@@ -217,6 +252,36 @@ __global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __
         }
         __syncthreads();
     }
+}
+
+// Late bounces: by the third bounce only a few per cent of a wave's paths are
+// alive, and a launch pair per bounce costs more than the work.  One thread per
+// remaining path runs the rest of its bounces in place (the same hit and shade
+// code, so the image is unchanged); its segments are added to counts[first + 1].
+__global__ void __launch_bounds__(256) tr_tail(const TracerParams* __restrict__ gp, uint32_t first, RayQueue q,
+                                               uint32_t* counts, float* result) {
+    __shared__ TracerSmem s;
+    extern __shared__ __align__(16) unsigned char dyn[];
+    const uint32_t n = counts[first];
+    if (blockIdx.x * blockDim.x >= n) return;
+    const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
+    uint32_t segs = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        PathState P;
+        P.o = mk(q.ox[i], q.oy[i], q.oz[i]);
+        P.d = mk(q.dx[i], q.dy[i], q.dz[i]);
+        P.tp = q.tp[i]; P.u = q.u[i]; P.rs = q.rng[i]; P.id = q.id[i]; P.flags = q.flags[i];
+        for (uint32_t b = first; b < s.p.max_depth; ++b) {
+            float t;
+            f3 nrm;
+            uint32_t info;
+            trace_hit(s, S, P.o, P.d, t, nrm, info);
+            if (b > first) ++segs;  // counts[first] already holds this bounce's rays
+            if (!shade_path(s, S, b, P, t, nrm, info, result)) break;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) segs += __shfl_xor_sync(0xffffffffu, segs, o);
+    if ((threadIdx.x & 31u) == 0 && segs) atomicAdd(counts + first + 1, segs);
 }
 
 // Per-pixel sample sum in sample order (tracer.rs:121-135), added to the running sum.
@@ -258,13 +323,18 @@ cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch&
     tr_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(d_params, first_pixel, n_pixels, n_paths, L.d_base, L.qa,
                                                        L.counts, L.result);
     const size_t dyn = tracer_dyn_smem(L.n_planes);
-    for (uint32_t b = 0; b < L.max_depth; ++b) {
+    // wavefront with compaction for the first bounces, then the tail in place
+    const uint32_t wave_bounces = L.max_depth < kWaveBounces ? L.max_depth : kWaveBounces;
+    for (uint32_t b = 0; b < wave_bounces; ++b) {
         const RayQueue& in = (b & 1u) ? L.qb : L.qa;
         const RayQueue& out = (b & 1u) ? L.qa : L.qb;
         uint32_t g = L.grid;
         tr_intersect<<<g, 256, dyn, st>>>(d_params, b, in, L.counts, L.hits);
         tr_shade<<<g, kShadeThreads, dyn, st>>>(d_params, b, in, L.hits, out, L.counts, L.result);
     }
+    if (L.max_depth > wave_bounces)
+        tr_tail<<<L.grid, 256, dyn, st>>>(d_params, wave_bounces, (wave_bounces & 1u) ? L.qb : L.qa, L.counts,
+                                          L.result);
     tr_accumulate<<<(n_pixels + 255) / 256, 256, 0, st>>>(first_pixel, n_pixels, L.spp, L.result, L.sum, L.counts,
                                                            L.max_depth, L.segments);
     return cudaGetLastError();
