@@ -96,11 +96,28 @@ __device__ __forceinline__ float tent(float dx2, float dy, float inv_r) {
     return fmaxf(1.0f - d * inv_r, 0.0f);
 }
 
+// Dirty bits of the tiles under a footprint box, set by the step's own lane
+// during the setup (most are already set, and mark_tile reads before it
+// writes): its corners' tiles when it spans at most 2 tiles per axis, else
+// every tile.
+__device__ __forceinline__ void mark_box(const PhotonParams& p, uint32_t* smask, int x0, int y0, int x1, int y1) {
+    const int tx0 = x0 >> 3, ty0 = y0 >> 3, tx1 = x1 >> 3, ty1 = y1 >> 3;
+    if (tx1 - tx0 <= 1 && ty1 - ty0 <= 1) {
+        mark_tile(p, smask, (uint32_t)(ty0 * (int)p.tiles_x + tx0));
+        mark_tile(p, smask, (uint32_t)(ty0 * (int)p.tiles_x + tx1));
+        mark_tile(p, smask, (uint32_t)(ty1 * (int)p.tiles_x + tx0));
+        mark_tile(p, smask, (uint32_t)(ty1 * (int)p.tiles_x + tx1));
+    } else {
+        for (int ty = ty0; ty <= ty1; ++ty)
+            for (int tx = tx0; tx <= tx1; ++tx) mark_tile(p, smask, (uint32_t)(ty * (int)p.tiles_x + tx));
+    }
+}
+
 // Per-step setup (volume.rs:268-300), one lane per step: the step point, its
 // projection, z-test, camera-connection weight and projected beam radius.
 template <bool SPEC, bool COUNT>
-__device__ __forceinline__ StepRec beam_step(const PhotonParams& p, const BeamSeg& B, float4 pay, uint32_t k,
-                                             BeamCounts& cnt) {
+__device__ __forceinline__ StepRec beam_step(const PhotonParams& p, uint32_t* smask, const BeamSeg& B, float4 pay,
+                                             uint32_t k, BeamCounts& cnt) {
     StepRec R;
     R.valid = 0u;
     const float dist = ((float)k + 0.5f) * B.ds;
@@ -152,6 +169,7 @@ __device__ __forceinline__ StepRec beam_step(const PhotonParams& p, const BeamSe
         }
     }
     R.valid = wsum > 0.0f ? 1u : 2u;
+    if (!COUNT) mark_box(p, smask, x0, y0, x1, y1);  // covers the centre pixel of an empty tent too
     R.inv_wsum = wsum > 0.0f ? 1.0f / wsum : 0.0f;
     return R;
 }
@@ -167,21 +185,6 @@ __device__ __forceinline__ void deposit_pixel(const PhotonParams& p, uint32_t px
         red_u64(c, to_fixed(R.c0 * w, p.scale));
         red_u64(c + 1, to_fixed(R.c1 * w, p.scale));
         red_u64(c + 2, to_fixed(R.c2 * w, p.scale));
-    }
-}
-
-// Dirty bits of the tiles under a footprint box: its corners' tiles when it
-// spans at most 2 tiles per axis, else every tile.
-__device__ __forceinline__ void mark_box(const PhotonParams& p, uint32_t* smask, int x0, int y0, int x1, int y1,
-                                         uint32_t lane) {
-    const int tx0 = x0 >> 3, ty0 = y0 >> 3, tx1 = x1 >> 3, ty1 = y1 >> 3;
-    if (tx1 - tx0 <= 1 && ty1 - ty0 <= 1) {
-        if (lane < 4u)
-            mark_tile(p, smask, (uint32_t)(((lane & 2u) ? ty1 : ty0) * (int)p.tiles_x + ((lane & 1u) ? tx1 : tx0)));
-    } else {
-        const int ntx = tx1 - tx0 + 1, nt = ntx * (ty1 - ty0 + 1);
-        for (int i = (int)lane; i < nt; i += 32)
-            mark_tile(p, smask, (uint32_t)((ty0 + i / ntx) * (int)p.tiles_x + tx0 + i % ntx));
     }
 }
 
@@ -226,16 +229,13 @@ __device__ __forceinline__ bool runnable(const StepRec& R) {
 }
 
 template <bool SPEC>
-__device__ __forceinline__ void run_add(const PhotonParams& p, uint32_t* smask, BoxRun& run, const StepRec& R,
-                                        uint32_t lane) {
+__device__ __forceinline__ void run_add(const PhotonParams& p, BoxRun& run, const StepRec& R, uint32_t lane) {
     const uint32_t bin = SPEC ? R.bin : 0u;
     if (R.x0y0 != run.x0y0 || R.box != run.box || bin != run.bin) {
         run_flush<SPEC>(p, run, lane);
         run.x0y0 = R.x0y0; run.box = R.box; run.bin = bin;
 #pragma unroll
         for (int k = 0; k < 2; ++k) run.acc[k][0] = run.acc[k][1] = run.acc[k][2] = 0ull;
-        const int x0 = (int)(R.x0y0 & 0xFFFFu), y0 = (int)(R.x0y0 >> 16);
-        mark_box(p, smask, x0, y0, x0 + (int)(R.box & 0xFFu) - 1, y0 + (int)((R.box >> 8) & 0xFFu) - 1, lane);
     }
     const int x0 = (int)(R.x0y0 & 0xFFFFu), y0 = (int)(R.x0y0 >> 16);
     const int bw = (int)(R.box & 0xFFu), bh = (int)((R.box >> 8) & 0xFFu), rows = (int)((R.box >> 16) & 0xFFu);
@@ -261,17 +261,15 @@ __device__ __forceinline__ void run_add(const PhotonParams& p, uint32_t* smask, 
 // splat_transverse (volume.rs:174-218) by the whole warp, its tent sum already
 // known: lanes cover the footprint box (rows packed 32 / width at a time, or
 // 32-column chunks of one row for boxes wider than 32) and deposit their pixels'
-// renormalised shares; tiles under the box are marked dirty once.
+// renormalised shares (the step's lane marked the tiles under the box).
 template <bool SPEC, bool COUNT>
-__device__ __forceinline__ void splat_warp(const PhotonParams& p, uint32_t* smask, const StepRec& R, uint32_t lane,
-                                           BeamCounts& cnt) {
+__device__ __forceinline__ void splat_warp(const PhotonParams& p, const StepRec& R, uint32_t lane, BeamCounts& cnt) {
     const float cx = R.cx, cy = R.cy;
     if (R.valid == 2u) {  // empty tent sum: the whole colour to the centre pixel
         if (lane == 0) {
             const uint32_t px = (uint32_t)min(max((int)roundf(cx), 0), (int)p.width - 1);
             const uint32_t py = (uint32_t)min(max((int)roundf(cy), 0), (int)p.height - 1);
             if (COUNT) { ++cnt.deposits; return; }
-            mark_tile(p, smask, film_tile(px, py, p.tiles_x));
             deposit_pixel<SPEC>(p, px, py, R, 1.0f);
         }
         return;
@@ -281,7 +279,6 @@ __device__ __forceinline__ void splat_warp(const PhotonParams& p, uint32_t* smas
     const int bw = (int)(box & 0xFFu), bh = (int)((box >> 8) & 0xFFu), rows = (int)((box >> 16) & 0xFFu);
     const int x1 = x0 + bw - 1, y1 = y0 + bh - 1;
     const float inv_r = R.inv_r, inv = R.inv_wsum;
-    if (!COUNT) mark_box(p, smask, x0, y0, x1, y1, lane);
     const int lrow = bw <= 32 ? (int)((lane * R.magic) >> 16) : 0;
     const int lcol = (int)lane - lrow * bw;
     if (lrow >= rows) return;
@@ -333,7 +330,7 @@ __device__ __forceinline__ void beam_flush(const PhotonParams& p, BeamWarpSmem& 
                 if (ws.start[mid] <= t) lo = mid; else hi = mid;
             }
             const BeamSeg B = ws.seg[lo];
-            R = beam_step<SPEC, COUNT>(p, B, ws.payload[B.lane], t - ws.start[lo], cnt);
+            R = beam_step<SPEC, COUNT>(p, smask, B, ws.payload[B.lane], t - ws.start[lo], cnt);
         }
         ws.step[lane] = R;
         unsigned todo = __ballot_sync(0xffffffffu, R.valid != 0u);
@@ -343,12 +340,12 @@ __device__ __forceinline__ void beam_flush(const PhotonParams& p, BeamWarpSmem& 
         while (todo) {
             const uint32_t j = __ffs(todo) - 1u;
             todo &= todo - 1u;
-            const StepRec& Rj = ws.step[j];  // fields read from shared memory as used
+            const StepRec Rj = ws.step[j];
             if (!COUNT && runnable(Rj)) {
-                run_add<SPEC>(p, smask, run, Rj, lane);
+                run_add<SPEC>(p, run, Rj, lane);
             } else {
                 if (!COUNT) run_flush<SPEC>(p, run, lane);
-                splat_warp<SPEC, COUNT>(p, smask, Rj, lane, cnt);
+                splat_warp<SPEC, COUNT>(p, Rj, lane, cnt);
             }
         }
         if (!COUNT) run_flush<SPEC>(p, run, lane);

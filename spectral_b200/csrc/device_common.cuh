@@ -231,6 +231,9 @@ __device__ __forceinline__ float phase_hg(float g, float cos_theta) {
 __device__ __forceinline__ unsigned long long to_fixed(float x, float scale) {
     float y = x * scale;
     if (!(y > 0.0f)) return 0ull;
+    // below 2^23 adding 2^23 rounds y to the nearest (even) integer in the
+    // mantissa, exactly as the conversion does, with two ALU operations
+    if (y < 8388608.0f) return (unsigned long long)(__float_as_uint(y + 8388608.0f) - 0x4B000000u);
     // below 2^31 the 32-bit conversion rounds identically and is cheaper
     if (y < 2147483648.0f) return (unsigned long long)(unsigned)__float2int_rn(y);
     y = fminf(y, 4.0e18f);

@@ -297,7 +297,8 @@ __global__ void __launch_bounds__(256) tr_accumulate(uint32_t first_pixel, uint3
     }
     if (j >= n_pixels) return;
     float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
-    for (uint32_t s = 0; s < spp; ++s) {
+#pragma unroll 8
+    for (uint32_t s = 0; s < spp; ++s) {  // loads run ahead; the adds stay in sample order
         const float* r = result + 3u * ((size_t)s * n_pixels + j);
         a0 += r[0]; a1 += r[1]; a2 += r[2];
     }
