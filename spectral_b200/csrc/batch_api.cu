@@ -55,6 +55,7 @@ struct sc_batch {
     // of pass k + 1.
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ran = nullptr, copied = nullptr;
+    cudaEvent_t uploaded = nullptr;  // orders a pass on a caller's stream after work on the batch's own stream
     std::mutex mu;
     std::vector<sc_scene_job> jobs;
     std::vector<JobGeom> geom;
@@ -256,6 +257,7 @@ int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs, cons
         if (b->copy_stream) cudaStreamDestroy(b->copy_stream);
         if (b->ran) cudaEventDestroy(b->ran);
         if (b->copied) cudaEventDestroy(b->copied);
+        if (b->uploaded) cudaEventDestroy(b->uploaded);
         delete b;
         return e == cudaErrorMemoryAllocation ? SC_E_NOMEM : SC_E_CUDA;
     };
@@ -264,6 +266,7 @@ int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs, cons
     if ((e = cudaStreamCreateWithFlags(&b->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
     if ((e = cudaEventCreateWithFlags(&b->ran, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
     if ((e = cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreateWithFlags(&b->uploaded, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
     if ((e = cudaEventRecord(b->ran, b->stream)) != cudaSuccess) return fail(e);
     if ((e = cudaEventRecord(b->copied, b->stream)) != cudaSuccess) return fail(e);
     if ((e = b->films.alloc(cells)) != cudaSuccess) return fail(e);
@@ -305,6 +308,7 @@ int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs, cons
         if (b->copy_stream) cudaStreamDestroy(b->copy_stream);
         if (b->ran) cudaEventDestroy(b->ran);
         if (b->copied) cudaEventDestroy(b->copied);
+        if (b->uploaded) cudaEventDestroy(b->uploaded);
         delete b;
         set_error("%s", msg.c_str());
         return rc;
@@ -329,6 +333,7 @@ int sc_batch_destroy(sc_batch* b) {
         if (b->copy_stream) cudaStreamDestroy(b->copy_stream);
         if (b->ran) cudaEventDestroy(b->ran);
         if (b->copied) cudaEventDestroy(b->copied);
+        if (b->uploaded) cudaEventDestroy(b->uploaded);
     }
     delete b;
     return SC_OK;
@@ -419,11 +424,8 @@ int sc_batch_run(sc_batch* b, void* stream) {
     BATCH_LOCK(b);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->stream;
     if (s != b->stream) {  // order after uploads made on the batch's own stream
-        cudaEvent_t ev;
-        SC_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        SC_CUDA(cudaEventRecord(ev, b->stream));
-        SC_CUDA(cudaStreamWaitEvent(s, ev, 0));
-        cudaEventDestroy(ev);
+        SC_CUDA(cudaEventRecord(b->uploaded, b->stream));
+        SC_CUDA(cudaStreamWaitEvent(s, b->uploaded, 0));
     }
     return b->run(s);
     SC_GUARD_END

@@ -473,12 +473,8 @@ size_t beam_smem(const PhotonParams& p, uint32_t mask_words) {
 }  // namespace
 
 int beam_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem) {
-    int n = 0;
-    const void* fn = reinterpret_cast<const void*>(beam_fn(spectral));
-    const size_t total = smem + 16 + 8 * sizeof(BeamWarpSmem);
-    if (total > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)shape.block, total) != cudaSuccess) return 1;
-    return n > 0 ? n : 1;
+    return occupancy_blocks(reinterpret_cast<const void*>(beam_fn(spectral)), (int)shape.block,
+                            smem + 16 + 8 * sizeof(BeamWarpSmem));
 }
 
 cudaError_t launch_beam_count(const PhotonParams& p, unsigned long long* out, uint32_t grid, cudaStream_t s) {

@@ -1,6 +1,9 @@
 // Film kernels: sensor reduction / drain, exposure, tonemap, Gaussian gather,
 // and the synthetic atomic-film splat.
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "internal.h"
 
@@ -310,18 +313,33 @@ size_t reduce_smem(uint32_t channels) {
 
 }  // namespace
 
+// Resident CTAs of a reduce kernel on the current device for `smem` bytes of
+// dynamic shared memory, worked out once per (device, kernel, size) (raising
+// the kernel's shared-memory limit on the way) and then served from a table.
+static uint32_t reduce_grid(const void* fn, int which, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, size_t>, uint32_t> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    const auto key = std::make_tuple(dev, which, smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kReduceThreads, smem);
+    const uint32_t grid = (uint32_t)sms * (uint32_t)(per_sm > 0 ? per_sm : 1);
+    cache.emplace(key, grid);
+    return grid;
+}
+
 cudaError_t launch_reduce(const ReduceParams& p, bool drain, cudaStream_t s) {
     const size_t smem = reduce_smem(p.channels);
     const uint32_t ntiles = p.tiles_x * p.tiles_y;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const void* fn = drain ? reinterpret_cast<const void*>(&reduce_kernel<true>)
                            : reinterpret_cast<const void*>(&reduce_kernel<false>);
-    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kReduceThreads, smem);
-    uint32_t grid = (uint32_t)sms * (uint32_t)(per_sm > 0 ? per_sm : 1);
+    uint32_t grid = reduce_grid(fn, drain ? 1 : 0, smem);
     if (grid > ntiles) grid = ntiles;
     if (grid == 0) return cudaSuccess;
     if (drain) reduce_kernel<true><<<grid, kReduceThreads, smem, s>>>(p);
@@ -333,15 +351,9 @@ cudaError_t launch_reduce_many(const FilmDesc* descs, uint32_t n_films, uint32_t
                                uint32_t max_channels, cudaStream_t s) {
     if (total_tiles == 0) return cudaSuccess;
     const size_t smem = reduce_smem(max_channels);
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const void* fn = drain ? reinterpret_cast<const void*>(&reduce_many_kernel<true>)
                            : reinterpret_cast<const void*>(&reduce_many_kernel<false>);
-    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kReduceThreads, smem);
-    uint32_t grid = (uint32_t)sms * (uint32_t)(per_sm > 0 ? per_sm : 1);
+    uint32_t grid = reduce_grid(fn, drain ? 3 : 2, smem);
     if (grid > total_tiles) grid = total_tiles;
     if (drain) reduce_many_kernel<true><<<grid, kReduceThreads, smem, s>>>(descs, n_films, total_tiles);
     else reduce_many_kernel<false><<<grid, kReduceThreads, smem, s>>>(descs, n_films, total_tiles);

@@ -47,6 +47,11 @@ uint32_t photon_mask_words(const PhotonParams& p);
 cudaError_t launch_photons(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s);
 cudaError_t launch_photon_debug(const PhotonParams& p, cudaStream_t s);
 cudaError_t launch_photon_count(const PhotonParams& p, unsigned long long* out, uint32_t grid, cudaStream_t s);
+// Resident CTAs per SM of kernel `fn` with `block` threads and `smem` bytes of
+// dynamic shared memory on the current device; the kernel's shared-memory
+// limit is raised the first time a size above 48 KB is asked for, and answers
+// are cached per (device, kernel, block, size).
+int occupancy_blocks(const void* fn, int block, size_t smem);
 int photon_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem);
 
 // Photon-beam estimator (beam.cu): same transport, each segment marched in

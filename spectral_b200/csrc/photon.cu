@@ -11,6 +11,10 @@
 // Splats land in a 64-bit fixed-point film with red.global.add.u64; the film is
 // tile-major (8x8 pixel tiles) and every touched tile raises a dirty flag so the
 // drain/reduce pass reads only tiles that received light.
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "photon_trace.cuh"
 
 namespace sc {
@@ -150,13 +154,26 @@ static PhotonKernelFn photon_fn(const LaunchShape& s, bool spec) {
 // Shared memory beyond scene + mask: one segment buffer per warp (8 warps).
 static size_t split_bytes(const LaunchShape& s) { return s.split ? 16 + 8 * sizeof(WarpSplitSmem) : 0; }
 
-int photon_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem) {
+int occupancy_blocks(const void* fn, int block, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, const void*, int, size_t>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    const auto key = std::make_tuple(dev, fn, block, smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
     int n = 0;
-    const void* fn = reinterpret_cast<const void*>(photon_fn(shape, spectral));
-    const size_t total = smem + split_bytes(shape);
-    if (total > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)shape.block, total) != cudaSuccess) return 1;
-    return n > 0 ? n : 1;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, block, smem) != cudaSuccess) return 1;
+    n = n > 0 ? n : 1;
+    cache.emplace(key, n);
+    return n;
+}
+
+int photon_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem) {
+    return occupancy_blocks(reinterpret_cast<const void*>(photon_fn(shape, spectral)), (int)shape.block,
+                            smem + split_bytes(shape));
 }
 
 uint32_t photon_mask_words(const PhotonParams& p) {
