@@ -222,6 +222,7 @@ int sc_ctx_destroy(sc_ctx* ctx) {
     {
         DeviceGuard g(ctx->device);
         ctx->cmf.reset();
+        ctx->binw_cache.clear();
     }
     delete ctx;
     return SC_OK;
@@ -745,24 +746,22 @@ int sc_sensor_reduce_device(sc_ctx* ctx, uint32_t w, uint32_t h, uint32_t channe
     DeviceGuard g(ctx->device);
     const FilmGeom fg = film_geom(w, h, channels);
     // Bin weights are cached per (bins, band) on the context.
-    static std::mutex cache_mu;
-    static std::map<std::tuple<sc_ctx*, uint32_t, float, float>, float*> cache;
     const float* binw = nullptr;
     if (channels != 3u) {
         if (lambda_min == 0.0f) lambda_min = 380.0f;
         if (lambda_max == 0.0f) lambda_max = 730.0f;
-        std::lock_guard<std::mutex> lk(cache_mu);
-        auto key = std::make_tuple(ctx, channels, lambda_min, lambda_max);
-        auto it = cache.find(key);
-        if (it == cache.end()) {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        const auto key = std::make_tuple(channels, lambda_min, lambda_max);
+        auto it = ctx->binw_cache.find(key);
+        if (it == ctx->binw_cache.end()) {
             std::vector<float> wv(3 * channels);
             bin_weights(ctx->tables, channels, lambda_min, lambda_max, wv.data());
-            float* dptr = nullptr;
-            SC_CUDA(cudaMalloc(&dptr, wv.size() * sizeof(float)));
-            SC_CUDA(cudaMemcpy(dptr, wv.data(), wv.size() * sizeof(float), cudaMemcpyHostToDevice));
-            it = cache.emplace(key, dptr).first;
+            std::unique_ptr<DevBuf<float>> buf(new DevBuf<float>());
+            SC_CUDA(buf->alloc(wv.size()));
+            SC_CUDA(cudaMemcpy(buf->p, wv.data(), wv.size() * sizeof(float), cudaMemcpyHostToDevice));
+            it = ctx->binw_cache.emplace(key, std::move(buf)).first;
         }
-        binw = it->second;
+        binw = it->second->p;
     }
     ReduceParams r;
     r.film = static_cast<unsigned long long*>(film_dev); r.flags = flags_dev; r.xyz = xyz_dev;

@@ -4,9 +4,12 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
+#include <tuple>
 
 #include <cuda_runtime.h>
 
@@ -85,4 +88,7 @@ struct sc_ctx {
     float tables[5 * 71];
     sc::DevBuf<float> cmf;  // 3 x 71 on the device
     std::mutex mu;
+    // bin-averaged CMF weights of spectral films reduced through the
+    // device-pointer API, per (bins, band); freed with the context
+    std::map<std::tuple<uint32_t, float, float>, std::unique_ptr<sc::DevBuf<float>>> binw_cache;
 };
