@@ -70,7 +70,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "serve", "tracer"], default="batch")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["atomics", "batch", "serve", "tracer"],
+                    default="batch")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps")
@@ -589,6 +590,103 @@ def run_gpu_tracer(args, rank, world, local_rank):
     return line
 
 
+# Atomic-throughput workload: the AtomicFilm synthetic splat (vol_splat.wgsl
+# semantics: random pixel, three u32 atomics x4096), 2^24 splats per step into a
+# 1920x1080 film that stays in L2 -- the in-project measure of L2 atomic
+# throughput, the ceiling of the splat kernels' film atomics.
+ATOMICS = dict(width=1920, height=1080, splats=1 << 24, seed=0xA70)
+
+
+def run_gpu_atomics(args, rank, world, local_rank):
+    import torch
+    import spectral_b200 as sb
+    from spectral_b200 import _lib
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ctx = sb.GpuContext(local_rank)
+    W, H, N = ATOMICS["width"], ATOMICS["height"], ATOMICS["splats"]
+    f = sb.AtomicFilm(ctx, W, H)
+    sp = C.c_void_p()
+    _lib.check(_lib.lib.sc_atomic_film_stream(f.h, C.byref(sp)))
+    st = torch.cuda.ExternalStream(sp.value, device=dev)
+    for k in range(args.warmup):
+        f.splat(ATOMICS["seed"] + k, N)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    with ClockSampler(uuid) as clk, torch.cuda.nvtx.range("timed"):  # nvtx range for ncu --nvtx-include
+        for k in range(args.steps):
+            ev[k][0].record(st)
+            f.splat(ATOMICS["seed"] + 1000 + k, N)
+            ev[k][1].record(st)
+        torch.cuda.synchronize()
+    total_ms = sum(ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps))
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    atomics = 3 * N
+    value = atomics * world * args.steps / (total_ms / 1e3)
+    # end to end: splat, then the raw film back to the host, every step
+    e2e_steps = args.e2e_steps or args.steps
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        f.splat(ATOMICS["seed"] + 2000 + k, N)
+        f.read_film_raw()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    f.close()
+    if rank != 0:
+        return None
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    step_s = total_ms / args.steps / 1e3
+    line = {
+        "metric": "L2 atomic throughput, u32 atomicAdd (AtomicFilm synthetic splat)",
+        "value": value, "unit": "atomics/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic (seeded splats)",
+        "config": {"workload": "atomics: %d splats x 3 u32 atomics per step into a %dx%d film (resident in L2)"
+                               % (N, W, H), "parallelism": "own film per rank, no collective"},
+        "e2e": {"value": atomics * world * e2e_steps / e2e_s, "unit": "atomics/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 3 * W * H * 4,
+                "path": "sc_atomic_film_splat + sc_atomic_film_read_raw (host u32 film)"},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": atomics * 4 / step_s / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": atomics * 4 / step_s / 1e9 / hbm, "traffic": None, "kernel": "synthetic_splat_kernel",
+                     "peak_source": "measured hbm_gbs" if peaks.get("hbm_gbs") else "fallback",
+                     "algorithmic": "4 B payload per atomic (the film stays in L2: this is the L2 atomic rate)"},
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        rate, done, dt = run_cpu_atomics(min(args.cpu_seconds, 5.0))
+        line["cpu_baseline"] = {"value": rate, "unit": "atomics/s", "cores": 1, "kind": "port",
+                                "sample": "%d x 2^20 splats on one host thread (%.1f s), %s" % (done, dt, cpu_model())}
+    return line
+
+
+def run_cpu_atomics(seconds):
+    """Atomics/s of the CPU restatement of the synthetic splat (serial, as the
+    film it restates is one buffer), over batches of 2^20 splats."""
+    import oracle
+    W, H = ATOMICS["width"], ATOMICS["height"]
+    film = np.zeros(3 * W * H, np.uint32)
+    n_cpu, done, t0 = 1 << 20, 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        oracle.lib.or_synthetic_splat(W, H, ATOMICS["seed"] + done, n_cpu, film.ctypes.data_as(C.POINTER(C.c_uint32)))
+        done += 1
+    dt = time.perf_counter() - t0
+    return 3 * n_cpu * done / dt, done, dt
+
+
 # Serving workload (config 5): Poisson arrivals at 200 req/s (a 15 s window of
 # the 60 s stream by default), prism scenes of the config-4 distribution,
 # 2^16-2^20 photons per frame, 30 % orbit sessions of 16-128 frames at 2 deg
@@ -872,7 +970,15 @@ def main():
             return 0
         rates = []
         per_step = max(1.0, args.cpu_seconds / max(1, args.steps))
-        if args.workload == "serve":
+        if args.workload == "atomics":
+            th = 1
+            for _ in range(args.steps):
+                rate, done, dt = run_cpu_atomics(per_step)
+                rates.append((3 * (1 << 20) * done, dt))
+            sample = "per step batches of 2^20 splats on one host thread for ~%.1f s" % per_step
+            metric = "L2 atomic throughput, u32 atomicAdd (AtomicFilm synthetic splat)"
+            cfg_line = {"workload": "atomics (see the GPU arm)", "splats_per_step": ATOMICS["splats"]}
+        elif args.workload == "serve":
             from spectral_b200.serve import poisson_requests
             reqs = [r[1] for r in poisson_requests(SERVE["rate"], SERVE["seconds"], SERVE["seed"])]
             run_cpu_batch(0.5, jobs=reqs)
@@ -916,7 +1022,8 @@ def main():
                         "film": [cfg["width"], cfg["height"], cfg["bins"]]}
         tot_n, tot_t = sum(n for n, _ in rates), sum(t for _, t in rates)
         value = tot_n / tot_t
-        unit, what = {"tracer": ("samples/s", "CpuTracer::accumulate"),
+        unit, what = {"atomics": ("atomics/s", "the synthetic splat of AtomicFilm"),
+                      "tracer": ("samples/s", "CpuTracer::accumulate"),
                       "beam": ("photons/s", "render_volumetric_scene (beam estimator)")}.get(
             args.workload, ("photons/s", "render_volumetric_scene_point"))
         line = {"metric": metric, "value": value,
@@ -934,7 +1041,8 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = {"batch": run_gpu_batch, "serve": run_gpu_serve, "tracer": run_gpu_tracer}.get(
+    line = {"atomics": run_gpu_atomics, "batch": run_gpu_batch, "serve": run_gpu_serve,
+            "tracer": run_gpu_tracer}.get(
         args.workload, run_gpu)(args, rank, world, local_rank)
     if world > 1:
         import torch.distributed as dist

@@ -215,6 +215,9 @@ int sc_atomic_film_resolve(sc_atomic_film* f);
 int sc_atomic_film_read_accum(sc_atomic_film* f, float* out);
 int sc_atomic_film_clear_film(sc_atomic_film* f);
 int sc_atomic_film_clear_accum(sc_atomic_film* f);
+/* The CUDA stream (cudaStream_t) this film's work runs on, for callers that
+ * order or time their own work against it.  Owned by the film. */
+int sc_atomic_film_stream(sc_atomic_film* f, void** stream);
 /* check_determinism (film.rs:282-305): returns SC_OK and *first_diff=-1 when identical. */
 int sc_atomic_film_check_determinism(sc_ctx* ctx, uint32_t width, uint32_t height, uint32_t seed,
                                      uint32_t n_splats, int64_t* first_diff);

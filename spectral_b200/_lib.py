@@ -162,6 +162,7 @@ PROTOTYPES = {
     "sc_atomic_film_clear_film": (_i32, [_vp]),
     "sc_atomic_film_clear_accum": (_i32, [_vp]),
     "sc_atomic_film_check_determinism": (_i32, [_vp, _u32, _u32, _u32, _u32, P(_i64)]),
+    "sc_atomic_film_stream": (_i32, [_vp, P(_vp)]),
     "sc_lighttrace": (_i32, [_vp, P(sc_primitive), _u32, P(sc_plane), _u32, P(sc_material), _u32, P(sc_screen),
                              _u32, _u32, P(sc_beam), _u32, _u32, P(sc_film_options), P(_f32)]),
     "sc_scene_zbuffer": (_i32, [_vp, P(sc_primitive), _u32, P(sc_plane), _u32, P(sc_material), _u32, P(sc_screen),

@@ -839,6 +839,13 @@ int sc_atomic_film_splat(sc_atomic_film* f, uint32_t seed, uint32_t n) {
     return SC_OK;
     SC_GUARD_END
 }
+int sc_atomic_film_stream(sc_atomic_film* f, void** stream) {
+    SC_GUARD_BEGIN
+    SC_REQUIRE(f && stream, SC_E_INVALID, "null argument");
+    *stream = f->stream;
+    return SC_OK;
+    SC_GUARD_END
+}
 int sc_atomic_film_read_raw(sc_atomic_film* f, uint32_t* out) {
     SC_GUARD_BEGIN
     AFILM_LOCK(f);
