@@ -91,6 +91,13 @@ int sc_camera_look_at(const float origin[3], const float target[3], const float 
                       float vfov_deg, float aspect, sc_camera* out);
 /* Glass::n (spectral-core/src/sellmeier.rs:28-44), f64 internally. */
 float sc_glass_n(uint32_t glass, float lambda_nm);
+/* Glass::n over an array on the host: out[i] = sc_glass_n(glass, lambda_nm[i]).
+ * glass 0 BK7, 1 SF11, 2 water, 3 fused silica; others return SC_E_INVALID. */
+int sc_glass_n_many(uint32_t glass, const float* lambda_nm, size_t n, float* out);
+/* The same with the kernels' own device code over device arrays, on `stream`
+ * (asynchronous; n <= 2^31). */
+int sc_glass_n_device(sc_ctx* ctx, uint32_t glass, const float* lambda_nm_dev, size_t n, float* out_dev,
+                      void* stream);
 /* Device RNG stream: n draws of PathRng(key, seed).next_u32() computed on the GPU
  * into host `out` (the kernel of spectral-gpu/tests/rng_parity.rs:4-16). */
 int sc_rng_draws(sc_ctx* ctx, uint32_t key, uint32_t seed, uint32_t n, uint32_t* out);

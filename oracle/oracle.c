@@ -80,6 +80,10 @@ float or_glass_n(uint32_t glass, float nm) {
     return (float)sqrt(n2);
 }
 
+void or_glass_n_many(uint32_t glass, const float* nm, size_t n, float* out) {
+    for (size_t i = 0; i < n; ++i) out[i] = or_glass_n(glass, nm[i]);
+}
+
 /* ------------------------------------------------------------------------ */
 /* cie.rs:17-144                                                             */
 /* ------------------------------------------------------------------------ */

@@ -141,7 +141,15 @@ class VolWeights:
 
 
 def glass_n(glass, lambda_nm):
-    return lib.sc_glass_n(int(glass), float(lambda_nm))
+    """Glass::n (spectral-core/src/sellmeier.rs:28-44) of one wavelength in nm,
+    or, for an array, of every element (float32 array of the same shape)."""
+    if np.ndim(lambda_nm) == 0:
+        return lib.sc_glass_n(int(glass), float(lambda_nm))
+    lam = np.ascontiguousarray(lambda_nm, dtype=np.float32)
+    out = np.empty_like(lam)
+    check(lib.sc_glass_n_many(int(glass), lam.ctypes.data_as(C.POINTER(C.c_float)), lam.size,
+                              out.ctypes.data_as(C.POINTER(C.c_float))))
+    return out
 
 
 def dsotm_scene(aspect=1.0):

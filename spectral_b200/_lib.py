@@ -114,6 +114,8 @@ PROTOTYPES = {
     "sc_load_sensor_tables": (_i32, [C.c_char_p, P(_f32)]),
     "sc_camera_look_at": (_i32, [P(_f32), P(_f32), P(_f32), _f32, _f32, P(sc_camera)]),
     "sc_glass_n": (_f32, [_u32, _f32]),
+    "sc_glass_n_many": (_i32, [_u32, P(_f32), C.c_size_t, P(_f32)]),
+    "sc_glass_n_device": (_i32, [_vp, _u32, _vp, C.c_size_t, _vp, _vp]),
     "sc_rng_draws": (_i32, [_vp, _u32, _u32, _u32, P(_u32)]),
     "sc_dsotm_scene": (_i32, [_f32, P(sc_primitive), P(sc_plane), P(sc_material), P(sc_beam), P(sc_camera)]),
     "sc_photon_film_create": (_i32, [_vp, P(sc_primitive), _u32, P(sc_plane), _u32, P(sc_material), _u32, _f32,

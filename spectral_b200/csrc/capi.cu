@@ -263,6 +263,29 @@ int sc_camera_look_at(const float origin[3], const float target[3], const float 
 
 float sc_glass_n(uint32_t glass, float lambda_nm) { return glass_n(glass, lambda_nm); }
 
+int sc_glass_n_many(uint32_t glass, const float* lambda_nm, size_t n, float* out) {
+    SC_GUARD_BEGIN
+    SC_REQUIRE(glass <= 3u, SC_E_INVALID, "glass %u", glass);
+    SC_REQUIRE((lambda_nm && out) || n == 0, SC_E_INVALID, "null argument");
+    for (size_t i = 0; i < n; ++i) out[i] = glass_n(glass, lambda_nm[i]);
+    return SC_OK;
+    SC_GUARD_END
+}
+
+int sc_glass_n_device(sc_ctx* ctx, uint32_t glass, const float* lambda_nm_dev, size_t n, float* out_dev,
+                      void* stream) {
+    SC_GUARD_BEGIN
+    SC_REQUIRE(ctx, SC_E_INVALID, "null context");
+    SC_REQUIRE(glass <= 3u, SC_E_INVALID, "glass %u", glass);
+    SC_REQUIRE((lambda_nm_dev && out_dev) || n == 0, SC_E_INVALID, "null argument");
+    SC_REQUIRE(n <= (size_t(1) << 31), SC_E_LIMIT, "n %zu > 2^31", n);
+    if (n == 0) return SC_OK;
+    DeviceGuard g(ctx->device);
+    SC_CUDA(launch_glass_n(glass, lambda_nm_dev, (uint32_t)n, out_dev, static_cast<cudaStream_t>(stream)));
+    return SC_OK;
+    SC_GUARD_END
+}
+
 int sc_rng_draws(sc_ctx* ctx, uint32_t key, uint32_t seed, uint32_t n, uint32_t* out) {
     SC_GUARD_BEGIN
     SC_REQUIRE(ctx && (out || n == 0), SC_E_INVALID, "null argument");

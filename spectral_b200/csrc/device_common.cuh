@@ -49,25 +49,49 @@ struct Rng {
 };
 
 // ---- dispersion: glass 0 BK7, 1 SF11, 2 water (Cauchy), 3 fused silica ----
-__host__ __device__ __forceinline__ float glass_n(uint32_t glass, float nm) {
+struct Sellmeier { double b0, b1, b2, c0, c1, c2; };
+__host__ __device__ __forceinline__ Sellmeier sellmeier_coef(uint32_t glass) {
+    if (glass == 0u) return {1.03961212, 0.231792344, 1.01046945, 0.00600069867, 0.0200179144, 103.560653};
+    if (glass == 1u) return {1.73759695, 0.313747346, 1.89878101, 0.013188707, 0.0623068142, 155.23629};
+    // Malitson (1965) fused silica
+    return {0.6961663, 0.4079426, 0.8974794, 0.0684043 * 0.0684043, 0.1162414 * 0.1162414, 9.896161 * 9.896161};
+}
+
+// Glass::n in the reference's operation order: l = nm / 1000, three divided
+// terms, sqrt, cast to f32 (spectral-core/src/sellmeier.rs:28-44).
+static __host__ __device__ __noinline__ float glass_n_ref(uint32_t glass, float nm) {
     double l_um = (double)nm / 1000.0;
     if (glass == 2u) return (float)(1.3238 + 0.00314 / (l_um * l_um));
     double l2 = l_um * l_um;
-    double b0, b1, b2, c0, c1, c2;
-    if (glass == 0u) {
-        b0 = 1.03961212; b1 = 0.231792344; b2 = 1.01046945;
-        c0 = 0.00600069867; c1 = 0.0200179144; c2 = 103.560653;
-    } else if (glass == 1u) {
-        b0 = 1.73759695; b1 = 0.313747346; b2 = 1.89878101;
-        c0 = 0.013188707; c1 = 0.0623068142; c2 = 155.23629;
-    } else {  // Malitson (1965) fused silica
-        b0 = 0.6961663; b1 = 0.4079426; b2 = 0.8974794;
-        c0 = 0.0684043 * 0.0684043; c1 = 0.1162414 * 0.1162414; c2 = 9.896161 * 9.896161;
-    }
-    double t0 = b0 * l2 / (l2 - c0);
-    double t1 = b1 * l2 / (l2 - c1);
-    double t2 = b2 * l2 / (l2 - c2);
+    const Sellmeier k = sellmeier_coef(glass);
+    double t0 = k.b0 * l2 / (l2 - k.c0);
+    double t1 = k.b1 * l2 / (l2 - k.c1);
+    double t2 = k.b2 * l2 / (l2 - k.c2);
     return (float)sqrt(1.0 + ((t0 + t1) + t2));
+}
+
+// Glass::n with one f64 division instead of four: the three Sellmeier terms
+// over a common denominator and nm^2 / 10^6 for the squared wavelength in um.
+// This f64 value differs from the reference-order one by a few f64 ulps
+// (below 2^-47 for n in [1, 2)).  Both round to the same f32 unless they lie
+// within that distance of a rounding midpoint (f +- 2^-24 for n in [1, 2)),
+// so the result is accepted only when it is more than 2^-40 away from both
+// midpoints and otherwise recomputed in the reference order (about one
+// evaluation in 2^16): the returned f32 is always the reference's.
+__host__ __device__ __forceinline__ float glass_n(uint32_t glass, float nm) {
+    const double x2 = (double)nm * (double)nm;  // exact
+    double n;
+    if (glass == 2u) {
+        n = 1.3238 + 3140.0 / x2;
+    } else {
+        const Sellmeier k = sellmeier_coef(glass);
+        const double l2 = x2 * 1e-6;
+        const double d0 = l2 - k.c0, d1 = l2 - k.c1, d2 = l2 - k.c2;
+        n = sqrt(1.0 + l2 * ((k.b0 * d1 + k.b1 * d0) * d2 + k.b2 * (d0 * d1)) / ((d0 * d1) * d2));
+    }
+    const float f = (float)n;
+    if (f >= 1.0f && f < 2.0f && fabs(n - (double)f) < 0x1p-24 - 0x1p-40) return f;
+    return glass_n_ref(glass, nm);
 }
 
 // ---- sensor table lerp, clamped (spectral-core/src/cie.rs:47-61) ----------

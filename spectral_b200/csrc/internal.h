@@ -74,6 +74,7 @@ struct RimParams {
 };
 cudaError_t launch_rim(const RimParams& p, cudaStream_t s);
 cudaError_t launch_rng_draws(uint32_t key, uint32_t seed, uint32_t n, uint32_t* out, cudaStream_t s);
+cudaError_t launch_glass_n(uint32_t glass, const float* lambda_nm, uint32_t n, float* out, cudaStream_t s);
 
 // Film reduction: tile-major int64 film -> interleaved f32 XYZ (3*w*h).
 struct ReduceParams {

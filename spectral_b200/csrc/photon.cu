@@ -125,7 +125,19 @@ __global__ void rng_draws_kernel(uint32_t key, uint32_t seed, uint32_t n, uint32
     for (uint32_t i = 0; i < n; ++i) out[i] = r.u32();
 }
 
+__global__ void glass_n_kernel(uint32_t glass, const float* __restrict__ lambda_nm, uint32_t n,
+                               float* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = glass_n(glass, lambda_nm[i]);
+}
+
 }  // namespace
+
+cudaError_t launch_glass_n(uint32_t glass, const float* lambda_nm, uint32_t n, float* out, cudaStream_t s) {
+    const uint32_t need = (n + 255u) / 256u, grid = need < 148u * 16u ? need : 148u * 16u;
+    glass_n_kernel<<<grid, 256, 0, s>>>(glass, lambda_nm, n, out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_rng_draws(uint32_t key, uint32_t seed, uint32_t n, uint32_t* out, cudaStream_t s) {
     rng_draws_kernel<<<1, 32, 0, s>>>(key, seed, n, out);

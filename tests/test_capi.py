@@ -58,6 +58,23 @@ def test_glass_index_bitwise_equals_oracle():
             assert x.tobytes() == y.tobytes(), (g, nm)
 
 
+def _all_f32(lo, hi):
+    return np.arange(np.float32(lo).view(np.uint32), np.float32(hi).view(np.uint32) + 1,
+                     dtype=np.uint32).view(np.float32)
+
+
+def test_glass_index_every_f32_wavelength_equals_oracle():
+    # every f32 wavelength of 380-780 nm (8.7 M values): the single-division
+    # Sellmeier sum with its midpoint check returns the reference-order f32
+    lam = _all_f32(380.0, 780.0)
+    for g in range(4):
+        got, ref = sb.glass_n(g, lam), np.empty_like(lam)
+        oracle.lib.or_glass_n_many(g, oracle.fp(lam), lam.size, oracle.fp(ref))
+        assert got.tobytes() == ref.tobytes(), (g, int((got != ref).sum()))
+    with pytest.raises(_lib.SpectralError):
+        sb.glass_n(4, lam[:4])
+
+
 def test_sensor_tables_equal_oracle():
     assert sb.sample_tables().tobytes() == oracle.tables().tobytes()
 

@@ -41,6 +41,24 @@ def test_rng_stream_bit_identical(ctx):
     assert list(cpu) == list(gpu)
 
 
+def test_glass_index_device_every_f32_wavelength(ctx):
+    # the kernels' own device code on every f32 wavelength of 380-780 nm
+    import torch
+    lam = np.arange(np.float32(380.0).view(np.uint32), np.float32(780.0).view(np.uint32) + 1,
+                    dtype=np.uint32).view(np.float32)
+    d_lam = torch.from_numpy(lam).cuda()
+    d_out = torch.empty_like(d_lam)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for g in range(4):
+        _lib.check(_lib.lib.sc_glass_n_device(ctx.h, g, C.c_void_p(d_lam.data_ptr()), lam.size,
+                                              C.c_void_p(d_out.data_ptr()), stream))
+        torch.cuda.synchronize()
+        ref = np.empty_like(lam)
+        oracle.lib.or_glass_n_many(g, oracle.fp(lam), lam.size, oracle.fp(ref))
+        got = d_out.cpu().numpy()
+        assert got.tobytes() == ref.tobytes(), (g, int((got != ref).sum()))
+
+
 def run_parity_for_beam(ctx, beam, seed, count, label, spectral=True, max_bounces=8):
     scene, _, cam = sb.dsotm_scene(1.0)
     film = sb.GpuPhotonFilm(ctx, scene, cam, beam, 256, 256, count, seed, 14.0, sb.VolWeights(),
