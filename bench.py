@@ -744,7 +744,7 @@ def run_gpu_serve(args, rank, world, local_rank):
         "e2e": {"value": total_rate, "unit": "photons/s", "h2d_bytes_per_step": in_bytes,
                 "d2h_bytes_per_step": out_bytes,
                 "path": "sc_server_submit per request, sc_server_step, sc_server_poll with the XYZ image to host"},
-        "gpu_launches": served["steps"],
+        "gpu_launches": served["steps"] * 3,  # per server step: batch_kernel, reduce_scan, reduce_list
         "clocks": clk.summary(),
     }
 
@@ -933,9 +933,9 @@ def run_gpu_batch(args, rank, world, local_rank):
                 "d2h_bytes_per_step": b.xyz_floats * 4,
                 "path": "sc_batch_update_jobs + sc_batch_run + sc_batch_read_all_xyz_async (pinned host; the "
                         "copy of a pass overlaps the next pass's tracing), all steps synchronised at the end"},
-        "gpu_launches": args.steps * 2,
+        "gpu_launches": args.steps * 3,  # per pass: batch_kernel, reduce_scan, reduce_list
         "work": stats,
-        "roofline": {"bound": "hbm", "kernel": "batch_kernel + reduce_many (one pass)",
+        "roofline": {"bound": "hbm", "kernel": "batch_kernel + reduce_scan + reduce_list (one pass)",
                      "achieved": (stats["in_frame_samples"] * 8 + 2 * stats["dirty_tile_bytes"] +
                                   b.xyz_floats * 4) / step_s / 1e9,
                      "peak": hbm, "unit": "GB/s", "traffic": None, "peak_source": "%s hbm_gbs" % peak_note,

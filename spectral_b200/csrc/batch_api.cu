@@ -66,9 +66,10 @@ struct sc_batch {
     DevBuf<BatchJobDev> d_jobs;
     DevBuf<WorkItem> d_items;
     DevBuf<FilmDesc> d_descs;
-    DevBuf<uint32_t> counter;
+    DevBuf<DirtyTile> dirty_list;  // reduce scratch: room for every tile, and its counter
+    DevBuf<uint32_t> counter, dirty_count;
     std::vector<BatchJobDev> h_jobs;
-    uint32_t n_items = 0, total_tiles = 0, max_channels = 0;
+    uint32_t n_items = 0, total_tiles = 0, total_words = 0, max_channels = 0;
     uint64_t total_photons = 0;
     sc_batch_tuning tuning{};
     uint32_t grid = 0;
@@ -167,7 +168,8 @@ struct sc_batch {
                              (int)tuning.aggregate, (int)tuning.minb, tuning.per_photon ? 0 : 1, grid, s));
         // the drain rewrites the images: wait for the last asynchronous copy of them
         SC_CUDA(cudaStreamWaitEvent(s, copied, cudaEventWaitExternal));
-        SC_CUDA(launch_reduce_many(d_descs.p, (uint32_t)jobs.size(), total_tiles, true, max_channels, s));
+        SC_CUDA(launch_reduce_many(d_descs.p, (uint32_t)jobs.size(), total_words, true, max_channels, dirty_list.p,
+                                   dirty_count.p, s));
         return SC_OK;
     }
 
@@ -250,6 +252,7 @@ int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs, cons
         b->total_photons += jobs[i].n_photons;
     }
     b->total_tiles = tiles;
+    b->total_words = (uint32_t)words;
     DeviceGuard g(ctx->device);
     auto fail = [&](cudaError_t e) {
         set_error("batch setup failed: %s", cudaGetErrorString(e));
@@ -276,12 +279,13 @@ int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs, cons
     if ((e = b->d_jobs.alloc(n_jobs)) != cudaSuccess) return fail(e);
     if ((e = b->d_descs.alloc(n_jobs)) != cudaSuccess) return fail(e);
     if ((e = b->counter.alloc(1)) != cudaSuccess) return fail(e);
+    if ((e = b->dirty_list.alloc(tiles)) != cudaSuccess) return fail(e);
+    if ((e = b->dirty_count.alloc(1)) != cudaSuccess) return fail(e);
     if ((e = cudaMemsetAsync(b->films.p, 0, b->films.bytes(), b->stream)) != cudaSuccess) return fail(e);
     if ((e = cudaMemsetAsync(b->flags.p, 0, b->flags.bytes(), b->stream)) != cudaSuccess) return fail(e);
     if ((e = cudaMemsetAsync(b->xyz.p, 0, b->xyz.bytes(), b->stream)) != cudaSuccess) return fail(e);
     std::vector<float> hw(bw);
     std::vector<FilmDesc> descs(n_jobs);
-    uint32_t tb = 0;
     for (uint32_t i = 0; i < n_jobs; ++i) {
         const sc_film_options& o = jobs[i].opts;
         bin_weights(ctx->tables, o.bins, o.lambda_min ? o.lambda_min : 380.0f, o.lambda_max ? o.lambda_max : 730.0f,
@@ -290,9 +294,8 @@ int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs, cons
         d.film = b->films.p + b->film_off[i]; d.flags = b->flags.p + b->flag_off[i]; d.xyz = b->xyz.p + b->xyz_off[i];
         d.binw = b->binw.p + b->binw_off[i];
         d.width = b->geom[i].w; d.height = b->geom[i].h; d.tiles_x = b->geom[i].tiles_x; d.tiles_y = b->geom[i].tiles_y;
-        d.channels = b->geom[i].channels; d.tile_begin = tb;
+        d.channels = b->geom[i].channels; d.word_begin = (uint32_t)b->flag_off[i];
         d.inv_scale = std::ldexp(1.0, -(int)(o.scale_log2 ? o.scale_log2 : 32u));
-        tb += d.tiles_x * d.tiles_y;
     }
     if ((e = cudaMemcpyAsync(b->binw.p, hw.data(), bw * sizeof(float), cudaMemcpyHostToDevice, b->stream)) != cudaSuccess)
         return fail(e);
@@ -526,8 +529,8 @@ int sc_batch_stats(sc_batch* b, uint64_t out[6]) {
         dirty += dj;
         dirty_bytes += dj * kTilePixels * b->geom[j].channels * 8u;
     }
-    SC_CUDA(launch_reduce_many(b->d_descs.p, (uint32_t)b->jobs.size(), b->total_tiles, true, b->max_channels,
-                               b->stream));
+    SC_CUDA(launch_reduce_many(b->d_descs.p, (uint32_t)b->jobs.size(), b->total_words, true, b->max_channels,
+                               b->dirty_list.p, b->dirty_count.p, b->stream));
     SC_CUDA(cudaStreamSynchronize(b->stream));
     out[0] = c[0]; out[1] = c[1]; out[2] = c[2]; out[3] = c[3]; out[4] = dirty; out[5] = dirty_bytes;
     return SC_OK;

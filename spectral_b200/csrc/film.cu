@@ -153,32 +153,73 @@ __global__ void __launch_bounds__(kReduceThreads, 3) reduce_kernel(const ReduceP
         sm, part);
 }
 
-// Many films in one persistent launch: global tile index -> (film, tile) by a
-// binary search over the films' tile prefix.
+// Many films, step 1: one warp per dirty-mask word (32 tiles).  Clean tiles get
+// zeros in the image; dirty ones go to the list (one atomic per warp), and
+// when draining the word is cleared.  Words are numbered over all films
+// (FilmDesc::word_begin), so a warp finds its film by a binary search.
 template <bool DRAIN>
-__global__ void __launch_bounds__(kReduceThreads, 3) reduce_many_kernel(const FilmDesc* __restrict__ descs, uint32_t n_films,
-                                                                     uint32_t total_tiles) {
+__global__ void __launch_bounds__(256) reduce_scan_kernel(const FilmDesc* __restrict__ descs, uint32_t n_films,
+                                                          uint32_t total_words, DirtyTile* __restrict__ list,
+                                                          uint32_t* __restrict__ count) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < total_words; w += warps) {
+        uint32_t lo = 0, hi = n_films;
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (descs[mid].word_begin <= w) lo = mid; else hi = mid;
+        }
+        const FilmDesc& d = descs[lo];
+        const uint32_t wl = w - d.word_begin;
+        const uint32_t bits = d.flags[wl];
+        const uint32_t tile = wl * 32u + lane;
+        const bool valid = tile < d.tiles_x * d.tiles_y;
+        const bool dirty = valid && ((bits >> lane) & 1u);
+        const unsigned dm = __ballot_sync(0xffffffffu, dirty);
+        if (dm) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(count, (uint32_t)__popc(dm));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (dirty) list[base + __popc(dm & ((1u << lane) - 1u))] = DirtyTile{lo, tile};
+            if (DRAIN && lane == 0) d.flags[wl] = 0u;
+        }
+        // zeros for the clean tiles: 8 rows x 24 floats each, 6 coalesced stores per lane
+        for (unsigned cm = __ballot_sync(0xffffffffu, valid && !dirty); cm; cm &= cm - 1u) {
+            const uint32_t t = wl * 32u + (uint32_t)(__ffs(cm) - 1);
+            const uint32_t tx = t % d.tiles_x, ty = t / d.tiles_x;
+#pragma unroll
+            for (uint32_t k = 0; k < 6u; ++k) {
+                const uint32_t i = lane + 32u * k, row = i / 24u, col = i % 24u;
+                const uint32_t px = tx * 8u + col / 3u, py = ty * 8u + row;
+                if (px < d.width && py < d.height) d.xyz[((size_t)py * d.width + tx * 8u) * 3u + col] = 0.0f;
+            }
+        }
+    }
+}
+
+// Many films, step 2: the listed dirty tiles through the pipelined walk.
+template <bool DRAIN>
+__global__ void __launch_bounds__(kReduceThreads, 3) reduce_list_kernel(const FilmDesc* __restrict__ descs,
+                                                                     const DirtyTile* __restrict__ list,
+                                                                     const uint32_t* __restrict__ count) {
     extern __shared__ __align__(16) unsigned char smem[];
     double* part = reinterpret_cast<double*>(smem);
     unsigned long long* sm = reinterpret_cast<unsigned long long*>(smem + 4 * 64 * 3 * sizeof(double));
+    const uint32_t n = *count;
     reduce_walk<DRAIN>(
         [&](uint32_t k) {
-            const uint32_t g = blockIdx.x + k * gridDim.x;
+            const uint32_t i = blockIdx.x + k * gridDim.x;
             ReduceParams p;
-            if (g >= total_tiles) {
+            if (i >= n) {
                 p = ReduceParams{};
                 return tile_ref(p, 0u, false);
             }
-            uint32_t lo = 0, hi = n_films;
-            while (hi - lo > 1u) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (descs[mid].tile_begin <= g) lo = mid; else hi = mid;
-            }
-            const FilmDesc& d = descs[lo];
-            p.film = d.film; p.flags = d.flags; p.xyz = d.xyz; p.width = d.width; p.height = d.height;
+            const DirtyTile e = list[i];
+            const FilmDesc& d = descs[e.film];
+            p.film = d.film; p.flags = nullptr; p.xyz = d.xyz; p.width = d.width; p.height = d.height;
             p.tiles_x = d.tiles_x; p.tiles_y = d.tiles_y; p.channels = d.channels; p.binw = d.binw;
             p.inv_scale = d.inv_scale;
-            return tile_ref(p, g - d.tile_begin, true);
+            return tile_ref(p, e.tile, true);
         },
         sm, part);
 }
@@ -347,16 +388,25 @@ cudaError_t launch_reduce(const ReduceParams& p, bool drain, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_reduce_many(const FilmDesc* descs, uint32_t n_films, uint32_t total_tiles, bool drain,
-                               uint32_t max_channels, cudaStream_t s) {
-    if (total_tiles == 0) return cudaSuccess;
+cudaError_t launch_reduce_many(const FilmDesc* descs, uint32_t n_films, uint32_t total_words, bool drain,
+                               uint32_t max_channels, DirtyTile* list, uint32_t* count, cudaStream_t s) {
+    if (total_words == 0 || n_films == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t need = (total_words + 7u) / 8u, cap = (uint32_t)sms * 8u;
+    const uint32_t sgrid = need < cap ? need : cap;
+    if (drain) reduce_scan_kernel<true><<<sgrid, 256, 0, s>>>(descs, n_films, total_words, list, count);
+    else reduce_scan_kernel<false><<<sgrid, 256, 0, s>>>(descs, n_films, total_words, list, count);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const size_t smem = reduce_smem(max_channels);
-    const void* fn = drain ? reinterpret_cast<const void*>(&reduce_many_kernel<true>)
-                           : reinterpret_cast<const void*>(&reduce_many_kernel<false>);
-    uint32_t grid = reduce_grid(fn, drain ? 3 : 2, smem);
-    if (grid > total_tiles) grid = total_tiles;
-    if (drain) reduce_many_kernel<true><<<grid, kReduceThreads, smem, s>>>(descs, n_films, total_tiles);
-    else reduce_many_kernel<false><<<grid, kReduceThreads, smem, s>>>(descs, n_films, total_tiles);
+    const void* fn = drain ? reinterpret_cast<const void*>(&reduce_list_kernel<true>)
+                           : reinterpret_cast<const void*>(&reduce_list_kernel<false>);
+    const uint32_t grid = reduce_grid(fn, drain ? 3 : 2, smem);
+    if (drain) reduce_list_kernel<true><<<grid, kReduceThreads, smem, s>>>(descs, list, count);
+    else reduce_list_kernel<false><<<grid, kReduceThreads, smem, s>>>(descs, list, count);
     return cudaGetLastError();
 }
 

@@ -90,11 +90,18 @@ cudaError_t launch_reduce(const ReduceParams& p, bool drain, cudaStream_t s);
 // Batched reduction over many films described in device memory.
 struct FilmDesc {
     unsigned long long* film; uint32_t* flags; float* xyz; const float* binw;
-    uint32_t width, height, tiles_x, tiles_y, channels, tile_begin;  // tile_begin: prefix over films
+    uint32_t width, height, tiles_x, tiles_y, channels;
+    uint32_t word_begin;  // prefix over films of their dirty-mask words
     double inv_scale;
 };
-cudaError_t launch_reduce_many(const FilmDesc* descs, uint32_t n_films, uint32_t total_tiles,
-                               bool drain, uint32_t max_channels, cudaStream_t s);
+struct DirtyTile { uint32_t film, tile; };
+// Two launches after zeroing `count`: a scan of every film's dirty-mask words
+// that writes zeros into the images of clean tiles and lists the dirty ones
+// (clearing their mask words when draining), then the pipelined reduction of
+// the listed tiles only.  Scratch: `list` with room for every tile of the
+// films, one counter.
+cudaError_t launch_reduce_many(const FilmDesc* descs, uint32_t n_films, uint32_t total_words, bool drain,
+                               uint32_t max_channels, DirtyTile* list, uint32_t* count, cudaStream_t s);
 
 cudaError_t launch_composite_max_y(const float* xyz, const float* surface, uint32_t n_pixels,
                                    uint32_t* out_bits, cudaStream_t s);

@@ -103,7 +103,8 @@ struct sc_server {
     DevBuf<BatchJobDev> d_jobs;
     DevBuf<FilmDesc> d_descs;
     DevBuf<WorkItem> d_items;
-    DevBuf<uint32_t> counter;
+    DevBuf<DirtyTile> dirty_list;  // reduce scratch, grown to the active films' tiles
+    DevBuf<uint32_t> counter, dirty_count;
     std::deque<Request*> queue;
     std::vector<Request*> active;
     std::deque<Request*> finished;
@@ -168,7 +169,7 @@ struct sc_server {
         h_jobs.resize(n);
         h_descs.resize(n);
         h_items.clear();
-        uint32_t tiles = 0, maxc = 0;
+        uint32_t tiles = 0, words = 0, maxc = 0;
         uint64_t step_photons = 0;
         std::vector<uint32_t> order(n);
         for (uint32_t i = 0; i < n; ++i) order[i] = i;
@@ -205,9 +206,10 @@ struct sc_server {
             FilmDesc& fd = h_descs[i];
             fd.film = p.film; fd.flags = p.flags; fd.xyz = xyz_ptr(q); fd.binw = binw_ptr(q);
             fd.width = J.width; fd.height = J.height; fd.tiles_x = q->tiles_x; fd.tiles_y = q->tiles_y;
-            fd.channels = J.opts.bins; fd.tile_begin = tiles;
+            fd.channels = J.opts.bins; fd.word_begin = words;
             fd.inv_scale = std::ldexp(1.0, -(int)(J.opts.scale_log2 ? J.opts.scale_log2 : 32u));
             tiles += q->tiles_x * q->tiles_y;
+            words += q->words;
             maxc = std::max(maxc, J.opts.bins);
             step_photons += J.n_photons;
         }
@@ -218,13 +220,14 @@ struct sc_server {
             for (uint32_t b = 0; b < N; b += chunk) h_items.push_back(WorkItem{i, base + b, std::min(chunk, N - b)});
         }
         if (d_items.n < h_items.size()) SC_CUDA(d_items.alloc(h_items.size() * 2));
+        if (dirty_list.n < tiles) SC_CUDA(dirty_list.alloc(tiles * 2ull));
         SC_CUDA(cudaMemcpyAsync(d_jobs.p, h_jobs.data(), n * sizeof(BatchJobDev), cudaMemcpyHostToDevice, stream));
         SC_CUDA(cudaMemcpyAsync(d_descs.p, h_descs.data(), n * sizeof(FilmDesc), cudaMemcpyHostToDevice, stream));
         SC_CUDA(cudaMemcpyAsync(d_items.p, h_items.data(), h_items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
                                 stream));
         SC_CUDA(launch_batch(d_jobs.p, d_items.p, (uint32_t)h_items.size(), counter.p, ctx->cmf.p, kBatchMaskWords, 0,
                              4, 1, grid, stream));
-        SC_CUDA(launch_reduce_many(d_descs.p, n, tiles, true, maxc, stream));
+        SC_CUDA(launch_reduce_many(d_descs.p, n, words, true, maxc, dirty_list.p, dirty_count.p, stream));
         SC_CUDA(cudaStreamSynchronize(stream));
         const double t1 = now_s();
         photons += step_photons;
@@ -275,6 +278,7 @@ int sc_server_create(sc_ctx* ctx, const sc_server_config* cfg, sc_server** out) 
     if ((e = s->d_jobs.alloc(s->cfg.max_slots)) != cudaSuccess) return fail(e);
     if ((e = s->d_descs.alloc(s->cfg.max_slots)) != cudaSuccess) return fail(e);
     if ((e = s->counter.alloc(1)) != cudaSuccess) return fail(e);
+    if ((e = s->dirty_count.alloc(1)) != cudaSuccess) return fail(e);
     s->arena.reset(cfg->hbm_budget_bytes);
     s->grid = (uint32_t)(ctx->sms * batch_occupancy(0, 4, 1, kBatchMaskWords));
     *out = s;
