@@ -63,6 +63,26 @@ WORKLOADS = {
 METRIC_POINT = "photons/s @<=0.5% film err (forward + volumetric single scatter)"
 METRIC_BEAM = "photons/s (forward + photon-beam estimator, volumetric single scatter)"
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of each workload's
+# roofline region, per launch (per step for the tracer and batch), from one
+# ncu capture of the default workload on a B200 (the profile summaries give the
+# commands); reported only when the workload runs at its default size.
+NCU_TRAFFIC = {
+    "prism": (2092544, "photon_kernel"),
+    "rainbow": (4839725056, "order_count + order_scan + order_scatter + photon_kernel"),
+    "beam": (3842560, "beam_kernel"),
+    "tracer": (10152085504, "all tracer wave kernels of one accumulate(64)"),
+    "batch": (4566429952, "batch_kernel + reduce_scan + reduce_list"),
+    "atomics": (24887296, "synthetic_splat_kernel"),
+}
+
+
+def ncu_traffic(workload, default_size=True):
+    if not default_size or workload not in NCU_TRAFFIC:
+        return None, None
+    b, what = NCU_TRAFFIC[workload]
+    return b, "ncu dram__bytes_read.sum + dram__bytes_write.sum of %s, one capture" % what
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -382,6 +402,11 @@ def run_gpu(args, rank, world, local_rank):
         alg_note = "8 B per film channel per in-frame haze sample: %d samples per launch" % splats
         flops = photons * 20 + segments * 14 * npl + segments * 4 * 60 + scatters * 45
     lit_bytes = dirty_tiles * 64 * CH * 8
+    # the library traces photons in film-bin order when a spectral film is larger than L2
+    film_bytes = ((W + 7) // 8) * ((H + 7) // 8) * 64 * CH * 8
+    ordered = (EST != 2 and B > 0 and N >= (1 << 16) and os.environ.get("SPECTRAL_CUDA_ORDER", "1") != "0"
+               and film_bytes > torch.cuda.get_device_properties(dev).L2_cache_size)
+    traffic, traffic_src = ncu_traffic(args.workload, not args.photons)
     workload_txt = {"prism": "SF11 prism apex 60 side 1, beam 0.02 @45deg, 2^20 photons, 640x360x64 bins",
                     "rainbow": "water sphere r=1, beam 2.2, 2^26 photons, 1920x1080x64 bins",
                     "beam": "photon-beam estimator, DSOTM prism scene, 2^18 photons, 800x800 XYZ film"}
@@ -398,10 +423,13 @@ def run_gpu(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": 3 * W * H * 4,
                 "path": "sc_photon_film_set_scene + dispatch + read_accum (host f32 XYZ) + clear"},
-        "gpu_launches": args.steps * 2,
-        "kernels": {"trace_ms": statistics.mean(trace_ms), "reduce_ms": statistics.mean(reduce_ms)},
+        # per step: the trace (3 wavelength-sort kernels first when ordered) and the drain
+        "gpu_launches": args.steps * (2 + (3 if ordered else 0)),
+        "kernels": {"trace_ms": statistics.mean(trace_ms), "reduce_ms": statistics.mean(reduce_ms),
+                    "wavelength_ordered": ordered},
         "roofline": {"bound": "hbm", "achieved": alg_bytes / trace_s / 1e9, "peak": hbm, "unit": "GB/s",
-                     "frac": alg_bytes / trace_s / 1e9 / hbm, "traffic": None, "kernel": kname,
+                     "frac": alg_bytes / trace_s / 1e9 / hbm, "traffic": traffic, "traffic_source": traffic_src,
+                     "kernel": kname + (" (after its wavelength sort)" if ordered else ""),
                      "peak_source": "%s hbm_gbs" % peak_note, "algorithmic": alg_note},
         "roofline_fp32": {"kernel": kname, "counted_flops": flops, "achieved_tflops": flops / trace_s / 1e12,
                           "peak_tflops": fp32_peak, "frac": flops / trace_s / 1e12 / fp32_peak,
@@ -573,7 +601,8 @@ def run_gpu_tracer(args, rank, world, local_rank):
         "gpu_launches": args.steps * waves * (2 + 2 * min(kw["max_depth"], 2) + (1 if kw["max_depth"] > 2 else 0)),
         "kernels": {"accumulate_ms": statistics.mean(step_ms)},
         "roofline": {"bound": "hbm", "achieved": qbytes / step_s / 1e9, "peak": hbm, "unit": "GB/s",
-                     "frac": qbytes / step_s / 1e9 / hbm, "traffic": None, "kernel": "tr_intersect + tr_shade",
+                     "frac": qbytes / step_s / 1e9 / hbm, "traffic": ncu_traffic("tracer")[0],
+                     "traffic_source": ncu_traffic("tracer")[1], "kernel": "tracer wave kernels (one accumulate)",
                      "peak_source": "%s hbm_gbs" % peak_note,
                      "algorithmic": "wavefront queue bytes: 176 B per path segment, %d segments per step" % segments},
         "roofline_fp32": {"kernel": "tr_intersect + tr_shade", "counted_flops": flops,
@@ -661,7 +690,8 @@ def run_gpu_atomics(args, rank, world, local_rank):
                 "path": "sc_atomic_film_splat + sc_atomic_film_read_raw (host u32 film)"},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": atomics * 4 / step_s / 1e9, "peak": hbm, "unit": "GB/s",
-                     "frac": atomics * 4 / step_s / 1e9 / hbm, "traffic": None, "kernel": "synthetic_splat_kernel",
+                     "frac": atomics * 4 / step_s / 1e9 / hbm, "traffic": ncu_traffic("atomics")[0],
+                     "traffic_source": ncu_traffic("atomics")[1], "kernel": "synthetic_splat_kernel",
                      "peak_source": "measured hbm_gbs" if peaks.get("hbm_gbs") else "fallback",
                      "algorithmic": "4 B payload per atomic (the film stays in L2: this is the L2 atomic rate)"},
         "clocks": clk.summary(),
@@ -938,7 +968,9 @@ def run_gpu_batch(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "kernel": "batch_kernel + reduce_scan + reduce_list (one pass)",
                      "achieved": (stats["in_frame_samples"] * 8 + 2 * stats["dirty_tile_bytes"] +
                                   b.xyz_floats * 4) / step_s / 1e9,
-                     "peak": hbm, "unit": "GB/s", "traffic": None, "peak_source": "%s hbm_gbs" % peak_note,
+                     "peak": hbm, "unit": "GB/s", "traffic": ncu_traffic("batch", not args.scenes)[0],
+                     "traffic_source": ncu_traffic("batch", not args.scenes)[1],
+                     "peak_source": "%s hbm_gbs" % peak_note,
                      "algorithmic": "8 B per in-frame haze sample + read and zero of every lit film tile + "
                                     "the f32 XYZ images"},
         "clocks": cl,

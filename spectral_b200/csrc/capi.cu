@@ -81,6 +81,8 @@ static int default_shape(sc_ctx* ctx, bool spectral, int aggregate, size_t smem,
     if (const char* agg = std::getenv("SPECTRAL_CUDA_AGGREGATE")) s.aggregate = std::atoi(agg) ? 1 : 0;
     if (const char* mb = std::getenv("SPECTRAL_CUDA_MINB")) s.minb = std::atoi(mb) >= 5 ? 5 : 4;
     if (const char* sp = std::getenv("SPECTRAL_CUDA_SPLIT")) s.split = std::atoi(sp) ? 1 : 0;
+    if (const char* od = std::getenv("SPECTRAL_CUDA_ORDER")) s.order = std::min(std::max(std::atoi(od), 0), 2);
+    s.pool = ctx->pool;
     const int per_sm = estimator == 2u ? beam_occupancy_blocks(s, spectral, smem)
                                        : photon_occupancy_blocks(s, spectral, smem);
     s.grid = (uint32_t)(ctx->sms * per_sm);
@@ -211,6 +213,18 @@ int sc_ctx_create(int device, const float* tables, sc_ctx** out) {
         delete c;
         return SC_E_CUDA;
     }
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof props);
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&c->pool, &props) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+        cudaGetLastError();
+        c->pool = nullptr;  // no pool: photon launches run in launch order
+    }
     *out = c;
     return SC_OK;
     SC_GUARD_END
@@ -223,6 +237,10 @@ int sc_ctx_destroy(sc_ctx* ctx) {
         DeviceGuard g(ctx->device);
         ctx->cmf.reset();
         ctx->binw_cache.clear();
+        if (ctx->pool) {
+            cudaDeviceSynchronize();  // frees still queued on streams return their blocks first
+            cudaMemPoolDestroy(ctx->pool);
+        }
     }
     delete ctx;
     return SC_OK;

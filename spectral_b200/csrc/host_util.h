@@ -87,6 +87,9 @@ struct sc_ctx {
     int cc_major = 0, cc_minor = 0;
     float tables[5 * 71];
     sc::DevBuf<float> cmf;  // 3 x 71 on the device
+    // stream-ordered scratch (the wavelength-ordered photon dispatch); memory
+    // freed to it stays reserved for the next launch until the context goes
+    cudaMemPool_t pool = nullptr;
     std::mutex mu;
     // bin-averaged CMF weights of spectral films reduced through the
     // device-pointer API, per (bins, band); freed with the context

@@ -26,13 +26,23 @@ struct PhotonParams {
     uint32_t n_prims, n_planes, n_mats;
     const float* cmf;                 // device 3x71 (xbar, ybar, zbar)
     sc_debug_photon* debug;           // debug launches only
+    const uint32_t* order;            // nullable: photon i of the launch is photon_base + order[i]
 };
 
 // Photon launch: CTAs of 256 threads, `grid` CTAs (grid-stride), warp
-// aggregation on/off, register bound (minimum CTAs per SM: 4 or 5), and the
+// aggregation on/off, register bound (minimum CTAs per SM: 4 or 5), the
 // warp-split transport (segments buffered per warp, haze samples processed as
-// one converged list) on/off.
-struct LaunchShape { uint32_t block, grid; int aggregate; int minb; int split = 1; };
+// one converged list) on/off, and the wavelength-ordered dispatch (0 never,
+// 1 for spectral films larger than L2, 2 for every spectral film; its scratch
+// comes from `pool`, and without a pool it is off).
+struct LaunchShape {
+    uint32_t block, grid;
+    int aggregate;
+    int minb;
+    int split = 1;
+    int order = 1;
+    cudaMemPool_t pool = nullptr;
+};
 
 // Dirty-tile masks up to this many 32-bit words (16 KB, 524288 tiles) are
 // accumulated in shared memory by each photon CTA.

@@ -120,6 +120,7 @@ extern "C" int sc_trace_xyz_noalloc(const float* tables_5x71, const sc_trace_des
 
     LaunchShape shape;
     shape.block = 256; shape.aggregate = 0; shape.minb = 4;
+    shape.order = 0;  // the ordered dispatch takes stream-ordered scratch memory
     const size_t smem = scene_smem_bytes(d->n_prims, d->n_planes, d->n_mats) +
                         (words <= kMaxSmemMaskWords ? words * sizeof(uint32_t) : 0);
     shape.grid = (uint32_t)(sp.sms * photon_occupancy_blocks(shape, o.bins != 0, smem));

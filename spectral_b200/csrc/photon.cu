@@ -41,13 +41,16 @@ __global__ void __launch_bounds__(256, MINB) photon_kernel(const PhotonParams p,
         WarpSplitSmem* ws = reinterpret_cast<WarpSplitSmem*>(smem + split_offset(p, mask_words));
         const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
         const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-        for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < p.photon_count; base += warps * 32u)
-            trace_warp_split<SPEC, AGG>(p, S, cmf, p.photon_base + base + lane, base + lane < p.photon_count, smask,
-                                        ws[warp]);
+        for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < p.photon_count; base += warps * 32u) {
+            const uint32_t i = base + lane;
+            const bool valid = i < p.photon_count;
+            const uint32_t k = p.order && valid ? p.order[i] : i;
+            trace_warp_split<SPEC, AGG>(p, S, cmf, p.photon_base + k, valid, smask, ws[warp]);
+        }
     } else {
         const uint32_t stride = gridDim.x * blockDim.x;
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += stride)
-            trace_photon<SPEC, AGG, false>(p, S, cmf, p.photon_base + i, smask);
+            trace_photon<SPEC, AGG, false>(p, S, cmf, p.photon_base + (p.order ? p.order[i] : i), smask);
     }
     if (smask) {  // publish this CTA's dirty tiles
         __syncthreads();
@@ -125,6 +128,113 @@ __global__ void rng_draws_kernel(uint32_t key, uint32_t seed, uint32_t n, uint32
     for (uint32_t i = 0; i < n; ++i) out[i] = r.u32();
 }
 
+// ---------------------------------------------------------------------------
+// Wavelength-ordered dispatch.  Film cells are pixel-major (the bins of a pixel
+// are adjacent), so photons of random wavelengths traced together touch every
+// 32-byte sector of every pixel they reach, and a spectral film larger than L2
+// misses on most of its atomics.  Tracing the photons of a launch in order of
+// their film bin keeps the photons in flight within a few bins: about one
+// sector per pixel is live at a time.  The photons and their paths are the
+// same and the film is a sum of exact integers, so the image is bit-identical.
+// Counting sort of the launch's photons by key (kOrderKeys groups of
+// consecutive bins): per-CTA key histograms of contiguous photon chunks
+// (key-major), one exclusive scan, then a scatter that stages 2048 photons at a
+// time in shared memory so that each key's run is written contiguously.
+constexpr uint32_t kOrderKeys = 16;
+constexpr uint32_t kOrderTile = 2048;  // photons per scatter step: 8 per thread
+
+// Sort key of photon `idx`: the group of its film bin (its third draw, as in
+// the transport).
+__device__ __forceinline__ uint32_t photon_key(const PhotonParams& p, uint32_t idx) {
+    Rng r = Rng::make(idx, p.seed);
+    r.state += 2u;  // the two aperture draws
+    const float lambda = p.lambda_min + p.lambda_range * r.f32();
+    const float fb = (lambda - p.bin_min) * p.bin_inv_width;
+    const int bi = (int)fb;
+    const uint32_t bin = fb < 0.0f ? 0u : (bi >= (int)p.bins ? p.bins - 1u : (uint32_t)bi);
+    return p.bins <= kOrderKeys ? bin : bin * kOrderKeys / p.bins;
+}
+
+__global__ void __launch_bounds__(256) order_count_kernel(const PhotonParams p, uint32_t per_cta,
+                                                          uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[kOrderKeys];
+    const uint32_t K = min(p.bins, kOrderKeys);
+    if (threadIdx.x < K) h[threadIdx.x] = 0u;
+    __syncthreads();
+    const uint32_t i0 = blockIdx.x * per_cta, i1 = min(i0 + per_cta, p.photon_count);
+    for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) atomicAdd(&h[photon_key(p, p.photon_base + i)], 1u);
+    __syncthreads();
+    if (threadIdx.x < K) hist[threadIdx.x * gridDim.x + blockIdx.x] = h[threadIdx.x];
+}
+
+// In-place exclusive scan of n counts by one CTA of 1024 threads.
+__global__ void __launch_bounds__(1024) order_scan_kernel(uint32_t* __restrict__ a, uint32_t n) {
+    __shared__ uint32_t part[1024];
+    const uint32_t t = threadIdx.x, per = (n + 1023u) / 1024u;
+    const uint32_t lo = min(t * per, n), hi = min(lo + per, n);
+    uint32_t sum = 0;
+    for (uint32_t i = lo; i < hi; ++i) sum += a[i];
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024u; off <<= 1) {
+        const uint32_t v = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = t ? part[t - 1] : 0u;
+    for (uint32_t i = lo; i < hi; ++i) {
+        const uint32_t c = a[i];
+        a[i] = run;
+        run += c;
+    }
+}
+
+// Blocks of 256 threads.
+__global__ void __launch_bounds__(256) order_scatter_kernel(const PhotonParams p, uint32_t per_cta,
+                                                            const uint32_t* __restrict__ offsets,
+                                                            uint32_t* __restrict__ order) {
+    __shared__ uint32_t cur[kOrderKeys], cnt[kOrderKeys], toff[kOrderKeys];
+    __shared__ uint32_t stage[kOrderTile];
+    __shared__ uint8_t skey[kOrderTile];
+    const uint32_t tid = threadIdx.x, K = min(p.bins, kOrderKeys);
+    if (tid < K) cur[tid] = offsets[tid * gridDim.x + blockIdx.x];
+    const uint32_t i0 = blockIdx.x * per_cta, i1 = min(i0 + per_cta, p.photon_count);
+    for (uint32_t t0 = i0; t0 < i1; t0 += kOrderTile) {
+        if (tid < K) cnt[tid] = 0u;
+        __syncthreads();
+        uint32_t key[8], rank[8];
+#pragma unroll
+        for (uint32_t j = 0; j < 8u; ++j) {
+            const uint32_t i = t0 + j * 256u + tid;
+            key[j] = i < i1 ? photon_key(p, p.photon_base + i) : 0xFFu;
+            rank[j] = key[j] != 0xFFu ? atomicAdd(&cnt[key[j]], 1u) : 0u;  // rank within the tile's key run
+        }
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t sum = 0;
+            for (uint32_t k = 0; k < K; ++k) { toff[k] = sum; sum += cnt[k]; }
+        }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t j = 0; j < 8u; ++j) {
+            if (key[j] != 0xFFu) {
+                const uint32_t pos = toff[key[j]] + rank[j];
+                stage[pos] = t0 + j * 256u + tid;
+                skey[pos] = (uint8_t)key[j];
+            }
+        }
+        __syncthreads();
+        const uint32_t n = min(kOrderTile, i1 - t0);
+        for (uint32_t q = tid; q < n; q += 256u) {
+            const uint32_t k = skey[q];
+            order[cur[k] + (q - toff[k])] = stage[q];
+        }
+        __syncthreads();
+        if (tid < K) cur[tid] += cnt[tid];
+    }
+}
+
 __global__ void glass_n_kernel(uint32_t glass, const float* __restrict__ lambda_nm, uint32_t n,
                                float* __restrict__ out) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -195,8 +305,65 @@ uint32_t photon_mask_words(const PhotonParams& p) {
     return words <= kMaxSmemMaskWords ? words : 0u;
 }
 
+// L2 bytes of the current device, read once per device.
+static size_t l2_bytes() {
+    static std::mutex mu;
+    static std::map<int, size_t> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(dev);
+    if (it != cache.end()) return it->second;
+    int b = 0;
+    cudaDeviceGetAttribute(&b, cudaDevAttrL2CacheSize, dev);
+    cache.emplace(dev, (size_t)(b > 0 ? b : 0));
+    return (size_t)(b > 0 ? b : 0);
+}
+
+// Whether a launch takes the wavelength-ordered dispatch: point / isotropic
+// estimators on a spectral film larger than L2 (order 1) or on any spectral
+// film (order 2), at least 2^16 photons to amortise the sort, and a memory
+// pool for its scratch.
+static bool ordered_dispatch(const PhotonParams& p, const LaunchShape& shape) {
+    if (shape.order == 0 || !shape.pool || p.bins == 0u || p.channels != p.bins || p.order ||
+        p.photon_count < (1u << 16))
+        return false;
+    if (shape.order >= 2) return true;
+    const size_t film = (size_t)p.tiles_x * ((p.height + 7u) / 8u) * kTilePixels * p.channels * 8u;
+    return film > l2_bytes();
+}
+
+static cudaError_t launch_photons_in(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s);
+
 cudaError_t launch_photons(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s) {
     if (p.photon_count == 0) return cudaSuccess;
+    if (!ordered_dispatch(p, shape)) return launch_photons_in(p, shape, s);
+    const uint32_t grid = 148u * 4u;  // sort CTAs, each a contiguous chunk of the launch's photons
+    const uint32_t per_cta = (p.photon_count + grid - 1u) / grid;
+    const uint32_t keys = p.bins < kOrderKeys ? p.bins : kOrderKeys;
+    const size_t words = (size_t)p.photon_count + (size_t)keys * grid;
+    uint32_t* buf = nullptr;
+    if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&buf), words * sizeof(uint32_t), shape.pool, s) !=
+        cudaSuccess) {
+        cudaGetLastError();  // no room for the sort: trace in launch order (same image)
+        return launch_photons_in(p, shape, s);
+    }
+    uint32_t* order = buf;
+    uint32_t* hist = buf + p.photon_count;
+    order_count_kernel<<<grid, 256, 0, s>>>(p, per_cta, hist);
+    order_scan_kernel<<<1, 1024, 0, s>>>(hist, keys * grid);
+    order_scatter_kernel<<<grid, 256, 0, s>>>(p, per_cta, hist, order);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        PhotonParams q = p;
+        q.order = order;
+        e = launch_photons_in(q, shape, s);
+    }
+    const cudaError_t f = cudaFreeAsync(buf, s);
+    return e != cudaSuccess ? e : f;
+}
+
+static cudaError_t launch_photons_in(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s) {
     const uint32_t mw = photon_mask_words(p);
     const size_t smem = shape.split ? split_offset(p, mw) + 8 * sizeof(WarpSplitSmem)
                                     : scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats) + mw * sizeof(uint32_t);

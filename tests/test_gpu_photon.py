@@ -183,6 +183,25 @@ def test_launch_variants_give_identical_films(ctx, aggregate, split, minb, bins,
     assert (f.read_raw() == g.read_raw()).all() and f.read_raw().sum() > 0
 
 
+@pytest.mark.parametrize("bins,w,h,n", [(24, 96, 80, 100_000), (64, 1280, 720, 1 << 18)])
+def test_wavelength_ordered_dispatch_gives_identical_film(ctx, monkeypatch, bins, w, h, n):
+    """Tracing a launch's photons in order of their film bin (the dispatch taken
+    for spectral films larger than L2; forced with 2, off with 0) only reorders
+    exact integer additions: the film bits are those of launch order."""
+    from spectral_b200.scenes import rainbow_workload
+    scene, beam, cam = rainbow_workload(w, h)
+    raws = []
+    for mode in ("0", "2", "1"):  # launch order, always ordered, automatic
+        monkeypatch.setenv("SPECTRAL_CUDA_ORDER", mode)
+        f = sb.GpuPhotonFilm(ctx, scene, cam, beam, w, h, n, 5, 8.0, sb.VolWeights(0.02, 0.02, 0.0), bins=bins,
+                             lambda_min=380.0, lambda_max=780.0, max_bounces=6)
+        f.dispatch_photons(0, n, 5)
+        f.dispatch_photons(n, n + 70_001, 5)  # a second, ragged launch into the same film
+        raws.append(f.read_raw())
+        f.close()
+    assert raws[0].sum() > 0 and (raws[0] == raws[1]).all() and (raws[0] == raws[2]).all()
+
+
 @pytest.mark.parametrize("bins,band", [(64, (380.0, 730.0)), (32, (380.0, 780.0)), (7, (400.0, 700.0))])
 def test_spectral_film_parity(ctx, bins, band):
     w, h, n, seed = 72, 41, 60_000, 11
