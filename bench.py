@@ -743,6 +743,10 @@ def run_gpu_serve(args, rank, world, local_rank):
     with ClockSampler(uuid) as clk, torch.cuda.nvtx.range("timed"):  # nvtx range for ncu --nvtx-include
         served = run_stream(srv, stream, want_image=True)
     srv.close()
+    # capacity: the same requests all submitted at once, served until drained
+    srv = Server(ctx, budget_bytes=budget)
+    capacity = run_stream(srv, stream, time_scale=0.0, want_image=True)
+    srv.close()
     plain = run_plain_stream(ctx, stream)
     total_rate = served["photons_per_s"]
     if world > 1:  # every rank served its own stream: total photons over the longest replay
@@ -771,6 +775,10 @@ def run_gpu_serve(args, rank, world, local_rank):
                    "timing": "host clock over the whole stream replayed in real time (one step = the stream)"},
         "served": served, "plain_per_request": plain,
         "served_over_plain": served["photons_per_s"] / plain["photons_per_s"],
+        # the replay serves the offered load; the burst shows how far above it the server goes
+        "capacity": dict(capacity, what="the same requests submitted at once (arrival time 0), served to the "
+                                        "last image"),
+        "capacity_over_plain": capacity["photons_per_s"] / plain["photons_per_s"],
         "e2e": {"value": total_rate, "unit": "photons/s", "h2d_bytes_per_step": in_bytes,
                 "d2h_bytes_per_step": out_bytes,
                 "path": "sc_server_submit per request, sc_server_step, sc_server_poll with the XYZ image to host"},
@@ -879,20 +887,25 @@ def run_gpu_batch(args, rank, world, local_rank):
     torch.cuda.synchronize()
     plain_ms = timed(b.run_plain, max(2, args.steps // 2))
     # plain per-scene launches through the drop-in object API (what a caller of
-    # the reference's GpuPhotonFilm does per scene): create, trace, read back, free
-    t0 = time.perf_counter()
-    for j in jobs:
-        sc = sb.Scene(background=0.0)
-        planes = [(tuple(j.planes[k].normal), j.planes[k].d) for k in range(j.n_planes)]
-        sc.add_solid(planes, sb.Dielectric(j.mats[0].glass))
-        f = sb.GpuPhotonFilm(ctx, sc, sb.Camera(j.cam), sb.Beam.from_c(j.beam), j.width, j.height, j.n_photons,
-                             j.seed, j.max_dist, sb.VolWeights(j.weights.sigma_s, j.weights.sigma_t, j.weights.g),
-                             bins=j.opts.bins, lambda_min=j.opts.lambda_min, lambda_max=j.opts.lambda_max,
-                             max_bounces=j.opts.max_bounces)
-        f.trace_and_resolve(j.n_photons, j.seed)
-        f.accum()
-        f.close()
-    plain_api_s = time.perf_counter() - t0
+    # the reference's GpuPhotonFilm does per scene): create, trace, read back,
+    # free.  Host-bound by the film allocations (cudaMalloc / cudaFree of up to
+    # 268 MB per scene), whose cost varies from pass to pass: best of two passes.
+    plain_api_s = float("inf")
+    for _ in range(2):
+        t0 = time.perf_counter()
+        for j in jobs:
+            sc = sb.Scene(background=0.0)
+            planes = [(tuple(j.planes[k].normal), j.planes[k].d) for k in range(j.n_planes)]
+            sc.add_solid(planes, sb.Dielectric(j.mats[0].glass))
+            f = sb.GpuPhotonFilm(ctx, sc, sb.Camera(j.cam), sb.Beam.from_c(j.beam), j.width, j.height,
+                                 j.n_photons, j.seed, j.max_dist,
+                                 sb.VolWeights(j.weights.sigma_s, j.weights.sigma_t, j.weights.g),
+                                 bins=j.opts.bins, lambda_min=j.opts.lambda_min, lambda_max=j.opts.lambda_max,
+                                 max_bounces=j.opts.max_bounces)
+            f.trace_and_resolve(j.n_photons, j.seed)
+            f.accum()
+            f.close()
+        plain_api_s = min(plain_api_s, time.perf_counter() - t0)
     total_ms = sum(ms)
     job_photons = b.total_photons  # photons of all ranks' batches (each rank draws its own scenes)
     if dist:
@@ -956,7 +969,8 @@ def run_gpu_batch(args, rank, world, local_rank):
                   "what": "the same %d scenes as plain per-scene launches (trace + drain/reduce each), one GPU"
                           % len(jobs)},
         "plain_api": {"value": b.total_photons / plain_api_s, "unit": "photons/s", "s_per_step": plain_api_s,
-                      "what": "per scene: GpuPhotonFilm create + trace_and_resolve + accum (host XYZ) + destroy"},
+                      "what": "per scene: GpuPhotonFilm create + trace_and_resolve + accum (host XYZ) + destroy; "
+                              "best of two passes over the 256 scenes"},
         "batched_over_plain": value / job_photons * b.total_photons / plain_value,
         "batched_e2e_over_plain_api": e2e_value / job_photons * b.total_photons / (b.total_photons / plain_api_s),
         "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": b.job_table_bytes,
