@@ -385,15 +385,22 @@ int sc_server_create(sc_ctx* ctx, const sc_server_config* cfg, sc_server** out);
 int sc_server_destroy(sc_server* s);
 /* Queue a request; SC_E_NOMEM when it could never fit the budget. */
 int sc_server_submit(sc_server* s, const sc_request* r, uint64_t* id);
-/* Admit what fits, trace one frame of every admitted request (one launch),
- * retire finished requests.  Blocks until the step's work is done. */
+/* Admit what fits and queue one frame of every admitted request (one batched
+ * launch and one drain) on the server's stream; returns once at most one step
+ * (two while requests wait for admission) is queued ahead of it.  Requests
+ * whose last frame was queued become pollable once their image is in host
+ * memory.  With nothing left to trace, a step waits for the queued work.
+ * `active` counts admitted requests plus those whose images are still on their
+ * way (sc_server_stats too), so a loop "while queued or active: step" ends
+ * with every result pollable. */
 int sc_server_step(sc_server* s, uint32_t* active);
 /* Pop a finished request: its last frame's XYZ image (3*w*h floats) and the
- * steady-clock times [submit, admit, first frame done, done] in seconds.
- * SC_E_STATE when nothing is finished. */
+ * steady-clock times [submit, admit, first frame done, done] in seconds (the
+ * last two as seen by the host).  SC_E_STATE when nothing is finished. */
 int sc_server_poll(sc_server* s, uint64_t* id, float* xyz_out, size_t capacity, uint32_t* width,
                    uint32_t* height, double times[4]);
-/* Drop a queued or active request (between steps nothing of it is in flight). */
+/* Drop a queued or active request (frames of it already queued still run;
+ * its device memory is reused only behind them). */
 int sc_server_cancel(sc_server* s, uint64_t id);
 int sc_server_stats(sc_server* s, uint64_t* photons_traced, uint64_t* bytes_in_use, uint32_t* queued,
                     uint32_t* active, uint32_t* finished);

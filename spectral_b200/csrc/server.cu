@@ -10,6 +10,14 @@
 // * Step: the current frame of EVERY active request is traced by one persistent
 //   batch launch (batch.cu) and drained/sensor-reduced by one launch over all
 //   active films; newly arrived requests join at the next step.
+// * Pipelining: a step only queues its work on the server's stream (tables go
+//   up from pinned staging, two sets used in turn) and returns, so the host
+//   prepares step k + 1 while the device runs step k.  Everything a request
+//   owns on the device is touched only by work on that one stream, in order,
+//   so its arena range can be handed to the next request as soon as its last
+//   frame is queued.  The images of requests that finished in a step are
+//   copied behind the step into a pinned host ring (allocated once), and the
+//   request becomes pollable once that copy is done.
 // * State on the device per request: its film, dirty mask and image.  The RNG
 //   state of a request is its photon index: frame f traces photons
 //   [f*N, (f+1)*N) of the request's own stream, so a request's result does not
@@ -71,6 +79,45 @@ class Arena {
     uint64_t cap_ = 0, used_ = 0;
 };
 
+// Pinned host memory for finished images: one ring allocated at creation.
+// Images are taken in the order requests finish and given back in the order
+// they are polled, which is the same order, so the ring is a FIFO of ranges.
+class PinnedRing {
+  public:
+    cudaError_t init(size_t floats) {
+        cap_ = floats;
+        return cudaMallocHost(reinterpret_cast<void**>(&base_), cap_ * sizeof(float));
+    }
+    float* get(size_t n) {
+        if (!base_ || n > cap_) return nullptr;
+        if (live_.empty()) { live_.push_back({0, n}); return base_; }
+        const size_t t = live_.front().first, h = live_.back().first + live_.back().second;
+        size_t at;
+        if (h > t) {  // free: [h, cap) and [0, t)
+            if (cap_ - h >= n) at = h;
+            else if (t >= n) at = 0;
+            else return nullptr;
+        } else {      // wrapped: free [h, t)
+            if (t - h >= n) at = h;
+            else return nullptr;
+        }
+        live_.push_back({at, n});
+        return base_ + at;
+    }
+    void pop() { if (!live_.empty()) live_.pop_front(); }
+    void release() {
+        if (base_) cudaFreeHost(base_);
+        base_ = nullptr;
+        live_.clear();
+    }
+
+  private:
+    float* base_ = nullptr;
+    size_t cap_ = 0;
+    std::deque<std::pair<size_t, size_t>> live_;
+};
+constexpr size_t kRingFloats = size_t(64) << 20;  // 256 MB: twenty 1024x1024 images
+
 struct Request {
     uint64_t id = 0;
     sc_request r{};
@@ -79,17 +126,37 @@ struct Request {
     uint64_t off = 0, bytes = 0;
     uint32_t tiles_x = 0, tiles_y = 0, words = 0;
     size_t film_cells = 0;
-    std::vector<float> result;
+    const float* binw = nullptr;  // bin-averaged CMF of its (bins, band), shared through the context
+    float* image = nullptr;       // pinned copy of the last frame's XYZ image
+    bool image_own = false;       // its own pinned allocation (the ring was full), not a ring range
 };
 
+// Film, dirty mask and image of one request in the arena.
 uint64_t request_bytes(const sc_scene_job& j, uint32_t& tiles_x, uint32_t& tiles_y, uint32_t& words, size_t& cells) {
     tiles_x = (j.width + 7u) / 8u;
     tiles_y = (j.height + 7u) / 8u;
     words = flag_words(j.width, j.height);
     cells = (size_t)tiles_x * tiles_y * kTilePixels * j.opts.bins;
     auto up = [](uint64_t b) { return (b + 255u) & ~uint64_t(255); };
-    return up(cells * 8) + up(words * 4ull) + up(3ull * j.width * j.height * 4) + up(3ull * j.opts.bins * 4);
+    return up(cells * 8) + up(words * 4ull) + up(3ull * j.width * j.height * 4);
 }
+
+// One set of pinned upload tables; `used` is recorded after the copies that
+// read it, so the host rewrites the set only after they ran.
+struct HostStage {
+    BatchJobDev* jobs = nullptr;
+    FilmDesc* descs = nullptr;
+    WorkItem* items = nullptr;
+    size_t items_cap = 0;
+    cudaEvent_t used = nullptr;
+};
+
+// A queued step: its completion event, the requests whose first frame it
+// traces and those whose last frame it traces (their image copies follow it).
+struct StepRecord {
+    cudaEvent_t done = nullptr;
+    std::vector<Request*> first, last;
+};
 
 }  // namespace
 
@@ -107,11 +174,14 @@ struct sc_server {
     DevBuf<uint32_t> counter, dirty_count;
     std::deque<Request*> queue;
     std::vector<Request*> active;
+    std::deque<StepRecord> inflight;  // queued steps, oldest first
     std::deque<Request*> finished;
     uint64_t next_id = 1, photons = 0;
     uint32_t grid = 0;
-    std::vector<BatchJobDev> h_jobs;
-    std::vector<FilmDesc> h_descs;
+    HostStage stage[2];
+    uint32_t stage_k = 0;
+    PinnedRing ring;
+    std::vector<cudaEvent_t> spare_events;
     std::vector<WorkItem> h_items;
 
     unsigned long long* film_ptr(const Request* q) { return reinterpret_cast<unsigned long long*>(mem.p + q->off); }
@@ -122,10 +192,68 @@ struct sc_server {
         return reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(flags_ptr(q)) +
                                         ((q->words * 4ull + 255u) & ~uint64_t(255)));
     }
-    float* binw_ptr(const Request* q) {
-        const sc_scene_job& j = q->r.job;
-        return reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(xyz_ptr(q)) +
-                                        ((3ull * j.width * j.height * 4 + 255u) & ~uint64_t(255)));
+    // Bin-averaged CMF of a (bins, band) on the device, kept by the context.
+    int binw_for(const sc_film_options& o, const float** out) {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        const auto key = std::make_tuple(o.bins, o.lambda_min, o.lambda_max);
+        auto it = ctx->binw_cache.find(key);
+        if (it == ctx->binw_cache.end()) {
+            std::vector<float> w(3 * o.bins);
+            bin_weights(ctx->tables, o.bins, o.lambda_min, o.lambda_max, w.data());
+            std::unique_ptr<DevBuf<float>> buf(new DevBuf<float>());
+            SC_CUDA(buf->alloc(w.size()));
+            SC_CUDA(cudaMemcpy(buf->p, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
+            it = ctx->binw_cache.emplace(key, std::move(buf)).first;
+        }
+        *out = it->second->p;
+        return SC_OK;
+    }
+
+    cudaError_t event(cudaEvent_t* e) {
+        if (!spare_events.empty()) {
+            *e = spare_events.back();
+            spare_events.pop_back();
+            return cudaSuccess;
+        }
+        return cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+    }
+
+    // Retire queued steps that are done (all of them, in order, when `wait`):
+    // first-frame and done times; finished requests become pollable.
+    int collect(bool wait) {
+        while (!inflight.empty()) {
+            StepRecord& r = inflight.front();
+            if (wait) {
+                SC_CUDA(cudaEventSynchronize(r.done));
+            } else {
+                const cudaError_t e = cudaEventQuery(r.done);
+                if (e == cudaErrorNotReady) break;
+                SC_CUDA(e);
+            }
+            const double t = now_s();
+            for (Request* q : r.first) q->t_first = t;
+            for (Request* q : r.last) {
+                q->t_done = t;
+                finished.push_back(q);
+            }
+            spare_events.push_back(r.done);
+            inflight.pop_front();
+        }
+        return SC_OK;
+    }
+
+    // Requests whose images are still being produced or copied.
+    uint32_t retiring() const {
+        size_t n = 0;
+        for (const StepRecord& r : inflight) n += r.last.size();
+        return (uint32_t)n;
+    }
+
+    void free_image(Request* q) {
+        if (!q->image) return;
+        if (q->image_own) cudaFreeHost(q->image);
+        else ring.pop();
+        q->image = nullptr;
     }
 
     sc_camera frame_camera(const Request* q) const {
@@ -148,34 +276,83 @@ struct sc_server {
             if (!arena.alloc(q->bytes, off)) { ++it; continue; }
             q->off = off;
             q->t_admit = t;
+            int rc = binw_for(q->r.job.opts, &q->binw);
+            if (rc != SC_OK) { arena.release(off, q->bytes); return rc; }
+            // behind every earlier use of this range on the same stream
             SC_CUDA(cudaMemsetAsync(film_ptr(q), 0, q->film_cells * 8, stream));
             SC_CUDA(cudaMemsetAsync(flags_ptr(q), 0, q->words * 4ull, stream));
-            std::vector<float> w(3 * q->r.job.opts.bins);
-            bin_weights(ctx->tables, q->r.job.opts.bins, q->r.job.opts.lambda_min, q->r.job.opts.lambda_max, w.data());
-            SC_CUDA(cudaMemcpyAsync(binw_ptr(q), w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
-            SC_CUDA(cudaStreamSynchronize(stream));  // the host vector goes out of scope
             active.push_back(q);
             it = queue.erase(it);
         }
         return SC_OK;
     }
 
+    // The pinned table set for this step, with room for `items` work items.
+    int stage_for(uint32_t items, HostStage** out) {
+        HostStage& h = stage[stage_k];
+        stage_k ^= 1u;
+        if (!h.used) SC_CUDA(cudaEventCreateWithFlags(&h.used, cudaEventDisableTiming));
+        else SC_CUDA(cudaEventSynchronize(h.used));  // its previous copies ran
+        if (!h.jobs) {
+            SC_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h.jobs), cfg.max_slots * sizeof(BatchJobDev)));
+            SC_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h.descs), cfg.max_slots * sizeof(FilmDesc)));
+        }
+        if (h.items_cap < items) {
+            if (h.items) cudaFreeHost(h.items);
+            h.items = nullptr;
+            h.items_cap = 0;
+            SC_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h.items), (size_t)items * 2 * sizeof(WorkItem)));
+            h.items_cap = (size_t)items * 2;
+        }
+        *out = &h;
+        return SC_OK;
+    }
+
+    void release_all() {
+        for (HostStage& h : stage) {
+            if (h.jobs) cudaFreeHost(h.jobs);
+            if (h.descs) cudaFreeHost(h.descs);
+            if (h.items) cudaFreeHost(h.items);
+            if (h.used) cudaEventDestroy(h.used);
+            h = HostStage{};
+        }
+        for (StepRecord& r : inflight) spare_events.push_back(r.done);
+        inflight.clear();
+        for (cudaEvent_t e : spare_events) cudaEventDestroy(e);
+        spare_events.clear();
+        ring.release();
+    }
+
     int step(uint32_t* n_active) {
         const double t0 = now_s();
-        int rc = admit(t0);
+        int rc = collect(false);
+        if (rc == SC_OK) rc = admit(t0);
         if (rc != SC_OK) return rc;
-        if (active.empty()) { if (n_active) *n_active = 0; return SC_OK; }
+        if (active.empty()) {
+            // nothing to trace: finish what is still queued (a drain loop ends here)
+            rc = collect(true);
+            if (n_active) *n_active = 0;
+            return rc;
+        }
         const uint32_t n = (uint32_t)active.size();
-        h_jobs.resize(n);
-        h_descs.resize(n);
-        h_items.clear();
-        uint32_t tiles = 0, words = 0, maxc = 0;
-        uint64_t step_photons = 0;
         std::vector<uint32_t> order(n);
         for (uint32_t i = 0; i < n; ++i) order[i] = i;
         std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
             return active[a]->r.job.n_photons > active[b]->r.job.n_photons;
         });
+        const uint32_t chunk = cfg.chunk_photons;
+        h_items.clear();
+        for (uint32_t i : order) {
+            const Request* q = active[i];
+            const uint32_t N = q->r.job.n_photons, base = q->frame * N;
+            for (uint32_t b = 0; b < N; b += chunk) h_items.push_back(WorkItem{i, base + b, std::min(chunk, N - b)});
+        }
+        HostStage* h = nullptr;
+        rc = stage_for((uint32_t)h_items.size(), &h);
+        if (rc != SC_OK) return rc;
+        std::memcpy(h->items, h_items.data(), h_items.size() * sizeof(WorkItem));
+        uint32_t tiles = 0, words = 0, maxc = 0;
+        uint64_t step_photons = 0;
         for (uint32_t i = 0; i < n; ++i) {
             Request* q = active[i];
             const sc_scene_job& J = q->r.job;
@@ -195,7 +372,7 @@ struct sc_server {
             p.film = film_ptr(q); p.flags = flags_ptr(q);
             p.n_prims = J.n_prims; p.n_planes = J.n_planes; p.n_mats = J.n_mats;
             p.cmf = ctx->cmf.p;
-            BatchJobDev& d = h_jobs[i];
+            BatchJobDev& d = h->jobs[i];
             std::memset(&d, 0, sizeof d);
             d.slot_image.p = p;
             std::memcpy(d.slot_image.prims, J.prims, sizeof d.slot_image.prims);
@@ -203,8 +380,8 @@ struct sc_server {
             std::memcpy(d.slot_image.mats, J.mats, sizeof d.slot_image.mats);
             d.flags = p.flags;
             d.mask_words = q->words;
-            FilmDesc& fd = h_descs[i];
-            fd.film = p.film; fd.flags = p.flags; fd.xyz = xyz_ptr(q); fd.binw = binw_ptr(q);
+            FilmDesc& fd = h->descs[i];
+            fd.film = p.film; fd.flags = p.flags; fd.xyz = xyz_ptr(q); fd.binw = q->binw;
             fd.width = J.width; fd.height = J.height; fd.tiles_x = q->tiles_x; fd.tiles_y = q->tiles_y;
             fd.channels = J.opts.bins; fd.word_begin = words;
             fd.inv_scale = std::ldexp(1.0, -(int)(J.opts.scale_log2 ? J.opts.scale_log2 : 32u));
@@ -213,40 +390,55 @@ struct sc_server {
             maxc = std::max(maxc, J.opts.bins);
             step_photons += J.n_photons;
         }
-        const uint32_t chunk = cfg.chunk_photons;
-        for (uint32_t i : order) {
-            const Request* q = active[i];
-            const uint32_t N = q->r.job.n_photons, base = q->frame * N;
-            for (uint32_t b = 0; b < N; b += chunk) h_items.push_back(WorkItem{i, base + b, std::min(chunk, N - b)});
+        if (d_items.n < h_items.size() || dirty_list.n < tiles) {
+            SC_CUDA(cudaStreamSynchronize(stream));  // queued steps still read the old tables (growth only)
+            if (d_items.n < h_items.size()) SC_CUDA(d_items.alloc(h_items.size() * 2));
+            if (dirty_list.n < tiles) SC_CUDA(dirty_list.alloc(tiles * 2ull));
         }
-        if (d_items.n < h_items.size()) SC_CUDA(d_items.alloc(h_items.size() * 2));
-        if (dirty_list.n < tiles) SC_CUDA(dirty_list.alloc(tiles * 2ull));
-        SC_CUDA(cudaMemcpyAsync(d_jobs.p, h_jobs.data(), n * sizeof(BatchJobDev), cudaMemcpyHostToDevice, stream));
-        SC_CUDA(cudaMemcpyAsync(d_descs.p, h_descs.data(), n * sizeof(FilmDesc), cudaMemcpyHostToDevice, stream));
-        SC_CUDA(cudaMemcpyAsync(d_items.p, h_items.data(), h_items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
+        SC_CUDA(cudaMemcpyAsync(d_jobs.p, h->jobs, n * sizeof(BatchJobDev), cudaMemcpyHostToDevice, stream));
+        SC_CUDA(cudaMemcpyAsync(d_descs.p, h->descs, n * sizeof(FilmDesc), cudaMemcpyHostToDevice, stream));
+        SC_CUDA(cudaMemcpyAsync(d_items.p, h->items, h_items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
                                 stream));
+        SC_CUDA(cudaEventRecord(h->used, stream));
         SC_CUDA(launch_batch(d_jobs.p, d_items.p, (uint32_t)h_items.size(), counter.p, ctx->cmf.p, kBatchMaskWords, 0,
                              4, 1, grid, stream));
         SC_CUDA(launch_reduce_many(d_descs.p, n, words, true, maxc, dirty_list.p, dirty_count.p, stream));
-        SC_CUDA(cudaStreamSynchronize(stream));
-        const double t1 = now_s();
         photons += step_photons;
+        StepRecord rec;
         std::vector<Request*> still;
         for (Request* q : active) {
-            if (q->frame == 0) q->t_first = t1;
+            if (q->frame == 0) rec.first.push_back(q);
             ++q->frame;
             if (q->frame >= q->r.frames) {
                 const size_t nf = 3ull * q->r.job.width * q->r.job.height;
-                q->result.resize(nf);
-                SC_CUDA(cudaMemcpy(q->result.data(), xyz_ptr(q), nf * sizeof(float), cudaMemcpyDeviceToHost));
-                q->t_done = now_s();
-                arena.release(q->off, q->bytes);
-                finished.push_back(q);
+                q->image = ring.get(nf);
+                if (!q->image) {  // ring full (results not polled): a pinned buffer of its own
+                    SC_CUDA(cudaMallocHost(reinterpret_cast<void**>(&q->image), nf * sizeof(float)));
+                    q->image_own = true;
+                }
+                SC_CUDA(cudaMemcpyAsync(q->image, xyz_ptr(q), nf * sizeof(float), cudaMemcpyDeviceToHost, stream));
+                arena.release(q->off, q->bytes);  // later users of the range queue behind this copy
+                rec.last.push_back(q);
             } else {
                 still.push_back(q);
             }
         }
         active.swap(still);
+        SC_CUDA(event(&rec.done));
+        SC_CUDA(cudaEventRecord(rec.done, stream));
+        inflight.push_back(std::move(rec));
+        // Queue depth: with requests waiting for admission, up to two steps
+        // queued (the device never idles between steps); otherwise one, so a
+        // new arrival waits behind at most the step being traced.
+        const size_t depth = queue.empty() ? 1u : 2u;
+        if (inflight.size() > depth) {
+            rc = collect(false);
+            while (rc == SC_OK && inflight.size() > depth) {
+                SC_CUDA(cudaEventSynchronize(inflight.front().done));
+                rc = collect(false);
+            }
+            if (rc != SC_OK) return rc;
+        }
         if (n_active) *n_active = (uint32_t)active.size();
         return SC_OK;
     }
@@ -279,6 +471,7 @@ int sc_server_create(sc_ctx* ctx, const sc_server_config* cfg, sc_server** out) 
     if ((e = s->d_descs.alloc(s->cfg.max_slots)) != cudaSuccess) return fail(e);
     if ((e = s->counter.alloc(1)) != cudaSuccess) return fail(e);
     if ((e = s->dirty_count.alloc(1)) != cudaSuccess) return fail(e);
+    if ((e = s->ring.init(kRingFloats)) != cudaSuccess) return fail(e);
     s->arena.reset(cfg->hbm_budget_bytes);
     s->grid = (uint32_t)(ctx->sms * batch_occupancy(0, 4, 1, kBatchMaskWords));
     *out = s;
@@ -294,7 +487,10 @@ int sc_server_destroy(sc_server* s) {
         if (s->stream) cudaStreamSynchronize(s->stream);
         for (Request* q : s->queue) delete q;
         for (Request* q : s->active) delete q;
-        for (Request* q : s->finished) delete q;
+        for (StepRecord& r : s->inflight)
+            for (Request* q : r.last) { if (q->image_own) cudaFreeHost(q->image); delete q; }
+        for (Request* q : s->finished) { if (q->image_own) cudaFreeHost(q->image); delete q; }
+        s->release_all();
         s->mem.reset(); s->d_jobs.reset(); s->d_descs.reset(); s->d_items.reset(); s->counter.reset();
         if (s->stream) cudaStreamDestroy(s->stream);
     }
@@ -356,13 +552,16 @@ int sc_server_poll(sc_server* s, uint64_t* id, float* xyz_out, size_t capacity, 
     SC_GUARD_BEGIN
     SERVER_LOCK(s);
     SC_REQUIRE(id, SC_E_INVALID, "null id");
+    int rc = s->collect(false);
+    if (rc != SC_OK) return rc;
     if (s->finished.empty()) { set_error("no finished request"); return SC_E_STATE; }
     Request* q = s->finished.front();
+    const size_t nf = 3ull * q->r.job.width * q->r.job.height;
     if (xyz_out) {
-        SC_REQUIRE(capacity >= q->result.size(), SC_E_INVALID, "output holds %zu floats, need %zu", capacity,
-                   q->result.size());
-        std::memcpy(xyz_out, q->result.data(), q->result.size() * sizeof(float));
+        SC_REQUIRE(capacity >= nf, SC_E_INVALID, "output holds %zu floats, need %zu", capacity, nf);
+        std::memcpy(xyz_out, q->image, nf * sizeof(float));
     }
+    s->free_image(q);
     *id = q->id;
     if (width) *width = q->r.job.width;
     if (height) *height = q->r.job.height;
@@ -379,7 +578,11 @@ int sc_server_cancel(sc_server* s, uint64_t id) {
     for (auto it = s->queue.begin(); it != s->queue.end(); ++it)
         if ((*it)->id == id) { delete *it; s->queue.erase(it); return SC_OK; }
     for (auto it = s->active.begin(); it != s->active.end(); ++it)
-        if ((*it)->id == id) {  // between steps nothing of this request is in flight
+        if ((*it)->id == id) {
+            // frames of it may still be queued: its range is reused only by work
+            // queued behind them on the same stream, and it leaves the queued
+            // steps' first-frame lists before it is deleted
+            for (StepRecord& r : s->inflight) r.first.erase(std::remove(r.first.begin(), r.first.end(), *it), r.first.end());
             s->arena.release((*it)->off, (*it)->bytes);
             delete *it;
             s->active.erase(it);
@@ -397,7 +600,7 @@ int sc_server_stats(sc_server* s, uint64_t* photons_traced, uint64_t* bytes_in_u
     if (photons_traced) *photons_traced = s->photons;
     if (bytes_in_use) *bytes_in_use = s->arena.used();
     if (queued) *queued = (uint32_t)s->queue.size();
-    if (active) *active = (uint32_t)s->active.size();
+    if (active) *active = (uint32_t)s->active.size() + s->retiring();  // with images still on their way
     if (finished) *finished = (uint32_t)s->finished.size();
     return SC_OK;
     SC_GUARD_END

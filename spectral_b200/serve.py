@@ -25,6 +25,7 @@ class Server:
         cfg = _lib.sc_server_config(int(budget_bytes), int(max_slots), int(chunk_photons))
         check(lib.sc_server_create(ctx.h, C.byref(cfg), C.byref(self.h)))
         self._dims = {}
+        self._buf = None
 
     def submit(self, job, frames=1, orbit_deg=0.0, target=ORBIT_TARGET, up=(0.0, 1.0, 0.0), vfov=42.0):
         r = _lib.sc_request()
@@ -44,9 +45,11 @@ class Server:
         """(id, xyz or None, (t_submit, t_admit, t_first_frame, t_done)) or None."""
         rid, w, h = C.c_uint64(), C.c_uint32(), C.c_uint32()
         times = (C.c_double * 4)()
-        # the largest possible image of any request still outstanding
+        # room for the largest image of any request still outstanding (buffer kept between polls)
         cap = max(self._dims.values()) if (want_image and self._dims) else 0
-        buf = np.empty(cap, np.float32) if cap else None
+        if cap and (self._buf is None or self._buf.size < cap):
+            self._buf = np.empty(cap, np.float32)
+        buf = self._buf
         rc = lib.sc_server_poll(self.h, C.byref(rid), buf.ctypes.data_as(C.POINTER(C.c_float)) if cap else None,
                                 cap, C.byref(w), C.byref(h), times)
         if rc == _lib.SC_E_STATE:
