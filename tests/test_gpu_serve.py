@@ -97,6 +97,42 @@ def test_budget_admission_and_cancel(ctx):
         s.cancel(12345)
 
 
+def test_queued_steps_overflowing_image_ring_and_cancel(ctx):
+    """Steps queue ahead of the host (two deep while requests wait): 24 requests
+    of 1024x1024 images (303 MB) finish before any poll, past the 256 MB pinned
+    ring, and each still equals its render alone; cancelling a session whose
+    frames are queued leaves the other request's result and frees the budget."""
+    big = [job(i, n=4096, side=1024, bins=1) for i in range(24)]
+    s = Server(ctx, budget_bytes=2 << 30, max_slots=8)
+    ids = [s.submit(j) for j in big]
+    while s.stats()["queued"] or s.stats()["active"]:
+        s.step()
+    got = {}
+    while (r := s.poll()) is not None:
+        got[r[0]] = r[1]
+    assert sorted(got) == sorted(ids) and s.stats()["bytes_in_use"] == 0
+    s.close()
+    for i in (0, 11, 23):
+        a = Server(ctx, budget_bytes=1 << 30)
+        rid = a.submit(big[i])
+        alone = drain(a)[rid]
+        a.close()
+        assert alone.sum() > 0 and got[ids[i]].tobytes() == alone.tobytes(), i
+    s = Server(ctx, budget_bytes=1 << 30)
+    session = s.submit(job(0), frames=6, orbit_deg=2.0)
+    single = s.submit(job(1))
+    s.step()
+    s.step()  # the session's frames are queued on the device
+    s.cancel(session)
+    res = drain(s)
+    assert list(res) == [single] and s.stats()["bytes_in_use"] == 0
+    a = Server(ctx, budget_bytes=1 << 30)
+    rid = a.submit(job(1))
+    assert drain(a)[rid].tobytes() == res[single].tobytes()
+    a.close()
+    s.close()
+
+
 def test_realtime_stream_completes(ctx):
     stream = poisson_requests(rate=60.0, seconds=1.0, seed=7, frames=(2, 6), photons=(2 ** 12, 2 ** 15),
                               side=(32, 128), bins=16)
