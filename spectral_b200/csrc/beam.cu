@@ -24,8 +24,9 @@
 // Lanes stay converged whatever the segment lengths and footprint sizes, and
 // the 32 atomics of one warp instruction hit 32 distinct pixels.  Film width
 // and height are below 2^16 (the box corner is packed into one word).
-// |d| is d2 * rsqrt(d2) (within 2 ulp) and |d| / r a multiply by 1/r, so a
-// deposit can differ from the reference's in the last few bits.
+// |d| is d2 * rsqrt(d2) (within 2 ulp), |d| / r a multiply by 1/r and the
+// tent's two sums fused, so a deposit can differ from the reference's in the
+// last few bits.
 #include "photon_trace.cuh"
 
 namespace sc {
@@ -37,7 +38,9 @@ constexpr uint32_t kMaxSteps = 4096u;
 
 struct BeamSeg { f3 o, d; float ds, power; uint32_t m, lane; };
 // One march step ready to splat: footprint centre and 1 / radius in pixels,
-// the step's colour (XYZ film) or weight and bin (spectral film), the footprint
+// the step's colour (XYZ film) or weight and bin (spectral film), times the
+// film's fixed-point scale (a power of two: exact, so a pixel's deposit
+// fixed_scaled(c * w) is to_fixed(c_unscaled * w, scale)), the footprint
 // box [x0, x0 + bw) x [y0, y0 + bh), the warp's lane layout over it (`rows` rows
 // of bw lanes per pass; lane / bw = (lane * magic) >> 16) and the tent sum,
 // all worked out one step per lane so the warp-wide splat does no division.
@@ -89,11 +92,19 @@ __device__ __forceinline__ uint32_t march_count(const PhotonParams& p, f3 o, f3 
 }
 
 // Tent weight max(1 - |d| / r, 0); the division is a multiply by 1/r (within
-// an ulp of the reference's quotient).
+// an ulp of the reference's quotient), both sums fused multiply-adds.
 __device__ __forceinline__ float tent(float dx2, float dy, float inv_r) {
-    const float d2 = dx2 + dy * dy;
+    const float d2 = __fmaf_rn(dy, dy, dx2);
     const float d = d2 > 0.0f ? d2 * rsqrtf(d2) : 0.0f;  // |d| within 2 ulp
-    return fmaxf(1.0f - d * inv_r, 0.0f);
+    return fmaxf(__fmaf_rn(-d, inv_r, 1.0f), 0.0f);
+}
+
+// Fixed-point value of an already scaled, non-negative deposit: the same
+// integer as to_fixed(x, scale) for y = x * scale (scale a power of two), with
+// the common case (y < 2^23) in two ALU operations and no sign test.
+__device__ __forceinline__ unsigned long long fixed_scaled(float y) {
+    if (y < 8388608.0f) return (unsigned long long)(__float_as_uint(y + 8388608.0f) - 0x4B000000u);
+    return to_fixed(y, 1.0f);
 }
 
 // Dirty bits of the tiles under a footprint box, set by the step's own lane
@@ -156,8 +167,8 @@ __device__ __forceinline__ StepRec beam_step(const PhotonParams& p, uint32_t* sm
     const uint32_t rows = bw <= 32u ? 32u / bw : 1u;
     R.box = bw | (bh << 8) | (rows << 16) | (((bh + rows - 1u) / rows) << 24);
     R.magic = (65536u + bw - 1u) / bw;
-    if (SPEC) { R.c0 = weight; R.c1 = R.c2 = 0.0f; }
-    else { R.c0 = pay.x * weight; R.c1 = pay.y * weight; R.c2 = pay.z * weight; }
+    if (SPEC) { R.c0 = weight * p.scale; R.c1 = R.c2 = 0.0f; }
+    else { R.c0 = pay.x * weight * p.scale; R.c1 = pay.y * weight * p.scale; R.c2 = pay.z * weight * p.scale; }
     R.bin = __float_as_uint(pay.w);
     // the tent sum over the box, row by row as the reference adds it
     float wsum = 0.0f;
@@ -180,11 +191,11 @@ __device__ __forceinline__ void deposit_pixel(const PhotonParams& p, uint32_t px
                                               float w) {
     unsigned long long* c = p.film + film_cell(px, py, p.tiles_x, p.channels);
     if (SPEC) {
-        red_u64(c + R.bin, to_fixed(R.c0 * w, p.scale));
+        red_u64(c + R.bin, fixed_scaled(R.c0 * w));
     } else {
-        red_u64(c, to_fixed(R.c0 * w, p.scale));
-        red_u64(c + 1, to_fixed(R.c1 * w, p.scale));
-        red_u64(c + 2, to_fixed(R.c2 * w, p.scale));
+        red_u64(c, fixed_scaled(R.c0 * w));
+        red_u64(c + 1, fixed_scaled(R.c1 * w));
+        red_u64(c + 2, fixed_scaled(R.c2 * w));
     }
 }
 
@@ -248,10 +259,10 @@ __device__ __forceinline__ void run_add(const PhotonParams& p, BoxRun& run, cons
         if (py < y0 + bh) {
             const float w = tent(dx2, (float)py - R.cy, inv_r) * inv;
             if (w > 0.0f) {
-                run.acc[k][0] += to_fixed(R.c0 * w, p.scale);
+                run.acc[k][0] += fixed_scaled(R.c0 * w);
                 if (!SPEC) {
-                    run.acc[k][1] += to_fixed(R.c1 * w, p.scale);
-                    run.acc[k][2] += to_fixed(R.c2 * w, p.scale);
+                    run.acc[k][1] += fixed_scaled(R.c1 * w);
+                    run.acc[k][2] += fixed_scaled(R.c2 * w);
                 }
             }
         }
