@@ -326,10 +326,10 @@ typedef struct {
 } sc_scene_job;
 /* Tuning knobs, 0 = default: photons per work chunk (queue granularity),
  * register bound (minimum CTAs per SM, 4 or 5), warp-aggregated splats, grid,
- * and per_photon = 1 to run each photon's haze samples in its own lane instead
+ * per_photon = 1 to run each photon's haze samples in its own lane instead
  * of the default warp-split transport (segments buffered per warp, samples
- * processed as one converged list). */
-typedef struct { uint32_t chunk_photons, minb, aggregate, grid, per_photon; } sc_batch_tuning;
+ * processed as one converged list), and threads per CTA (128 or 256). */
+typedef struct { uint32_t chunk_photons, minb, aggregate, grid, per_photon, block; } sc_batch_tuning;
 int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs,
                     const sc_batch_tuning* tuning, sc_batch** out);
 int sc_batch_destroy(sc_batch* b);

@@ -86,7 +86,7 @@ class sc_scene_job(C.Structure):
 
 class sc_batch_tuning(C.Structure):
     _fields_ = [("chunk_photons", C.c_uint32), ("minb", C.c_uint32), ("aggregate", C.c_uint32), ("grid", C.c_uint32),
-                ("per_photon", C.c_uint32)]
+                ("per_photon", C.c_uint32), ("block", C.c_uint32)]
 
 
 class sc_server_config(C.Structure):

@@ -43,10 +43,10 @@ def prism_jobs(specs):
 
 
 class Batch:
-    def __init__(self, ctx, jobs, chunk_photons=0, minb=0, aggregate=0, per_photon=0):
+    def __init__(self, ctx, jobs, chunk_photons=0, minb=0, aggregate=0, per_photon=0, block=0):
         self.jobs = jobs
         self.h = C.c_void_p()
-        t = _lib.sc_batch_tuning(chunk_photons, minb, aggregate, 0, per_photon)
+        t = _lib.sc_batch_tuning(chunk_photons, minb, aggregate, 0, per_photon, block)
         check(lib.sc_batch_create(ctx.h, jobs, len(jobs), C.byref(t), C.byref(self.h)))
         tp, fb, xf, jb = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
         check(lib.sc_batch_info(self.h, C.byref(tp), C.byref(fb), C.byref(xf), C.byref(jb)))
@@ -57,16 +57,16 @@ class Batch:
         t = _lib.sc_batch_tuning()
         check(lib.sc_batch_autotune(self.h, C.byref(t)))
         return dict(chunk_photons=t.chunk_photons, minb=t.minb, aggregate=t.aggregate, grid=t.grid,
-                    per_photon=t.per_photon)
+                    per_photon=t.per_photon, block=t.block)
 
     def tuning(self):
         t = _lib.sc_batch_tuning()
         check(lib.sc_batch_get_tuning(self.h, C.byref(t)))
         return dict(chunk_photons=t.chunk_photons, minb=t.minb, aggregate=t.aggregate, grid=t.grid,
-                    per_photon=t.per_photon)
+                    per_photon=t.per_photon, block=t.block)
 
-    def set_tuning(self, chunk_photons=0, minb=0, aggregate=0, grid=0, per_photon=0):
-        t = _lib.sc_batch_tuning(chunk_photons, minb, aggregate, grid, per_photon)
+    def set_tuning(self, chunk_photons=0, minb=0, aggregate=0, grid=0, per_photon=0, block=0):
+        t = _lib.sc_batch_tuning(chunk_photons, minb, aggregate, grid, per_photon, block)
         check(lib.sc_batch_set_tuning(self.h, C.byref(t)))
 
     def update_jobs(self, jobs):

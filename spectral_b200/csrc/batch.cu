@@ -96,27 +96,29 @@ BatchFn batch_fn(int agg, int minb, int split) { return split ? batch_fn_t<true>
 static_assert(sizeof(WarpSlot) % 16 == 0, "warp slot must be a multiple of 16 bytes");
 static_assert(sizeof(WarpSlot) == sizeof(BatchSlotImage), "slot image layout");
 
-size_t batch_smem(uint32_t mask_words_max, int split) {
-    return kCmfBytes16 + 8 * sizeof(WarpSlot) + 8 * mask_words_max * sizeof(uint32_t) +
-           (split ? 8 * sizeof(WarpSplitSmem) : 0);
+size_t batch_smem(uint32_t mask_words_max, int split, uint32_t block) {
+    const size_t warps = block / 32u;
+    return kCmfBytes16 + warps * sizeof(WarpSlot) + warps * mask_words_max * sizeof(uint32_t) +
+           (split ? warps * sizeof(WarpSplitSmem) : 0);
 }
 
-int batch_occupancy(int agg, int minb, int split, uint32_t mask_words_max) {
+int batch_occupancy(int agg, int minb, int split, uint32_t mask_words_max, uint32_t block) {
     int n = 0;
     const void* fn = reinterpret_cast<const void*>(batch_fn(agg, minb, split));
-    const size_t smem = batch_smem(mask_words_max, split);
+    const size_t smem = batch_smem(mask_words_max, split, block);
     if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, smem) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)block, smem) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 
 cudaError_t launch_batch(const BatchJobDev* jobs, const WorkItem* items, uint32_t n_items, uint32_t* counter,
                          const float* cmf, uint32_t mask_words_max, int agg, int minb, int split, uint32_t grid,
-                         cudaStream_t s) {
-    const size_t smem = batch_smem(mask_words_max, split);  // attribute set by batch_occupancy before capture
+                         cudaStream_t s, uint32_t block) {
+    // the shared-memory attribute was raised by batch_occupancy before any capture
+    const size_t smem = batch_smem(mask_words_max, split, block);
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
-    batch_fn(agg, minb, split)<<<grid, 256, smem, s>>>(jobs, items, n_items, counter, cmf, mask_words_max);
+    batch_fn(agg, minb, split)<<<grid, block, smem, s>>>(jobs, items, n_items, counter, cmf, mask_words_max);
     return cudaGetLastError();
 }
 

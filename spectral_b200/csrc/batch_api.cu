@@ -1,7 +1,8 @@
 // extern "C" batch object: many uneven scenes in one persistent, graph-captured
 // launch (batch.cu), the same work as plain per-scene launches for comparison,
-// and an autotuner that picks chunk size, register bound and splat aggregation
-// by timing the batch itself.
+// and an autotuner that picks chunk size (work-queue granularity), threads per
+// CTA, register bound, splat aggregation and transport by timing the batch
+// itself.
 #include <algorithm>
 #include <cmath>
 #include <numeric>
@@ -151,7 +152,8 @@ struct sc_batch {
         n.minb = n.minb >= 5 ? 5 : 4;
         n.aggregate = n.aggregate ? 1 : 0;
         n.per_photon = n.per_photon ? 1 : 0;
-        const int occ = batch_occupancy((int)n.aggregate, (int)n.minb, n.per_photon ? 0 : 1, kBatchMaskWords);
+        n.block = n.block == 128u ? 128u : 256u;
+        const int occ = batch_occupancy((int)n.aggregate, (int)n.minb, n.per_photon ? 0 : 1, kBatchMaskWords, n.block);
         grid = n.grid ? n.grid : (uint32_t)(ctx->sms * occ);
         if (n.chunk_photons != tuning.chunk_photons || n_items == 0) {
             int rc = build_items(n.chunk_photons);
@@ -165,7 +167,8 @@ struct sc_batch {
 
     int enqueue_batch(cudaStream_t s) {
         SC_CUDA(launch_batch(d_jobs.p, d_items.p, n_items, counter.p, ctx->cmf.p, kBatchMaskWords,
-                             (int)tuning.aggregate, (int)tuning.minb, tuning.per_photon ? 0 : 1, grid, s));
+                             (int)tuning.aggregate, (int)tuning.minb, tuning.per_photon ? 0 : 1, grid, s,
+                             tuning.block));
         // the drain rewrites the images: wait for the last asynchronous copy of them
         SC_CUDA(cudaStreamWaitEvent(s, copied, cudaEventWaitExternal));
         SC_CUDA(launch_reduce_many(d_descs.p, (uint32_t)jobs.size(), total_words, true, max_channels, dirty_list.p,
@@ -375,11 +378,12 @@ int sc_batch_autotune(sc_batch* b, sc_batch_tuning* chosen) {
     SC_CUDA(cudaEventCreate(&e1));
     sc_batch_tuning best{};
     float best_ms = 1e30f;
+    for (uint32_t block : {256u, 128u})
     for (uint32_t per_photon : {0u, 1u})
     for (uint32_t chunk : {512u, 2048u, 8192u})
         for (uint32_t minb : {4u, 5u})
             for (uint32_t agg : {0u, 1u}) {
-                sc_batch_tuning t{chunk, minb, agg, 0, per_photon};
+                sc_batch_tuning t{chunk, minb, agg, 0, per_photon, block};
                 int rc = b->apply_tuning(t);
                 if (rc == SC_OK) rc = b->run(b->stream);  // warm-up (also builds the graph)
                 if (rc != SC_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
@@ -518,7 +522,7 @@ int sc_batch_stats(sc_batch* b, uint64_t out[6]) {
     // dirty tiles of one pass: trace only, count the set bits, then drain
     SC_CUDA(launch_batch(b->d_jobs.p, b->d_items.p, b->n_items, b->counter.p, b->ctx->cmf.p, kBatchMaskWords,
                          (int)b->tuning.aggregate, (int)b->tuning.minb, b->tuning.per_photon ? 0 : 1, b->grid,
-                         b->stream));
+                         b->stream, b->tuning.block));
     std::vector<uint32_t> fl(b->flags.n);
     SC_CUDA(cudaMemcpyAsync(fl.data(), b->flags.p, b->flags.bytes(), cudaMemcpyDeviceToHost, b->stream));
     SC_CUDA(cudaStreamSynchronize(b->stream));

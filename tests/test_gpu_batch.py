@@ -65,7 +65,9 @@ def test_autotune_and_tunings_agree(ctx):
     ref = b.read_all_xyz().copy()
     chosen = b.autotune()
     assert chosen["chunk_photons"] in (512, 2048, 8192) and chosen["minb"] in (4, 5)
-    for t in [(64, 4, 0, 0, 0), (1024, 5, 1, 0, 0), (32, 4, 1, 0, 1), (96, 5, 0, 0, 1), (4096, 4, 0, 7, 0)]:
+    assert chosen["block"] in (128, 256)
+    for t in [(64, 4, 0, 0, 0), (1024, 5, 1, 0, 0), (32, 4, 1, 0, 1), (96, 5, 0, 0, 1), (4096, 4, 0, 7, 0),
+              (512, 4, 0, 0, 0, 128), (2048, 5, 1, 0, 1, 128), (96, 4, 0, 13, 0, 128)]:
         b.set_tuning(*t)
         b.run()
         assert b.read_all_xyz().tobytes() == ref.tobytes(), t
