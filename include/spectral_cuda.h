@@ -203,6 +203,10 @@ int sc_tracer_set_camera(sc_tracer* t, const sc_camera* cam);
 /* clear_accum (lib.rs:386-389): zero the sum and the sample count. */
 int sc_tracer_clear_accum(sc_tracer* t);
 int sc_tracer_dims(sc_tracer* t, uint32_t* width, uint32_t* height);
+/* set_spectral (lib.rs:369-372): on (the default) refracts at the hero
+ * wavelength; off uses n(550 nm) for every path (trace.wgsl:477-480).  The
+ * accumulation is kept, as in the reference. */
+int sc_tracer_set_spectral(sc_tracer* t, int on);
 /* The CUDA stream (cudaStream_t) all of this tracer's work runs on, for callers
  * that order or time their own work against it.  Owned by the tracer. */
 int sc_tracer_stream(sc_tracer* t, void** stream);
@@ -222,6 +226,10 @@ int sc_atomic_film_resolve(sc_atomic_film* f);
 int sc_atomic_film_read_accum(sc_atomic_film* f, float* out);
 int sc_atomic_film_clear_film(sc_atomic_film* f);
 int sc_atomic_film_clear_accum(sc_atomic_film* f);
+/* auto_expose_accum (film.rs:262-270): max(scale / max(max Y, 1e-6), 1). */
+int sc_atomic_film_auto_expose_accum(sc_atomic_film* f, float scale, float* exposure);
+/* to_rgb8 (film.rs:243-258): XYZ -> linear sRGB -> tonemap_to_u8, out 3*w*h bytes. */
+int sc_atomic_film_to_rgb8(sc_atomic_film* f, float exposure, uint8_t* out);
 /* The CUDA stream (cudaStream_t) this film's work runs on, for callers that
  * order or time their own work against it.  Owned by the film. */
 int sc_atomic_film_stream(sc_atomic_film* f, void** stream);

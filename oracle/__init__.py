@@ -78,6 +78,7 @@ for name, res, args in [
     ("or_rng_draws_f32", None, [_u32, _u32, _u32, P(_f32)]),
     ("or_glass_n", _f32, [_u32, _f32]),
     ("or_glass_n_many", None, [_u32, P(_f32), C.c_size_t, P(_f32)]),
+    ("or_tracer_set_spectral", None, [C.c_int]),
     ("or_load_tables_csv", _i32, [C.c_char_p]),
     ("or_get_tables", None, [P(_f32)]),
     ("or_cmf", None, [_f32, P(_f32)]),
@@ -192,12 +193,15 @@ def simulate_photon(scene, beam, p, idx, max_pairs=9):
 
 
 def tracer_accumulate(scene, cam, w, h, illuminant, seed, spp, base=0, max_bounces=8, threads=8, ext=None,
-                      out=None):
-    """CpuTracer::accumulate into `out` (3*w*h f32 running sum); returns it."""
+                      out=None, spectral=True):
+    """CpuTracer::accumulate into `out` (3*w*h f32 running sum); returns it.
+    spectral=False: dielectrics at n(550 nm), as the GPU tracer's set_spectral(false)."""
     out = np.zeros(3 * w * h, np.float32) if out is None else out
     _lib.or_tracer_set_ext(C.byref(ext) if ext is not None else None)
+    _lib.or_tracer_set_spectral(1 if spectral else 0)
     _lib.or_tracer_accumulate_mt(C.byref(scene.c), C.byref(cam), w, h, illuminant, seed, spp, base, max_bounces,
                                  fp(out), threads)
+    _lib.or_tracer_set_spectral(1)
     _lib.or_tracer_set_ext(None)
     return out
 

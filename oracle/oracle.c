@@ -678,6 +678,8 @@ static or_tracer_ext g_ext; /* zero: reference behaviour */
 void or_tracer_set_ext(const or_tracer_ext* ext) {
     if (ext) g_ext = *ext; else memset(&g_ext, 0, sizeof g_ext);
 }
+static int g_spectral = 1;
+void or_tracer_set_spectral(int on) { g_spectral = on ? 1 : 0; }
 
 void or_tracer_sample(const or_scene* sc, const or_camera* cam, uint32_t W, uint32_t H,
                       uint32_t illum, uint32_t seed, uint32_t px, uint32_t py, uint32_t sidx,
@@ -715,7 +717,7 @@ void or_tracer_sample(const or_scene* sc, const or_camera* cam, uint32_t W, uint
             break;
         }
         const or_mat* m = &sc->mats[mi];
-        float nh = m->kind == 1u ? or_glass_n(m->glass, lam[0]) : 1.0f;
+        float nh = m->kind == 1u ? or_glass_n(m->glass, g_spectral ? lam[0] : 550.0f) : 1.0f;
         v3 nd; float w;
         scatter(m, d, &h, nh, &r, &nd, &w);
         for (int k = 0; k < 4; ++k) tp[k] *= w;

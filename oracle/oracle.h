@@ -118,6 +118,9 @@ void or_lighttrace(const or_scene* sc, const float screen_cuv[9], uint32_t w, ui
  * scatters (survival p = min(throughput, 0.95), throughput /= p). */
 typedef struct { float center[3]; float radius; float scale; uint32_t rr_start; } or_tracer_ext;
 void or_tracer_set_ext(const or_tracer_ext* ext);
+/* GpuTracer::set_spectral (spectral-gpu/src/lib.rs:369-372; trace.wgsl:477-480):
+ * 0 makes every dielectric hit use n(550 nm) instead of n(hero wavelength). */
+void or_tracer_set_spectral(int on);
 
 /* Hero-wavelength camera tracer (tracer.rs:44-141). Accumulates spp samples starting
  * at sample index `base` into sum_xyz (3*w*h); rows [row0,row1). */

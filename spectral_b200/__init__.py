@@ -369,6 +369,10 @@ class GpuTracer:
     def set_camera(self, camera):
         check(lib.sc_tracer_set_camera(self.h, C.byref(camera.c)))
 
+    def set_spectral(self, on):
+        """set_spectral (spectral-gpu/src/lib.rs:369-372): off = dielectrics at n(550 nm)."""
+        check(lib.sc_tracer_set_spectral(self.h, 1 if on else 0))
+
     def clear_accum(self):
         check(lib.sc_tracer_clear_accum(self.h))
 
@@ -424,6 +428,18 @@ class AtomicFilm:
 
     def clear_accum(self):
         check(lib.sc_atomic_film_clear_accum(self.h))
+
+    def auto_expose_accum(self, scale=1.0):
+        """auto_expose_accum (spectral-gpu/src/film.rs:262-270) on the device."""
+        e = C.c_float()
+        check(lib.sc_atomic_film_auto_expose_accum(self.h, float(scale), C.byref(e)))
+        return e.value
+
+    def to_rgb8(self, exposure):
+        """to_rgb8 (spectral-gpu/src/film.rs:243-258): 3*w*h bytes."""
+        out = np.empty(3 * self.width * self.height, np.uint8)
+        check(lib.sc_atomic_film_to_rgb8(self.h, float(exposure), out.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return out
 
     def dims(self):
         return self.width, self.height

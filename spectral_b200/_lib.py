@@ -114,6 +114,9 @@ PROTOTYPES = {
     "sc_load_sensor_tables": (_i32, [C.c_char_p, P(_f32)]),
     "sc_camera_look_at": (_i32, [P(_f32), P(_f32), P(_f32), _f32, _f32, P(sc_camera)]),
     "sc_glass_n": (_f32, [_u32, _f32]),
+    "sc_tracer_set_spectral": (_i32, [_vp, _i32]),
+    "sc_atomic_film_auto_expose_accum": (_i32, [_vp, _f32, P(_f32)]),
+    "sc_atomic_film_to_rgb8": (_i32, [_vp, _f32, P(C.c_uint8)]),
     "sc_glass_n_many": (_i32, [_u32, P(_f32), C.c_size_t, P(_f32)]),
     "sc_glass_n_device": (_i32, [_vp, _u32, _vp, C.c_size_t, _vp, _vp]),
     "sc_rng_draws": (_i32, [_vp, _u32, _u32, _u32, P(_u32)]),

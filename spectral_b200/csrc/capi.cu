@@ -825,6 +825,8 @@ struct sc_atomic_film {
     uint32_t w = 0, h = 0;
     DevBuf<uint32_t> film;
     DevBuf<float> accum;
+    DevBuf<uint32_t> work;  // max-Y bits of auto_expose_accum
+    DevBuf<uint8_t> rgb;    // to_rgb8 staging
 };
 
 extern "C" {
@@ -909,6 +911,33 @@ int sc_atomic_film_read_accum(sc_atomic_film* f, float* out) {
     AFILM_LOCK(f);
     SC_REQUIRE(out, SC_E_INVALID, "null output");
     SC_CUDA(cudaMemcpyAsync(out, f->accum.p, f->accum.bytes(), cudaMemcpyDeviceToHost, f->stream));
+    SC_CUDA(cudaStreamSynchronize(f->stream));
+    return SC_OK;
+    SC_GUARD_END
+}
+int sc_atomic_film_auto_expose_accum(sc_atomic_film* f, float scale, float* exposure) {
+    SC_GUARD_BEGIN
+    AFILM_LOCK(f);
+    SC_REQUIRE(exposure, SC_E_INVALID, "null output");
+    if (!f->work.p) SC_CUDA(f->work.alloc(1));
+    SC_CUDA(launch_composite_max_y(f->accum.p, nullptr, f->w * f->h, f->work.p, f->stream));
+    uint32_t bits = 0;
+    SC_CUDA(cudaMemcpyAsync(&bits, f->work.p, 4, cudaMemcpyDeviceToHost, f->stream));
+    SC_CUDA(cudaStreamSynchronize(f->stream));
+    float max_y;
+    std::memcpy(&max_y, &bits, 4);
+    *exposure = std::max(scale / std::max(max_y, 1e-6f), 1.0f);
+    return SC_OK;
+    SC_GUARD_END
+}
+int sc_atomic_film_to_rgb8(sc_atomic_film* f, float exposure, uint8_t* out) {
+    SC_GUARD_BEGIN
+    AFILM_LOCK(f);
+    SC_REQUIRE(out, SC_E_INVALID, "null output");
+    const size_t n = (size_t)f->w * f->h;
+    if (f->rgb.n < 3 * n) SC_CUDA(f->rgb.alloc(3 * n));
+    SC_CUDA(launch_to_rgb8(f->accum.p, nullptr, (uint32_t)n, exposure, f->rgb.p, f->stream));
+    SC_CUDA(cudaMemcpyAsync(out, f->rgb.p, 3 * n, cudaMemcpyDeviceToHost, f->stream));
     SC_CUDA(cudaStreamSynchronize(f->stream));
     return SC_OK;
     SC_GUARD_END

@@ -152,7 +152,7 @@ __device__ __forceinline__ bool shade_path(const TracerSmem& s, const SceneView&
     h.point = add(P.o, mul(P.d, t));
     h.normal = n;
     h.front_face = ((info >> 16) & 1u) != 0u;
-    const float nh = m.kind == 1u ? glass_n(m.glass, lane_lambda(P.u, 0)) : 1.0f;
+    const float nh = m.kind == 1u ? glass_n(m.glass, s.p.spectral ? lane_lambda(P.u, 0) : 550.0f) : 1.0f;
     Rng r;
     r.state = P.rs;
     f3 nd;

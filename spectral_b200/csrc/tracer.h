@@ -12,6 +12,7 @@ struct TracerParams {
     uint32_t width, height, seed, illuminant;
     float background, horizon;
     uint32_t has_horizon, max_depth, rr_start;
+    uint32_t spectral;  // 1: n at the hero wavelength; 0: n(550 nm) for every path (trace.wgsl:477-480)
     f3 em_center;
     float em_radius, em_scale;
     const sc_primitive* prims; const sc_plane* planes; const sc_material* mats;

@@ -180,6 +180,7 @@ int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, c
     hp.cam = *cam; hp.width = width; hp.height = height; hp.seed = seed; hp.illuminant = illuminant;
     hp.background = background; hp.horizon = horizon; hp.has_horizon = has_horizon ? 1u : 0u;
     hp.max_depth = o.max_depth; hp.rr_start = o.rr_start;
+    hp.spectral = 1u;
     hp.em_center = ld3(o.emitter_center); hp.em_radius = o.emitter_radius; hp.em_scale = o.emitter_scale;
     hp.prims = t->prims.p; hp.planes = t->planes.p; hp.mats = t->mats.p;
     hp.n_prims = n_prims; hp.n_planes = n_planes; hp.n_mats = n_mats;
@@ -249,6 +250,14 @@ int sc_tracer_set_camera(sc_tracer* t, const sc_camera* cam) {
     TR_LOCK(t);
     SC_REQUIRE(cam, SC_E_INVALID, "null camera");
     t->hp.cam = *cam;
+    return t->upload_params();
+    SC_GUARD_END
+}
+
+int sc_tracer_set_spectral(sc_tracer* t, int on) {
+    SC_GUARD_BEGIN
+    TR_LOCK(t);
+    t->hp.spectral = on ? 1u : 0u;
     return t->upload_params();
     SC_GUARD_END
 }

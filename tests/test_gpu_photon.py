@@ -338,6 +338,17 @@ def test_atomic_film(ctx):
     assert (raw == ref).all() and (raw > 0).any()
     f.resolve()
     assert not f.read_film_raw().any()
-    assert np.array_equal(f.accum(), ref.astype(np.float32) / np.float32(4096.0))
+    acc = f.accum()
+    assert np.array_equal(acc, ref.astype(np.float32) / np.float32(4096.0))
+    # auto_expose_accum and to_rgb8 (film.rs:243-270) against the oracle's sensor math
+    exp = f.auto_expose_accum(1.0)
+    assert exp == max(np.float32(1.0) / max(acc[1::3].max(), np.float32(1e-6)), np.float32(1.0))
+    rgb = f.to_rgb8(exp).reshape(-1, 3).astype(int)
+    ref8, out, lin = np.zeros_like(rgb), (C.c_uint8 * 3)(), np.zeros(3, np.float32)
+    for i in range(w * h):
+        oracle.lib.or_xyz_to_linear_srgb(oracle.fp(acc[3 * i:3 * i + 3].copy()), oracle.fp(lin))
+        oracle.lib.or_tonemap_to_u8(oracle.fp(lin), exp, out)
+        ref8[i] = list(out)
+    assert rgb.any() and np.abs(rgb - ref8).max() <= 1 and (rgb != ref8).mean() < 1e-2
     f.clear_accum()
     assert not f.accum().any()

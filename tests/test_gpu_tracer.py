@@ -99,6 +99,29 @@ def test_dielectric_scene_bit_identical(ctx):
     assert paths == 96 * 64 * 8 and segs > paths
 
 
+def test_set_spectral_off_uses_n550_bit_identical(ctx):
+    """set_spectral(false) (lib.rs:369-372, trace.wgsl:477-480): every dielectric
+    hit refracts with n(550 nm); the image equals the oracle's with the same
+    switch, and differs from the dispersive image."""
+    s = sb.Scene(background=1.0, horizon=2.0)
+    s.add_sphere((0, 0, -3), 1.0, sb.Dielectric(sb.SF11))
+    s.add_solid(axis_box((-3, -2, -6), (-1.5, 2, -4)), sb.Dielectric(sb.BK7))
+    cam = sb.Camera.look_at((0, 0.3, 0.5), (0, 0, -3), (0, 1, 0), 55.0, 1.5)
+    t = sb.GpuTracer(ctx, s, cam, 80, 56, sb.D65, 21)
+    t.set_spectral(False)
+    t.accumulate(8)
+    off = t.read_xyz()
+    cpu = oracle.tracer_accumulate(oscene(s), ocam(cam), 80, 56, 0, 21, 8, spectral=False) / np.float32(8)
+    assert off.tobytes() == cpu.tobytes()
+    t.clear_accum()
+    t.set_spectral(True)
+    t.accumulate(8)
+    on = t.read_xyz()
+    assert on.tobytes() != off.tobytes()
+    cpu_on = oracle.tracer_accumulate(oscene(s), ocam(cam), 80, 56, 0, 21, 8) / np.float32(8)  # cleared: from 0
+    assert on.tobytes() == cpu_on.tobytes()
+
+
 def test_background_integrates_to_d65_and_illuminant_a(ctx):
     cam = sb.Camera.look_at((0, 0, 0), (0, 0, -1), (0, 1, 0), 60.0, 1.0)
     t = sb.GpuTracer(ctx, sb.Scene(background=1.0), cam, 32, 32, sb.D65, 7)
