@@ -89,6 +89,10 @@ int sc_load_sensor_tables(const char* csv_path, float* out_5x71);
 /* Camera::look_at (spectral-core/src/camera.rs:15-27). */
 int sc_camera_look_at(const float origin[3], const float target[3], const float up[3],
                       float vfov_deg, float aspect, sc_camera* out);
+/* camera_proj_params (spectral-gpu/src/vol_photons.rs:100-115): out[16] =
+ * (origin, 0), (horizontal unit, |horizontal|), (vertical unit, |vertical|),
+ * (origin - horizontal/2 - vertical/2 - lower_left, 0). */
+int sc_camera_proj_params(const sc_camera* cam, float out[16]);
 /* Glass::n (spectral-core/src/sellmeier.rs:28-44), f64 internally. */
 float sc_glass_n(uint32_t glass, float lambda_nm);
 /* Glass::n over an array on the host: out[i] = sc_glass_n(glass, lambda_nm[i]).

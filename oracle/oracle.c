@@ -332,6 +332,12 @@ static inline int proj(const proj_t* P, v3 p, float* s, float* t, float* depth) 
     if (ss >= 0.0f && ss < 1.0f && tt >= 0.0f && tt < 1.0f) { *s = ss; *t = tt; *depth = -c; return 1; }
     return 0;
 }
+void or_camera_proj_params(const or_camera* c, float out[16]) {
+    const proj_t P = proj_make(c);
+    const float v[16] = {P.o.x, P.o.y, P.o.z, 0.0f, P.u.x, P.u.y, P.u.z, P.vw,
+                         P.v.x, P.v.y, P.v.z, P.vh, P.w.x, P.w.y, P.w.z, 0.0f};
+    memcpy(out, v, sizeof v);
+}
 int or_camera_project(const or_camera* c, const float p[3], float out[3]) {
     proj_t P = proj_make(c);
     return proj(&P, L(p), &out[0], &out[1], &out[2]);

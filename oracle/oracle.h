@@ -81,6 +81,8 @@ void or_camera_look_at(const float origin[3], const float target[3], const float
                        float vfov_deg, float aspect, or_camera* out);
 void or_camera_primary_ray(const or_camera* c, float s, float t, float o[3], float d[3]);
 int or_camera_project(const or_camera* c, const float p[3], float out_std[3]);
+/* camera_proj_params (spectral-gpu/src/vol_photons.rs:100-115), 16 floats. */
+void or_camera_proj_params(const or_camera* c, float out[16]);
 
 /* volume.rs */
 float or_phase_hg(float g, float cos_theta);

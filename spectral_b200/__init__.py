@@ -140,6 +140,14 @@ class VolWeights:
         return _lib.sc_vol_weights(self.sigma_s, self.sigma_t, self.g)
 
 
+def camera_proj_params(camera):
+    """camera_proj_params (spectral-gpu/src/vol_photons.rs:100-115): 4x4 float32,
+    rows (origin, 0), (u_hat, vw), (v_hat, vh), (w, 0)."""
+    out = np.empty(16, np.float32)
+    check(lib.sc_camera_proj_params(C.byref(camera.c), out.ctypes.data_as(C.POINTER(C.c_float))))
+    return out.reshape(4, 4)
+
+
 def glass_n(glass, lambda_nm):
     """Glass::n (spectral-core/src/sellmeier.rs:28-44) of one wavelength in nm,
     or, for an array, of every element (float32 array of the same shape)."""

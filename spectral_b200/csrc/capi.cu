@@ -279,6 +279,17 @@ int sc_camera_look_at(const float origin[3], const float target[3], const float 
     SC_GUARD_END
 }
 
+int sc_camera_proj_params(const sc_camera* cam, float out[16]) {
+    SC_GUARD_BEGIN
+    SC_REQUIRE(cam && out, SC_E_INVALID, "null argument");
+    const Proj p = make_proj(*cam);  // the basis the photon kernels project with
+    const float v[16] = {p.o.x, p.o.y, p.o.z, 0.0f, p.u.x, p.u.y, p.u.z, p.vw,
+                         p.v.x, p.v.y, p.v.z, p.vh, p.w.x, p.w.y, p.w.z, 0.0f};
+    std::memcpy(out, v, sizeof v);
+    return SC_OK;
+    SC_GUARD_END
+}
+
 float sc_glass_n(uint32_t glass, float lambda_nm) { return glass_n(glass, lambda_nm); }
 
 int sc_glass_n_many(uint32_t glass, const float* lambda_nm, size_t n, float* out) {

@@ -75,6 +75,18 @@ def test_glass_index_every_f32_wavelength_equals_oracle():
         sb.glass_n(4, lam[:4])
 
 
+def test_camera_proj_params_bitwise_equals_oracle():
+    for args in [((0.5, -0.5, 12.0), (0.5, -0.5, 0.0), (0, 1, 0), 42.0, 1.0),
+                 ((3.0, 2.0, 9.0), (0.1, -0.3, 0.2), (0, 1, 0), 35.0, 16 / 9)]:
+        cam = sb.Camera.look_at(*args)
+        got = sb.camera_proj_params(cam)
+        ref = np.empty(16, np.float32)
+        oc = oracle.camera_look_at(*args)
+        oracle.lib.or_camera_proj_params(C.byref(oc), oracle.fp(ref))
+        assert got.tobytes() == ref.tobytes()
+        assert abs(np.linalg.norm(got[1, :3]) - 1.0) < 1e-6 and got[0, 3] == 0.0 and got[1, 3] > 0.0
+
+
 def test_sensor_tables_equal_oracle():
     assert sb.sample_tables().tobytes() == oracle.tables().tobytes()
 
