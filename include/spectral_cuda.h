@@ -211,6 +211,12 @@ int sc_tracer_dims(sc_tracer* t, uint32_t* width, uint32_t* height);
  * wavelength; off uses n(550 nm) for every path (trace.wgsl:477-480).  The
  * accumulation is kept, as in the reference. */
 int sc_tracer_set_spectral(sc_tracer* t, int on);
+/* Trace only image rows [row_begin, row_end) in later accumulate calls (all
+ * rows by default; no counterpart in the reference).  A pixel's samples are
+ * keyed by the pixel and sample index, so a row renders the same whichever
+ * rows are traced with it: GPUs that own bands of rows gather their bands into
+ * the full image with no reduction.  Rows outside the range keep their sums. */
+int sc_tracer_set_rows(sc_tracer* t, uint32_t row_begin, uint32_t row_end);
 /* The CUDA stream (cudaStream_t) all of this tracer's work runs on, for callers
  * that order or time their own work against it.  Owned by the tracer. */
 int sc_tracer_stream(sc_tracer* t, void** stream);

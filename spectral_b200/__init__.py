@@ -381,6 +381,10 @@ class GpuTracer:
         """set_spectral (spectral-gpu/src/lib.rs:369-372): off = dielectrics at n(550 nm)."""
         check(lib.sc_tracer_set_spectral(self.h, 1 if on else 0))
 
+    def set_rows(self, row_begin, row_end):
+        """Trace only rows [row_begin, row_end) in later accumulate calls."""
+        check(lib.sc_tracer_set_rows(self.h, int(row_begin), int(row_end)))
+
     def clear_accum(self):
         check(lib.sc_tracer_clear_accum(self.h))
 

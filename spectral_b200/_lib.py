@@ -116,6 +116,7 @@ PROTOTYPES = {
     "sc_glass_n": (_f32, [_u32, _f32]),
     "sc_camera_proj_params": (_i32, [_vp, P(_f32)]),
     "sc_tracer_set_spectral": (_i32, [_vp, _i32]),
+    "sc_tracer_set_rows": (_i32, [_vp, _u32, _u32]),
     "sc_atomic_film_auto_expose_accum": (_i32, [_vp, _f32, P(_f32)]),
     "sc_atomic_film_to_rgb8": (_i32, [_vp, _f32, P(C.c_uint8)]),
     "sc_glass_n_many": (_i32, [_u32, P(_f32), C.c_size_t, P(_f32)]),

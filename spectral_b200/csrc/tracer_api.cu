@@ -22,6 +22,7 @@ struct sc_tracer {
     cudaEvent_t fork = nullptr, join = nullptr;
     std::mutex mu;
     uint32_t w = 0, h = 0, samples = 0;
+    uint32_t row0 = 0, row1 = 0;  // rows traced by accumulate (all by default)
     TracerParams hp{};
     DevBuf<TracerParams> params;
     DevBuf<float> tables;
@@ -77,9 +78,9 @@ struct sc_tracer {
         return SC_OK;
     }
     int run(uint32_t spp) {
-        const uint32_t npx = w * h;
+        const uint32_t px0 = row0 * w, px1 = row1 * w, npx = px1 - px0;
         const uint32_t px_per_wave = std::max(1u, kWavePaths / spp);
-        int rc = ensure_queues(std::min(npx, px_per_wave) * spp);
+        int rc = ensure_queues(std::max(1u, std::min(npx, px_per_wave)) * spp);
         if (rc != SC_OK) return rc;
         for (uint32_t c = 0; c < kChains; ++c) L[c].spp = spp;
         SC_CUDA(cudaMemcpyAsync(base.p, &samples, 4, cudaMemcpyHostToDevice, stream));
@@ -91,9 +92,9 @@ struct sc_tracer {
             cudaError_t e = cudaEventRecord(fork, stream);
             if (e == cudaSuccess) e = cudaStreamWaitEvent(stream2, fork, 0);
             uint32_t wave = 0;
-            for (uint32_t first = 0; first < npx && e == cudaSuccess; first += px_per_wave, ++wave) {
+            for (uint32_t first = px0; first < px1 && e == cudaSuccess; first += px_per_wave, ++wave) {
                 const uint32_t c = wave % kChains;
-                e = launch_tracer_wave(params.p, L[c], first, std::min(px_per_wave, npx - first),
+                e = launch_tracer_wave(params.p, L[c], first, std::min(px_per_wave, px1 - first),
                                        c ? stream2 : stream);
             }
             if (e == cudaSuccess) e = cudaEventRecord(join, stream2);
@@ -176,6 +177,7 @@ int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, c
     if (n_mats) cudaMemcpy(t->mats.p, mats, n_mats * sizeof(sc_material), cudaMemcpyHostToDevice);
     cudaMemset(t->sum.p, 0, t->sum.bytes());
     cudaMemset(t->segments.p, 0, 8);
+    t->row0 = 0; t->row1 = height;
     TracerParams& hp = t->hp;
     hp.cam = *cam; hp.width = width; hp.height = height; hp.seed = seed; hp.illuminant = illuminant;
     hp.background = background; hp.horizon = horizon; hp.has_horizon = has_horizon ? 1u : 0u;
@@ -251,6 +253,20 @@ int sc_tracer_set_camera(sc_tracer* t, const sc_camera* cam) {
     SC_REQUIRE(cam, SC_E_INVALID, "null camera");
     t->hp.cam = *cam;
     return t->upload_params();
+    SC_GUARD_END
+}
+
+int sc_tracer_set_rows(sc_tracer* t, uint32_t row_begin, uint32_t row_end) {
+    SC_GUARD_BEGIN
+    TR_LOCK(t);
+    SC_REQUIRE(row_begin <= row_end && row_end <= t->h, SC_E_INVALID, "rows [%u, %u) outside [0, %u)", row_begin,
+               row_end, t->h);
+    if (row_begin != t->row0 || row_end != t->row1) {
+        t->row0 = row_begin;
+        t->row1 = row_end;
+        t->drop_graph();  // the captured waves cover the old rows
+    }
+    return SC_OK;
     SC_GUARD_END
 }
 

@@ -8,8 +8,15 @@ films over NCCL (NVLink / NVSwitch) gives the film of the whole range,
 bit-identical to a single-GPU trace and independent of the number of ranks or
 the reduction order.  Batches and serving shard by whole scenes / requests and
 need no collective at all.
+
+The camera tracer shards by pixels instead: each rank owns a contiguous band
+of image rows (a pixel's samples are keyed by the pixel and sample index, so
+a row renders the same on any rank), traces only that band, and the bands are
+gathered into the full image.  Every pixel has one owner: no reduction.
 """
 import ctypes as C
+
+import numpy as np
 
 from ._lib import check, lib
 
@@ -48,6 +55,44 @@ def allreduce_film_(tensor, group=None):
         raise TypeError("films are int64 fixed point; a float all-reduce would not be exact")
     dist.all_reduce(tensor, op=dist.ReduceOp.SUM, group=group)
     return tensor
+
+
+def row_band(rank, world, height):
+    """Contiguous [begin, end) of image rows owned by `rank`."""
+    return photon_range(rank, world, height)
+
+
+def gather_bands(band, rank, world, height, group=None, device="cpu"):
+    """All-gather every rank's band of rows (band: rows x width x 3 float32, the
+    rows row_band(rank, world, height)) into the full image on every rank."""
+    import torch
+    import torch.distributed as dist
+    band = np.ascontiguousarray(band, dtype=np.float32)
+    width = band.shape[1]
+    rows = max(e - b for b, e in (row_band(r, world, height) for r in range(world)))
+    pad = torch.zeros((rows, width, 3), dtype=torch.float32, device=device)
+    pad[: band.shape[0]] = torch.from_numpy(band).to(device)
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad, group=group)
+    out = np.empty((height, width, 3), np.float32)
+    for r, t in enumerate(parts):
+        b, e = row_band(r, world, height)
+        out[b:e] = t[: e - b].cpu().numpy()
+    return out
+
+
+def trace_rows_sharded(tracer, spp, group=None):
+    """Accumulate spp samples of this rank's band of rows on its GPU, then gather
+    the bands: every rank returns the full mean XYZ image (height x width x 3)."""
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    w, h = tracer.dims()
+    b, e = row_band(rank, world, h)
+    tracer.set_rows(b, e)
+    tracer.accumulate(spp)
+    img = tracer.read_xyz().reshape(h, w, 3)
+    device = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    return gather_bands(img[b:e], rank, world, h, group, device)
 
 
 def trace_sharded(film, n_photons, seed, group=None):

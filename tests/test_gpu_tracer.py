@@ -12,6 +12,7 @@ import pytest
 
 import oracle
 import spectral_b200 as sb
+from spectral_b200 import _lib
 
 from helpers import axis_box, ocam, oscene
 
@@ -120,6 +121,31 @@ def test_set_spectral_off_uses_n550_bit_identical(ctx):
     assert on.tobytes() != off.tobytes()
     cpu_on = oracle.tracer_accumulate(oscene(s), ocam(cam), 80, 56, 0, 21, 8) / np.float32(8)  # cleared: from 0
     assert on.tobytes() == cpu_on.tobytes()
+
+
+def test_row_bands_render_like_the_full_image(ctx):
+    """set_rows (the camera tracer's pixel-row ownership for multi-GPU): a band
+    traced alone equals the same rows of the full render bit for bit, rows
+    outside it stay empty, and an empty band traces nothing."""
+    s = sb.Scene(background=1.0, horizon=2.0)
+    s.add_sphere((0, 0, -3), 1.0, sb.Dielectric(sb.SF11))
+    cam = sb.Camera.look_at((0, 0.3, 0.5), (0, 0, -3), (0, 1, 0), 55.0, 1.5)
+    w, h = 64, 41
+    full = sb.GpuTracer(ctx, s, cam, w, h, sb.D65, 9)
+    full.accumulate(8)
+    full.accumulate(4)
+    ref = full.read_xyz().reshape(h, w, 3)
+    for b, e in ((0, 13), (13, 41), (20, 20)):
+        t = sb.GpuTracer(ctx, s, cam, w, h, sb.D65, 9)
+        t.set_rows(b, e)
+        t.accumulate(8)
+        t.accumulate(4)
+        img = t.read_xyz().reshape(h, w, 3)
+        assert img[b:e].tobytes() == ref[b:e].tobytes(), (b, e)
+        assert not img[:b].any() and not img[e:].any()
+        t.close()
+    with pytest.raises(_lib.SpectralError):
+        full.set_rows(5, h + 1)
 
 
 def test_background_integrates_to_d65_and_illuminant_a(ctx):

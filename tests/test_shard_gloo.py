@@ -1,6 +1,7 @@
 """Multi-process path on CPU (gloo, world size 2): photon-range sharding plus the
 exact int64 film all-reduce reproduce the single-process film bit for bit.
 The per-rank films come from the CPU oracle standing in for each rank's GPU."""
+import ctypes as C
 import os
 import socket
 
@@ -10,7 +11,7 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from spectral_b200.shard import allreduce_film_, photon_range
+from spectral_b200.shard import allreduce_film_, gather_bands, photon_range, row_band
 
 
 def _free_port():
@@ -44,6 +45,56 @@ def _worker(rank, world, port, n, out_path):
         np.save(out_path, t.numpy())
     dist.barrier()
     dist.destroy_process_group()
+
+
+def _tracer_scene():
+    import oracle
+    from helpers import ocam, oscene
+    import spectral_b200 as sb
+    s = sb.Scene(background=1.0)
+    s.add_sphere((0, 0, -3), 1.0, sb.Dielectric(sb.SF11))
+    cam = sb.Camera.look_at((0, 0.3, 0.5), (0, 0, -3), (0, 1, 0), 55.0, 1.5)
+    return oracle, oscene(s), ocam(cam)
+
+
+def _tracer_worker(rank, world, port, w, h, spp, out_path):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    oracle, osc, oc = _tracer_scene()
+    b, e = row_band(rank, world, h)
+    acc = np.zeros(3 * w * h, np.float32)
+    oracle.lib.or_tracer_accumulate(C.byref(osc.c), C.byref(oc), w, h, 0, 5, spp, 0, 8, b, e, oracle.fp(acc))
+    img = (acc / np.float32(spp)).reshape(h, w, 3)
+    full = gather_bands(img[b:e], rank, world, h)
+    np.save(out_path % rank, full)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_tracer_row_bands_gather_to_the_full_image(tmp_path, world):
+    """Pixel-row ownership for the camera tracer: each rank renders its band of
+    rows (the CPU oracle standing in for its GPU) and the gathered image equals
+    the single-process render bit for bit on every rank."""
+    w, h, spp = 24, 17, 4
+    out = str(tmp_path / "img%d.npy")
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_tracer_worker, args=(r, world, port, w, h, spp, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    oracle, osc, oc = _tracer_scene()
+    whole = np.zeros(3 * w * h, np.float32)
+    oracle.lib.or_tracer_accumulate(C.byref(osc.c), C.byref(oc), w, h, 0, 5, spp, 0, 8, 0, h, oracle.fp(whole))
+    whole = (whole / np.float32(spp)).reshape(h, w, 3)
+    assert whole.sum() > 0
+    for r in range(world):
+        assert np.load(out % r).tobytes() == whole.tobytes(), r
 
 
 def test_photon_range_partitions():
