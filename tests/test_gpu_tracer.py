@@ -14,7 +14,7 @@ import oracle
 import spectral_b200 as sb
 from spectral_b200 import _lib
 
-from helpers import axis_box, ocam, oscene
+from helpers import axis_box, ocam, oscene, triangular_prism
 
 pytestmark = pytest.mark.gpu
 
@@ -146,6 +146,32 @@ def test_row_bands_render_like_the_full_image(ctx):
         t.close()
     with pytest.raises(_lib.SpectralError):
         full.set_rows(5, h + 1)
+
+
+def _chroma_spread(img):
+    """Largest chromaticity distance from the D65 white point over the pixels
+    (core/tests/scene_a_prism.rs:51-65)."""
+    px = img.reshape(-1, 3).astype(np.float32)
+    s = px.sum(1)
+    m = s > 1e-5
+    x, y = px[m, 0] / s[m], px[m, 1] / s[m]
+    return float(np.sqrt((x - 0.3127) ** 2 + (y - 0.3290) ** 2).max()) if m.any() else 0.0
+
+
+def test_dispersive_prism_colors_horizon_more_than_diffuse(ctx):
+    """core/tests/scene_a_prism.rs:67-90 on the GPU tracer: an SF11 prism in
+    front of a bright horizon colours the image far more than a Lambertian prism
+    of the same shape (128x128, 256 spp, seed 11)."""
+    def render(mat):
+        s = sb.Scene(background=0.3, horizon=4.0)
+        s.add_solid(triangular_prism(1.0, 2.0), mat)
+        cam = sb.Camera.look_at((0.0, 0.0, 4.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 50.0, 1.0)
+        t = sb.GpuTracer(ctx, s, cam, 128, 128, sb.D65, 11)
+        t.accumulate(256)
+        return t.read_xyz()
+    cg = _chroma_spread(render(sb.Dielectric(sb.SF11)))
+    cd = _chroma_spread(render(sb.Lambertian(0.8)))
+    assert cg > 0.05 and cg > 2.0 * cd, (cg, cd)
 
 
 def test_background_integrates_to_d65_and_illuminant_a(ctx):

@@ -164,6 +164,26 @@ def test_refract_matches_snell_angle():
         assert abs(got - math.asin(math.sin(th) / 1.5)) < 1e-5 and abs(t[2]) < 1e-6
 
 
+# ---- core/tests/scene_a_prism.rs:18-47 (analytic gate) ------------------------
+def _bk7_deviation(d, lam):
+    t = refract(d, [0, 1, 0], 1.0, O.or_glass_n(0, lam))
+    c = float(np.clip(np.dot(d.astype(np.float64), t.astype(np.float64)), -1.0, 1.0))
+    return math.acos(c)
+
+
+def test_prism_interface_blue_deviates_more_than_red():
+    d = unit([0.5, -0.8660254, 0.0])  # 30 deg incidence
+    assert _bk7_deviation(d, 450.0) > _bk7_deviation(d, 650.0)
+
+
+def test_prism_interface_spread_matches_analytic():
+    th = math.radians(30.0)
+    d = unit([math.sin(th), -math.cos(th), 0.0])
+    for lam in (440.0, 520.0, 600.0, 680.0):
+        analytic = th - math.asin(math.sin(th) / O.or_glass_n(0, lam))
+        assert abs(_bk7_deviation(d, lam) - analytic) / analytic < 0.03, lam
+
+
 def test_transmitted_ray_forward_and_tangential_sense():
     th = math.radians(50.0)
     d = unit([math.sin(th), -math.cos(th), 0])
