@@ -597,8 +597,9 @@ def run_gpu_tracer(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": C.sizeof(cam.c),
                 "d2h_bytes_per_step": 3 * W * H * 4,
                 "path": "sc_tracer_set_camera + clear_accum + accumulate(64) + read_xyz (host f32 XYZ)"},
-        # per wave: generate, 2 compacted bounces (intersect + shade), the tail, per-pixel sums
-        "gpu_launches": args.steps * waves * (2 + 2 * min(kw["max_depth"], 2) + (1 if kw["max_depth"] > 2 else 0)),
+        # per wave: primary rays made and intersected, its shade, the second bounce
+        # (intersect + shade), the tail, per-pixel sums
+        "gpu_launches": args.steps * waves * (1 + 2 * min(kw["max_depth"], 2) + (1 if kw["max_depth"] > 2 else 0)),
         "kernels": {"accumulate_ms": statistics.mean(step_ms)},
         "roofline": {"bound": "hbm", "achieved": qbytes / step_s / 1e9, "peak": hbm, "unit": "GB/s",
                      "frac": qbytes / step_s / 1e9 / hbm, "traffic": ncu_traffic("tracer")[0],

@@ -191,6 +191,45 @@ __global__ void __launch_bounds__(256) tr_intersect(const TracerParams* __restri
     }
 }
 
+// Bounce 0 without a ray queue round trip: each path's primary ray is made as
+// tr_generate makes it, intersected at once, and queued with its hit for the
+// first shade (persistent grid, scene in shared memory).
+__global__ void __launch_bounds__(256) tr_primary(const TracerParams* __restrict__ gp, uint32_t first_pixel,
+                                                  uint32_t n_pixels, uint32_t n_paths,
+                                                  const uint32_t* __restrict__ base, RayQueue q, uint32_t* counts,
+                                                  HitQueue hq, float* result) {
+    __shared__ TracerSmem s;
+    extern __shared__ __align__(16) unsigned char dyn[];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counts[0] = n_paths;
+        for (uint32_t b = 1; b <= gp->max_depth; ++b) counts[b] = 0u;
+    }
+    if (blockIdx.x * blockDim.x >= n_paths) return;
+    const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
+    const uint32_t W = s.p.width, H = s.p.height, b0 = *base;
+    const f3 org = ld3(s.p.cam.origin);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_paths; i += gridDim.x * blockDim.x) {
+        const uint32_t smp = i / n_pixels, pixel = first_pixel + (i - smp * n_pixels);
+        const uint32_t px = pixel % W, py = pixel / W;
+        Rng r = Rng::make(mix2(pixel, b0 + smp), s.p.seed);
+        const float fs = ((float)px + r.f32()) / (float)W;
+        const float ft = 1.0f - ((float)py + r.f32()) / (float)H;
+        const float u = r.f32();
+        const f3 d = primary_dir(s.p.cam, fs, ft);
+        q.ox[i] = org.x; q.oy[i] = org.y; q.oz[i] = org.z;
+        q.dx[i] = d.x; q.dy[i] = d.y; q.dz[i] = d.z;
+        q.rng[i] = r.state; q.tp[i] = 1.0f; q.u[i] = u; q.id[i] = i; q.flags[i] = 4u;
+        result[3 * i] = 0.0f; result[3 * i + 1] = 0.0f; result[3 * i + 2] = 0.0f;
+        float t;
+        f3 nrm;
+        uint32_t info;
+        trace_hit(s, S, org, d, t, nrm, info);
+        hq.t[i] = t;
+        if ((info >> 24) == 1u) { hq.nx[i] = nrm.x; hq.ny[i] = nrm.y; hq.nz[i] = nrm.z; }
+        hq.info[i] = info;
+    }
+}
+
 __global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __restrict__ gp, uint32_t bounce,
                                                           RayQueue q, HitQueue hq, RayQueue out, uint32_t* counts,
                                                           float* result) {
@@ -321,16 +360,22 @@ int tracer_grid(int sms) {
 cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch& L, uint32_t first_pixel,
                                uint32_t n_pixels, cudaStream_t st) {
     const uint32_t n_paths = n_pixels * L.spp;
-    tr_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(d_params, first_pixel, n_pixels, n_paths, L.d_base, L.qa,
-                                                       L.counts, L.result);
     const size_t dyn = tracer_dyn_smem(L.n_planes);
-    // wavefront with compaction for the first bounces, then the tail in place
+    // wavefront with compaction for the first bounces, then the tail in place;
+    // bounce 0 makes and intersects the primary rays in one kernel
     const uint32_t wave_bounces = L.max_depth < kWaveBounces ? L.max_depth : kWaveBounces;
+    if (wave_bounces == 0)
+        tr_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(d_params, first_pixel, n_pixels, n_paths, L.d_base,
+                                                           L.qa, L.counts, L.result);
     for (uint32_t b = 0; b < wave_bounces; ++b) {
         const RayQueue& in = (b & 1u) ? L.qb : L.qa;
         const RayQueue& out = (b & 1u) ? L.qa : L.qb;
         uint32_t g = L.grid;
-        tr_intersect<<<g, 256, dyn, st>>>(d_params, b, in, L.counts, L.hits);
+        if (b == 0)
+            tr_primary<<<g, 256, dyn, st>>>(d_params, first_pixel, n_pixels, n_paths, L.d_base, in, L.counts, L.hits,
+                                            L.result);
+        else
+            tr_intersect<<<g, 256, dyn, st>>>(d_params, b, in, L.counts, L.hits);
         tr_shade<<<g, kShadeThreads, dyn, st>>>(d_params, b, in, L.hits, out, L.counts, L.result);
     }
     if (L.max_depth > wave_bounces)
