@@ -71,7 +71,7 @@ NCU_TRAFFIC = {
     "prism": (2092544, "photon_kernel"),
     "rainbow": (4839725056, "order_count + order_scan + order_scatter + photon_kernel"),
     "beam": (3842560, "beam_kernel"),
-    "tracer": (10152085504, "all tracer wave kernels of one accumulate(64)"),
+    "tracer": (8738738944, "all tracer wave kernels of one accumulate(64)"),
     "batch": (4566429952, "batch_kernel + reduce_scan + reduce_list"),
     "atomics": (24887296, "synthetic_splat_kernel"),
 }
