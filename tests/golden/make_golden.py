@@ -1,6 +1,7 @@
 """Regenerate the committed golden fixtures in this directory from the CPU oracle.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # all fixtures
+    python tests/golden/make_golden.py --extra    # the beam and tracer fixtures only
 
 * rng_draws.json: 16 draws of PathRng(0xABCD, 0x1234) (the stream of
   spectral-gpu/tests/rng_parity.rs; its first four are the reference's frozen
@@ -10,6 +11,11 @@
   (spectral-gpu/src/vol_photons.rs:1280-1414).
 * dsotm_film_64.npz: the 64x64 XYZ fixed-point film (scale 2^32) of 4096 DSOTM
   photons, seed 7, DSOTM weights (spectral-gpu/src/vol_photons.rs:1425-1458).
+* beam_film_48x40.npz: the photon-beam estimator image (render_volumetric_scene,
+  spectral-core/src/volume.rs:233-329) of 600 DSOTM photons, seed 3, 48x40.
+* tracer_glass_32x24.npz: the camera tracer's mean XYZ image (CpuTracer,
+  spectral-core/src/tracer.rs:44-141) of two dielectric spheres under a
+  horizon, 32x24, 8 spp, seed 77, D65.
 """
 import json
 import os
@@ -50,6 +56,30 @@ def dsotm():
     return scene, beam, tir
 
 
+def glass_spheres():
+    """SF11 sphere r=1 at (0, 0, -3) and water sphere r=0.7 at (1.8, 0.5, -4),
+    background 1, horizon 2; camera at (0, 0.3, 0.5) looking at (0, 0, -3)."""
+    from oracle import F3
+    prims = bytes(oracle.or_prim(F3(0, 0, -3), 1.0, 0, 0, 0, 0)) + bytes(oracle.or_prim(F3(1.8, 0.5, -4), 0.7, 0, 0, 0, 1))
+    mats = bytes(oracle.or_mat(0.0, 1, 1, 0)) + bytes(oracle.or_mat(0.0, 2, 1, 0))
+    scene = oracle.OScene(prims, 2, b"", 0, mats, 2, 1.0, 2.0)
+    cam = oracle.camera_look_at((0.0, 0.3, 0.5), (0.0, 0.0, -3.0), (0, 1, 0), 55.0, 32.0 / 24.0)
+    return scene, cam
+
+
+def extra_fixtures():
+    """The beam-estimator and camera-tracer fixtures (written by themselves so
+    that the older fixtures are not rewritten)."""
+    scene, beam, _ = dsotm()
+    cam = oracle.camera_look_at((0.5, -0.5, 12.0), (0.5, -0.5, 0.0), (0, 1, 0), 42.0, 48.0 / 40.0)
+    p = oracle.vol_params(48, 40, 3, 0.5, 0.06, 0.5, 14.0)
+    img = oracle.render_beam(scene, cam, beam, p, 0, 600)
+    np.savez_compressed(os.path.join(HERE, "beam_film_48x40.npz"), img_f32=img)
+    gs, gcam = glass_spheres()
+    acc = oracle.tracer_accumulate(gs, gcam, 32, 24, 0, 77, 8)
+    np.savez_compressed(os.path.join(HERE, "tracer_glass_32x24.npz"), mean_xyz=acc / np.float32(8))
+
+
 def main():
     out = {}
     d = (C.c_uint32 * 16)()
@@ -80,8 +110,12 @@ def main():
     p = oracle.vol_params(64, 64, 7, 0.5, 0.06, 0.5, 14.0)
     img, fx, _ = oracle.render_point(scene, cam, beam, p, 0, 4096)
     np.savez_compressed(os.path.join(HERE, "dsotm_film_64.npz"), film_xyz=fx, img_f32=img)
+    extra_fixtures()
     print("wrote golden fixtures to", HERE)
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["--extra"]:
+        extra_fixtures()
+    else:
+        main()

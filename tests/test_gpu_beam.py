@@ -1,5 +1,7 @@
 """Photon-beam estimator (render_volumetric_scene + splat_transverse,
 spectral-core/src/volume.rs:170-329) on the GPU against the oracle."""
+import os
+
 import numpy as np
 import pytest
 
@@ -33,6 +35,15 @@ def test_beam_dsotm_matches_oracle(ctx, w, h, n, seed):
     got = f.accum()
     assert exp.sum() > 0
     assert rel_l1(got, exp) < BEAM_TOL
+
+
+def test_beam_film_against_golden_fixture(ctx):
+    """The committed beam-estimator fixture (tests/golden/make_golden.py:
+    600 DSOTM photons, seed 3, 48x40)."""
+    scene, beam, cam = sb.dsotm_scene(48 / 40)
+    f = beam_film(ctx, scene, cam, beam, 48, 40, 600, 3)
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "beam_film_48x40.npz"))["img_f32"]
+    assert g.sum() > 0 and rel_l1(f.accum(), g) < BEAM_TOL
 
 
 def test_beam_empty_scene_energy_matches_point_estimator(ctx):

@@ -7,6 +7,8 @@ required to be bit-identical.  Lambertian sampling calls cosf/sinf, whose last
 bits differ between CUDA and glibc, so those scenes use the reference's
 statistical gates (frac of pixels above 10x the mean difference, p99, energy).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -172,6 +174,19 @@ def test_dispersive_prism_colors_horizon_more_than_diffuse(ctx):
     cg = _chroma_spread(render(sb.Dielectric(sb.SF11)))
     cd = _chroma_spread(render(sb.Lambertian(0.8)))
     assert cg > 0.05 and cg > 2.0 * cd, (cg, cd)
+
+
+def test_tracer_against_golden_fixture(ctx):
+    """The committed camera-tracer fixture (tests/golden/make_golden.py: SF11 and
+    water spheres under a horizon, 32x24, 8 spp, seed 77): bit-identical."""
+    s = sb.Scene(background=1.0, horizon=2.0)
+    s.add_sphere((0.0, 0.0, -3.0), 1.0, sb.Dielectric(sb.SF11))
+    s.add_sphere((1.8, 0.5, -4.0), 0.7, sb.Dielectric(sb.WATER))
+    cam = sb.Camera.look_at((0.0, 0.3, 0.5), (0.0, 0.0, -3.0), (0.0, 1.0, 0.0), 55.0, 32.0 / 24.0)
+    t = sb.GpuTracer(ctx, s, cam, 32, 24, sb.D65, 77)
+    t.accumulate(8)
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "tracer_glass_32x24.npz"))["mean_xyz"]
+    assert t.read_xyz().tobytes() == g.tobytes()
 
 
 def test_background_integrates_to_d65_and_illuminant_a(ctx):

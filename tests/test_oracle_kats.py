@@ -528,3 +528,20 @@ def test_synthetic_splat_deterministic_and_nonzero():
     O.or_synthetic_splat(32, 32, 0xDEADBEEF, 4096, a.ctypes.data_as(C.POINTER(C.c_uint32)))
     O.or_synthetic_splat(32, 32, 0xDEADBEEF, 4096, b.ctypes.data_as(C.POINTER(C.c_uint32)))
     assert (a == b).all() and (a > 0).any()
+
+
+# ---- committed fixtures of the beam estimator and the camera tracer ----------
+def test_oracle_reproduces_beam_and_tracer_fixtures():
+    import importlib.util
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(here, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    scene, beam, _ = mg.dsotm()
+    cam = oracle.camera_look_at((0.5, -0.5, 12.0), (0.5, -0.5, 0.0), (0, 1, 0), 42.0, 1.2)
+    img = oracle.render_beam(scene, cam, beam, oracle.vol_params(48, 40, 3, 0.5, 0.06, 0.5, 14.0), 0, 600)
+    assert img.tobytes() == np.load(os.path.join(here, "beam_film_48x40.npz"))["img_f32"].tobytes()
+    gs, gcam = mg.glass_spheres()
+    acc = oracle.tracer_accumulate(gs, gcam, 32, 24, 0, 77, 8) / np.float32(8)
+    assert acc.tobytes() == np.load(os.path.join(here, "tracer_glass_32x24.npz"))["mean_xyz"].tobytes()
