@@ -79,6 +79,7 @@ for name, res, args in [
     ("or_glass_n", _f32, [_u32, _f32]),
     ("or_glass_n_many", None, [_u32, P(_f32), C.c_size_t, P(_f32)]),
     ("or_tracer_set_spectral", None, [C.c_int]),
+    ("or_set_fault", None, [C.c_int]),
     ("or_camera_proj_params", None, [C.c_void_p, P(_f32)]),
     ("or_load_tables_csv", _i32, [C.c_char_p]),
     ("or_get_tables", None, [P(_f32)]),

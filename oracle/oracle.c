@@ -32,11 +32,18 @@ static inline v3 cross(v3 a, v3 b) {
     return V(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
 }
 
+/* Planted faults (0 = none), set only by the test that checks that the parity
+ * gates catch a wrong restatement: 1 PCG multiplier, 2 Sellmeier index off by
+ * 2e-4, 3 Fresnel without its p term, 4 haze weight without the 1/4, 5 HG
+ * phase with g negated. */
+static int g_fault = 0;
+void or_set_fault(int fault) { g_fault = fault; }
+
 /* ------------------------------------------------------------------------ */
 /* rng.rs:7-40                                                               */
 /* ------------------------------------------------------------------------ */
 uint32_t or_pcg32(uint32_t input) {
-    uint32_t state = input * 747796405u + 2891336453u;
+    uint32_t state = input * (g_fault == 1 ? 747796403u : 747796405u) + 2891336453u;
     uint32_t word = ((state >> ((state >> 28) + 4u)) ^ state) * 277803737u;
     return (word >> 22) ^ word;
 }
@@ -58,7 +65,12 @@ void or_rng_draws_f32(uint32_t key, uint32_t seed, uint32_t n, float* out) {
 /* sellmeier.rs:13-44.  Glass ids: 0 BK7, 1 SF11, 2 water (Cauchy), 3 fused   */
 /* silica (Malitson 1965 Sellmeier; not in the reference crate).             */
 /* ------------------------------------------------------------------------ */
+static float glass_n_ref(uint32_t glass, float nm);
 float or_glass_n(uint32_t glass, float nm) {
+    const float n = glass_n_ref(glass, nm);
+    return g_fault == 2 ? n + 2e-4f : n;
+}
+static float glass_n_ref(uint32_t glass, float nm) {
     double l_um = (double)nm / 1000.0;
     if (glass == 2u) return (float)(1.3238 + 0.00314 / (l_um * l_um));
     double l2 = l_um * l_um;
@@ -179,7 +191,7 @@ static inline float fresnel(float cos_i, float n1, float n2) {
     float cos_t = sqrtf(1.0f - sin_t2);
     float rs = (n1 * cos_i - n2 * cos_t) / (n1 * cos_i + n2 * cos_t);
     float rp = (n1 * cos_t - n2 * cos_i) / (n1 * cos_t + n2 * cos_i);
-    return 0.5f * (rs * rs + rp * rp);
+    return g_fault == 3 ? 0.5f * (rs * rs) : 0.5f * (rs * rs + rp * rp);
 }
 void or_reflect(const float d[3], const float n[3], float out[3]) { S(out, reflect3(L(d), L(n))); }
 int or_refract(const float d[3], const float n[3], float n1, float n2, float out[3]) {
@@ -347,6 +359,7 @@ int or_camera_project(const or_camera* c, const float p[3], float out[3]) {
 /* volume.rs                                                                 */
 /* ------------------------------------------------------------------------ */
 float or_phase_hg(float g, float cos_theta) { /* volume.rs:88-92 */
+    if (g_fault == 5) g = -g;
     float g2 = g * g;
     float denom = powf(fmaxf(1.0f + g2 - 2.0f * g * cos_theta, 1e-6f), 1.5f);
     return (1.0f - g2) / (4.0f * 3.14159265358979323846f * denom);
@@ -435,7 +448,7 @@ void or_render_point(const or_scene* sc, const or_camera* cam, const or_beam* be
                     float cos_t = dot(d, vdiv(to, dd));
                     float phase = or_phase_hg(p->g, cos_t);
                     float trans = expf(-p->sigma_t * dd);
-                    contrib = power * p->sigma_s * phase * trans / (dd * dd) * seg / 4.0f;
+                    contrib = power * p->sigma_s * phase * trans / (dd * dd) * seg / (g_fault == 4 ? 1.0f : 4.0f);
                 } else {
                     contrib = power * p->sigma_s * seg / 4.0f * inv_4pi;
                 }

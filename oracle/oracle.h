@@ -57,6 +57,8 @@ void or_rng_draws_f32(uint32_t key, uint32_t seed, uint32_t n, float* out);
 
 /* sellmeier.rs (+ fused silica, glass id 3) */
 float or_glass_n(uint32_t glass, float nm);
+/* Planted faults for the gate-sensitivity test only (0 = none; see oracle.c). */
+void or_set_fault(int fault);
 /* or_glass_n of every element of nm[0..n). */
 void or_glass_n_many(uint32_t glass, const float* nm, size_t n, float* out);
 
