@@ -1,0 +1,44 @@
+"""bench.py's output contract, checked on CPU: the reference arm (the CPU
+restatement on the host cores) prints one JSON line with the keys the bench
+contract names, and the GPU arm without a GPU fails instead of falling back to
+a CPU path."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _run(*args):
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], capture_output=True, text=True,
+                          cwd=ROOT, timeout=600)
+
+
+@pytest.mark.parametrize("workload", ["prism", "tracer"])
+def test_reference_arm_prints_one_contract_line(workload):
+    r = _run("--impl", "reference", "--workload", workload, "--steps", "1", "--warmup", "1", "--cpu-seconds", "0.5")
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.strip().startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["n_gpus"] == 1 and d["steps"] == 1
+    assert d["higher_is_better"] is True and d["vs_baseline"] is None and "workload" in d["config"]
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
+    e = d["e2e"]
+    assert e["value"] == d["value"] and e["unit"] == d["unit"]
+    assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+
+
+def test_gpu_arm_without_a_gpu_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    r = _run("--workload", "prism", "--steps", "1", "--warmup", "1", "--no-cpu-baseline")
+    assert r.returncode != 0 and not any(ln.startswith("{") for ln in r.stdout.splitlines())
