@@ -42,11 +42,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    # SF11 prism (apex 60, side 1), 0.02 beam at 45 deg, 2^20
+    # Plain prism pass: SF11 prism (apex 60, side 1), 0.02 beam at 45 deg, 2^20
     # photons, lambda U(380, 780), sigma_s 0.05, sigma_a 0, isotropic, 640x360x64.
     "prism": dict(width=640, height=360, bins=64, photons=1 << 20, sigma_s=0.05, sigma_t=0.05, g=0.0,
                   lambda_min=380.0, lambda_max=780.0, max_dist=6.0, max_bounces=8, seed=0xDED),
-    # water sphere r=1, beam width 2.2, 2^26 photons, up to 4
+    # Rainbow: water sphere r=1, beam width 2.2, 2^26 photons, up to 4
     # internal bounces (6 surface interactions), sigma_s 0.02, 1920x1080x64.
     "rainbow": dict(width=1920, height=1080, bins=64, photons=1 << 26, sigma_s=0.02, sigma_t=0.02, g=0.0,
                     lambda_min=380.0, lambda_max=780.0, max_dist=8.0, max_bounces=6, seed=0x8A1B),
@@ -452,7 +452,7 @@ def run_gpu(args, rank, world, local_rank):
     return line
 
 
-# Camera-tracer workload (config 2): SF11 prism on a diffuse ground plane,
+# Camera-tracer workload: SF11 prism on a diffuse ground plane,
 # spherical D65 emitter r=0.2 at (2,3,1), 1280x720, 64 spp per step, hero comb
 # of 4 wavelengths, depth 8, Russian roulette after bounce 3.
 TRACER = dict(width=1280, height=720, spp=64, seed=0x7ACE)
@@ -718,8 +718,8 @@ def run_cpu_atomics(seconds):
     return 3 * n_cpu * done / dt, done, dt
 
 
-# Serving workload (config 5): Poisson arrivals at 200 req/s (a 15 s window of
-# the 60 s stream by default), prism scenes of the config-4 distribution,
+# Serving workload: Poisson arrivals at 200 req/s (a 15 s window of
+# the 60 s stream by default), prism scenes of the batch workload's distribution,
 # 2^16-2^20 photons per frame, 30 % orbit sessions of 16-128 frames at 2 deg
 # per frame, 40 GB HBM budget.
 SERVE = dict(rate=200.0, seconds=15.0, budget_gb=40.0, seed=0x5E7E)
