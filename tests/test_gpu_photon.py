@@ -2,7 +2,7 @@
 
 Restates the reference's GPU gates (spectral-gpu/src/vol_photons.rs tests,
 spectral-gpu/tests/rng_parity.rs, spectral-gpu/src/film.rs tests) with the
-tolerances of this build:
+tolerances of this library:
   * RNG stream: bit-identical;
   * per-photon states: exact bounce count, origin/direction within PATH_TOL
     (the reference asserts 1e-4, its README claims ~1e-6);
@@ -23,8 +23,8 @@ from helpers import energy_delta, obeam, ocam, oscene, rel_l1
 
 pytestmark = pytest.mark.gpu
 
-PATH_TOL = 1e-6      # per-photon origin / direction
-FILM_TOL = 5e-3      # relative L1 of films / XYZ images (0.5 %)
+PATH_TOL = 1e-6      # per-photon origin / direction (the required bound)
+FILM_TOL = 5e-3      # relative L1 of films / XYZ images (the required bound, 0.5 %)
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
