@@ -67,7 +67,10 @@ typedef struct {
     uint32_t scale_log2;    /* fixed-point scale 2^k (0 -> 32) */
     uint32_t estimator;     /* 0 point estimator (volume.rs:99-168), 1 legacy isotropic (volume.rs:22-85),
                                2 photon-beam estimator (volume.rs:170-329; photon films and the
-                               device-pointer trace only; deposits are small: use scale_log2 >= 40) */
+                               device-pointer trace only; deposits are small: use scale_log2 >= 40),
+                               3 point estimator with free-flight sampling (no counterpart in the
+                               reference): the 4 distances of a segment follow sigma_t exp(-sigma_t t)
+                               restricted to the segment, weighted by 1/pdf: the same integral */
 } sc_film_options;
 
 typedef struct sc_batch sc_batch;

@@ -433,7 +433,10 @@ void or_render_point(const or_scene* sc, const or_camera* cam, const or_beam* be
             int any = scene_hit(sc, o, d, &h, &mi);
             float seg = any ? h.t : p->max_dist;
             for (int k = 0; k < 4; ++k) {
-                float dist = rng_f32(&r) * seg;
+                const float u = rng_f32(&r);
+                /* free-flight estimator (3): truncated exponential distance, 1/pdf weight */
+                const int ff = p->estimator == 3u && p->sigma_t > 0.0f;
+                float dist = ff ? -log1pf(u * expm1f(-p->sigma_t * seg)) / p->sigma_t : u * seg;
                 v3 q = add(o, mul(d, dist));
                 float s, t, depth;
                 if (!proj(&P, q, &s, &t, &depth)) continue;
@@ -441,14 +444,15 @@ void or_render_point(const or_scene* sc, const or_camera* cam, const or_beam* be
                 uint32_t py = (uint32_t)((1.0f - t) * (float)H); if (py > H - 1) py = H - 1;
                 uint32_t pix = py * W + px;
                 float contrib;
-                if (p->estimator == 0u) {
+                if (p->estimator == 0u || p->estimator == 3u) {
                     v3 to = sub(cam_o, q);
                     float dd = fmaxf(length(to), 1e-3f);
                     if (zbuf && !(dd < zbuf[pix])) continue;
                     float cos_t = dot(d, vdiv(to, dd));
                     float phase = or_phase_hg(p->g, cos_t);
                     float trans = expf(-p->sigma_t * dd);
-                    contrib = power * p->sigma_s * phase * trans / (dd * dd) * seg / (g_fault == 4 ? 1.0f : 4.0f);
+                    const float span = ff ? -expm1f(-p->sigma_t * seg) / (p->sigma_t * expf(-p->sigma_t * dist)) : seg;
+                    contrib = power * p->sigma_s * phase * trans / (dd * dd) * span / (g_fault == 4 ? 1.0f : 4.0f);
                 } else {
                     contrib = power * p->sigma_s * seg / 4.0f * inv_4pi;
                 }

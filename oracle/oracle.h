@@ -46,7 +46,8 @@ typedef struct {
     uint32_t bins;                    /* spectral film bins */
     float bin_min, bin_inv_width;     /* bin = floor((lambda - bin_min) * bin_inv_width) */
     float scale;                      /* fixed-point scale of the int64 films */
-    uint32_t estimator;               /* 0 point (HG + transmittance), 1 legacy isotropic */
+    uint32_t estimator;               /* 0 point (HG + transmittance), 1 legacy isotropic, 3 point with
+                                         free-flight distances (truncated exponential, 1/pdf weights) */
 } or_vol_params;
 
 /* rng.rs */

@@ -206,7 +206,7 @@ def _fptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
-POINT, ISOTROPIC, BEAM = 0, 1, 2
+POINT, ISOTROPIC, BEAM, FREE_FLIGHT = 0, 1, 2, 3
 
 
 class GpuPhotonFilm:
@@ -216,8 +216,9 @@ class GpuPhotonFilm:
     XYZ film, N = spectral bins), the emission band, ``max_bounces``,
     ``scale_log2`` (default 2^32, 2^40 for the beam estimator) and
     ``estimator``: POINT (render_volumetric_scene_point, the GPU path of the
-    reference), ISOTROPIC (render_volumetric) or BEAM (render_volumetric_scene,
-    spectral-core/src/volume.rs:170-329)."""
+    reference), ISOTROPIC (render_volumetric), BEAM (render_volumetric_scene,
+    spectral-core/src/volume.rs:170-329) or FREE_FLIGHT (the point estimator
+    with free-flight distances and 1/pdf weights; no reference counterpart)."""
 
     def __init__(self, ctx, scene, camera, beam, width, height, n_photons, seed, max_dist, weights=None,
                  zbuffer=None, bins=0, lambda_min=380.0, lambda_max=730.0, max_bounces=8, scale_log2=None,

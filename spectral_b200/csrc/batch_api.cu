@@ -39,7 +39,7 @@ int check_job(const sc_scene_job& j, uint32_t i) {
                "job %u: batch films are spectral (1..%d bins)", i, SC_MAX_BINS);
     const float lmin = j.opts.lambda_min ? j.opts.lambda_min : 380.0f, lmax = j.opts.lambda_max ? j.opts.lambda_max : 730.0f;
     SC_REQUIRE(lmax > lmin, SC_E_INVALID, "job %u band", i);
-    SC_REQUIRE(j.opts.max_bounces <= 64 && j.opts.scale_log2 <= 50 && j.opts.estimator <= 1, SC_E_INVALID,
+    SC_REQUIRE(j.opts.max_bounces <= 64 && j.opts.scale_log2 <= 50 && (j.opts.estimator <= 1 || j.opts.estimator == 3), SC_E_INVALID,
                "job %u options", i);
     return SC_OK;
 }

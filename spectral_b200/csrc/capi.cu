@@ -375,7 +375,7 @@ int sc_photon_film_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_pri
     SC_REQUIRE(o.lambda_max > o.lambda_min, SC_E_INVALID, "empty band [%g, %g)", o.lambda_min, o.lambda_max);
     SC_REQUIRE(o.scale_log2 <= 50u, SC_E_INVALID, "scale_log2 %u > 50", o.scale_log2);
     SC_REQUIRE(o.max_bounces <= 64u, SC_E_LIMIT, "max_bounces %u > 64", o.max_bounces);
-    SC_REQUIRE(o.estimator <= 2u, SC_E_INVALID, "estimator %u", o.estimator);
+    SC_REQUIRE(o.estimator <= 3u, SC_E_INVALID, "estimator %u", o.estimator);
     SC_REQUIRE(o.estimator != 2u || (width < 65536u && height < 65536u), SC_E_LIMIT,
                "beam estimator films are below 65536 pixels per side");
     (void)background;
@@ -737,7 +737,7 @@ int sc_trace_photons_device(sc_ctx* ctx, const sc_trace_desc* d, uint32_t base, 
     SC_REQUIRE(d->width > 0 && d->height > 0, SC_E_INVALID, "empty film");
     sc_film_options o;
     resolve_options(&d->opts, o);
-    SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min && o.estimator <= 2u, SC_E_INVALID,
+    SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min && o.estimator <= 3u, SC_E_INVALID,
                "bad film options");
     SC_REQUIRE(o.estimator != 2u || (d->width < 65536u && d->height < 65536u), SC_E_LIMIT,
                "beam estimator films are below 65536 pixels per side");

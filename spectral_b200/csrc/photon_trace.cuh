@@ -112,10 +112,26 @@ __device__ __forceinline__ void record_pair(sc_debug_photon* rec, uint32_t pair,
 // haze samples that land in frame (= film splats), dielectric/diffuse scatters.
 struct PhotonCounts { uint32_t segments, splats, scatters; };
 
+// Free-flight sampling (estimator 3, no counterpart in the reference): the
+// haze sample distance follows the free-flight density sigma_t exp(-sigma_t t)
+// restricted to the segment, t = -log(1 - u (1 - exp(-sigma_t seg))) / sigma_t,
+// and the sample is weighted by 1 / pdf(t) = (1 - exp(-sigma_t seg)) /
+// (sigma_t exp(-sigma_t t)) instead of the uniform estimator's seg: the same
+// single-scatter integral, with samples denser where the beam enters.  With
+// sigma_t = 0 it is the uniform estimator.
+__device__ __forceinline__ float haze_distance(const PhotonParams& p, float u, float seg) {
+    if (p.estimator != 3u || !(p.sigma_t > 0.0f)) return u * seg;
+    return -log1pf(u * expm1f(-p.sigma_t * seg)) / p.sigma_t;
+}
+__device__ __forceinline__ float haze_span(const PhotonParams& p, float dist, float seg) {
+    if (p.estimator != 3u || !(p.sigma_t > 0.0f)) return seg;
+    return -expm1f(-p.sigma_t * seg) / (p.sigma_t * expf(-p.sigma_t * dist));
+}
+
 // One point-estimator haze sample at distance `dist` along a segment
 // (spectral-core/src/volume.rs:130-150): camera projection, z-test, HG phase x
-// transmittance / d^2 x seg/4.  Returns whether the sample lands in frame;
-// `contrib`, px, py are its weight and pixel.
+// transmittance / d^2 x seg/4 (x 1/pdf / 4 for free-flight samples).  Returns
+// whether the sample lands in frame; `contrib`, px, py are its weight and pixel.
 __device__ __forceinline__ bool haze_sample(const PhotonParams& p, f3 o, f3 d, float dist, float seg, float power,
                                             uint32_t& px, uint32_t& py, float& contrib) {
     const f3 q = add(o, mul(d, dist));
@@ -126,7 +142,7 @@ __device__ __forceinline__ bool haze_sample(const PhotonParams& p, f3 o, f3 d, f
     if (ok) {
         px = min((uint32_t)(s * (float)p.width), p.width - 1u);
         py = min((uint32_t)((1.0f - t) * (float)p.height), p.height - 1u);
-        if (p.estimator == 0u) {
+        if (p.estimator == 0u || p.estimator == 3u) {
             const f3 to = sub(p.proj.o, q);
             const float dd = fmaxf(length(to), 1e-3f);
             if (p.zbuf && !(dd < p.zbuf[py * p.width + px])) {
@@ -136,7 +152,7 @@ __device__ __forceinline__ bool haze_sample(const PhotonParams& p, f3 o, f3 d, f
                 // direction to the camera is not needed.
                 const float phase = p.g == 0.0f ? kInv4Pi : phase_hg(p.g, dot(d, vdiv(to, dd)));
                 const float trans = expf(-p.sigma_t * dd);
-                contrib = power * p.sigma_s * phase * trans / (dd * dd) * seg / 4.0f;
+                contrib = power * p.sigma_s * phase * trans / (dd * dd) * haze_span(p, dist, seg) / 4.0f;
             }
         } else {
             contrib = power * p.sigma_s * seg / 4.0f * kInv4Pi;
@@ -190,7 +206,7 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
         if (COUNT) ++cnt->segments;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            const float dist = r.f32() * seg;
+            const float dist = haze_distance(p, r.f32(), seg);
             if (DEBUG) continue;
             uint32_t px, py;
             float contrib;
@@ -246,7 +262,7 @@ __device__ __forceinline__ void flush_segments(const PhotonParams& p, WarpSplitS
         const float u = (float)(pcg32(R.rng + (t & 3u) + 1u) >> 8) * (1.0f / 16777216.0f);
         uint32_t px, py;
         float contrib;
-        const bool ok = haze_sample(p, R.o, R.d, u * R.seg, R.seg, R.power, px, py, contrib);
+        const bool ok = haze_sample(p, R.o, R.d, haze_distance(p, u, R.seg), R.seg, R.power, px, py, contrib);
         const float4 pl = ws.payload[R.lane];
         deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, pl.x, pl.y, pl.z, __float_as_uint(pl.w));
     }

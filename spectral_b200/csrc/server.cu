@@ -520,6 +520,8 @@ int sc_server_submit(sc_server* s, const sc_request* r, uint64_t* id) {
                    "request material %u invalid", k);
     SC_REQUIRE(j.width > 0 && j.height > 0 && (uint64_t)j.width * j.height <= (1ull << 26), SC_E_INVALID, "film");
     SC_REQUIRE(j.opts.bins >= 1 && j.opts.bins <= SC_MAX_BINS, SC_E_INVALID, "bins %u", j.opts.bins);
+    SC_REQUIRE(j.opts.estimator <= 1u || j.opts.estimator == 3u, SC_E_INVALID,
+               "estimator %u: requests take the point, isotropic or free-flight estimator", j.opts.estimator);
     SC_REQUIRE(j.opts.lambda_max > j.opts.lambda_min && j.opts.lambda_min > 0.0f, SC_E_INVALID, "band");
     SC_REQUIRE(r->frames >= 1 && (uint64_t)r->frames * j.n_photons <= 0xFFFFFFFFull, SC_E_INVALID,
                "frames x photons must fit 32-bit photon indices");

@@ -118,5 +118,5 @@ def test_beam_rejects_point_only_calls(ctx):
     with pytest.raises(_lib.SpectralError) as e:
         f.trace_debug(10, 1, 4)
     assert e.value.code == _lib.SC_E_STATE
-    with pytest.raises(_lib.SpectralError):
-        sb.GpuPhotonFilm(ctx, scene, cam, beam, 16, 16, 100, 1, 14.0, sb.VolWeights(), estimator=3)
+    with pytest.raises(_lib.SpectralError):  # estimators are 0-3
+        sb.GpuPhotonFilm(ctx, scene, cam, beam, 16, 16, 100, 1, 14.0, sb.VolWeights(), estimator=4)

@@ -545,3 +545,25 @@ def test_oracle_reproduces_beam_and_tracer_fixtures():
     gs, gcam = mg.glass_spheres()
     acc = oracle.tracer_accumulate(gs, gcam, 32, 24, 0, 77, 8) / np.float32(8)
     assert acc.tobytes() == np.load(os.path.join(here, "tracer_glass_32x24.npz"))["mean_xyz"].tobytes()
+
+
+# ---- free-flight sampling: the same single-scatter integral -------------------
+def test_free_flight_and_uniform_point_estimators_agree():
+    """Estimator 3 draws each haze distance from sigma_t exp(-sigma_t t) on the
+    segment and weights it by 1/pdf; it estimates the same in-scatter as the
+    uniform point estimator (volume.rs:130-150).  DSOTM scene with sigma_t 0.3,
+    40k photons: total Y within 2 %."""
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location(
+        "make_golden", os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    scene, beam, _ = mg.dsotm()
+    cam = oracle.camera_look_at((0.5, -0.5, 12.0), (0.5, -0.5, 0.0), (0, 1, 0), 42.0, 1.0)
+    ys = {}
+    for est in (0, 3):
+        p = oracle.vol_params(96, 96, 5, 0.5, 0.3, 0.5, 14.0, estimator=est)
+        img, _, _ = oracle.render_point(scene, cam, beam, p, 0, 40_000)
+        ys[est] = img[1::3].astype(np.float64).sum()
+    assert ys[0] > 0 and abs(ys[3] / ys[0] - 1.0) < 0.02, ys
