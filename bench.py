@@ -171,6 +171,14 @@ def run_cpu(wl, seconds, threads=None):
     return done / dt, done, dt, threads
 
 
+def cpu_serial(wl, seconds):
+    """The restatement on ONE host thread, as the reference's serial photon loop
+    (spectral-core/src/volume.rs:118): photons/s on a shorter sample."""
+    rate, n_s, dt, _ = run_cpu(wl, max(1.0, seconds / 4), threads=1)
+    return {"value": rate, "unit": "photons/s", "cores": 1,
+            "sample": "%d photons from photon 0 on one thread, %.1f s" % (n_s, dt)}
+
+
 def cpu_model():
     try:
         for ln in open("/proc/cpuinfo"):
@@ -448,7 +456,8 @@ def run_gpu(args, rank, world, local_rank):
         rate, n_s, dt, th = run_cpu(args.workload, args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": "photons/s", "cores": th, "kind": "port",
                                 "sample": "%d photons of the workload from photon 0 (whole steps repeated), %.1f s, %s"
-                                          % (n_s, dt, cpu_model())}
+                                          % (n_s, dt, cpu_model()),
+                                "serial": cpu_serial(args.workload, args.cpu_seconds)}
     return line
 
 
@@ -1015,7 +1024,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        rates = []
+        rates, serial = [], None
         per_step = max(1.0, args.cpu_seconds / max(1, args.steps))
         if args.workload == "atomics":
             th = 1
@@ -1064,6 +1073,7 @@ def main():
                 rate, n_s, dt, th = run_cpu(args.workload, per_step)
                 rates.append((n_s, dt))
             sample = "per step %d photons from photon 0 (the whole workload repeated when shorter)" % rates[0][0]
+            serial = cpu_serial(args.workload, args.cpu_seconds)
             metric = METRIC_BEAM if args.workload == "beam" else METRIC_POINT
             cfg_line = {"workload": args.workload, "photons_per_step": cfg["photons"],
                         "film": [cfg["width"], cfg["height"], cfg["bins"]]}
@@ -1081,6 +1091,8 @@ def main():
                 "cpu_baseline": {"value": value, "unit": unit, "cores": th, "kind": "port",
                                  "sample": sample + "; CPU restatement of spectral-core %s, %s" % (what, cpu_model())},
                 "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if args.workload in WORKLOADS:
+            line["cpu_baseline"]["serial"] = serial
         print(json.dumps(line))
         return 0
     if world > 1:

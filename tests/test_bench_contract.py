@@ -31,6 +31,8 @@ def test_reference_arm_prints_one_contract_line(workload):
     assert d["higher_is_better"] is True and d["vs_baseline"] is None and "workload" in d["config"]
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
+    if workload == "prism":  # the reference's serial photon loop, timed beside the threaded one
+        assert d["cpu_baseline"]["serial"]["cores"] == 1 and d["cpu_baseline"]["serial"]["value"] > 0
     e = d["e2e"]
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
