@@ -73,6 +73,63 @@ def _tracer_worker(rank, world, port, w, h, spp, out_path):
     dist.destroy_process_group()
 
 
+class _OracleTracer:
+    """Stand-in for GpuTracer on a gloo rank: the same dims / set_rows /
+    accumulate / read_xyz calls, rendered by the CPU oracle."""
+
+    def __init__(self, w, h, seed):
+        self.oracle, self.osc, self.oc = _tracer_scene()
+        self.w, self.h, self.seed = w, h, seed
+        self.rows, self.samples = (0, h), 0
+        self.sum = np.zeros(3 * w * h, np.float32)
+
+    def dims(self):
+        return self.w, self.h
+
+    def set_rows(self, b, e):
+        self.rows = (b, e)
+
+    def accumulate(self, spp):
+        self.oracle.lib.or_tracer_accumulate(C.byref(self.osc.c), C.byref(self.oc), self.w, self.h, 0, self.seed, spp,
+                                             self.samples, 8, self.rows[0], self.rows[1], self.oracle.fp(self.sum))
+        self.samples += spp
+
+    def read_xyz(self):
+        return self.sum / np.float32(max(self.samples, 1))
+
+
+def _trace_rows_worker(rank, world, port, w, h, spp, out_path):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    from spectral_b200.shard import trace_rows_sharded
+    np.save(out_path % rank, trace_rows_sharded(_OracleTracer(w, h, 5), spp))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_trace_rows_sharded_on_two_ranks(tmp_path):
+    """shard.trace_rows_sharded end to end on two gloo ranks (set_rows,
+    accumulate, read back, gather), the oracle standing in for each GPU."""
+    w, h, spp, world = 20, 13, 3, 2
+    out = str(tmp_path / "rows%d.npy")
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_trace_rows_worker, args=(r, world, port, w, h, spp, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    whole = _OracleTracer(w, h, 5)
+    whole.accumulate(spp)
+    ref = whole.read_xyz().reshape(h, w, 3)
+    assert ref.sum() > 0
+    for r in range(world):
+        assert np.load(out % r).tobytes() == ref.tobytes(), r
+
+
 @pytest.mark.parametrize("world", [2, 3])
 def test_tracer_row_bands_gather_to_the_full_image(tmp_path, world):
     """Pixel-row ownership for the camera tracer: each rank renders its band of
