@@ -116,6 +116,18 @@ def test_null_arguments_fail_with_status():
     assert b"null" in _lib.lib.sc_last_error()
     assert _lib.lib.sc_ctx_create(0, None, None) == _lib.SC_E_INVALID
     assert _lib.lib.sc_load_sensor_tables(b"/nonexistent.csv", (C.c_float * 355)()) == _lib.SC_E_INVALID
+    # entry points added beside the reference API refuse null handles the same way
+    f16 = (C.c_float * 16)()
+    assert _lib.lib.sc_camera_proj_params(None, f16) == _lib.SC_E_INVALID
+    assert _lib.lib.sc_glass_n_device(None, 0, None, 4, None, None) == _lib.SC_E_INVALID
+    assert _lib.lib.sc_tracer_set_rows(None, 0, 1) == _lib.SC_E_INVALID
+    assert _lib.lib.sc_tracer_set_spectral(None, 0) == _lib.SC_E_INVALID
+    e = C.c_float()
+    assert _lib.lib.sc_atomic_film_auto_expose_accum(None, 1.0, C.byref(e)) == _lib.SC_E_INVALID
+    assert _lib.lib.sc_atomic_film_to_rgb8(None, 1.0, None) == _lib.SC_E_INVALID
+    n = C.c_float(500.0)
+    assert _lib.lib.sc_glass_n_many(0, None, 1, None) == _lib.SC_E_INVALID
+    assert _lib.lib.sc_glass_n_many(0, C.byref(n), 0, None) == _lib.SC_OK  # nothing to do
 
 
 def test_no_gpu_means_error_not_fallback():
