@@ -7,6 +7,7 @@ required to be bit-identical.  Lambertian sampling calls cosf/sinf, whose last
 bits differ between CUDA and glibc, so those scenes use the reference's
 statistical gates (frac of pixels above 10x the mean difference, p99, energy).
 """
+import math
 import os
 
 import numpy as np
@@ -197,6 +198,11 @@ def test_background_integrates_to_d65_and_illuminant_a(ctx):
     assert abs(m[0] / m.sum() - 0.3127) < 6e-3 and abs(m[1] / m.sum() - 0.3290) < 6e-3
     gpu, cpu, _ = run_both(ctx, sb.Scene(background=1.0), cam, 32, 32, 16, 3, illuminant=sb.ILLUMINANT_A)
     assert gpu.tobytes() == cpu.tobytes()
+    # the render-level illuminant gate (core/tests/scene_b_metamerism.rs:69-100):
+    # the chromaticity moves by more than 0.05 from D65 to illuminant A
+    a = gpu.reshape(-1, 3).sum(0).astype(np.float64)
+    dist = math.hypot(m[0] / m.sum() - a[0] / a.sum(), m[1] / m.sum() - a[1] / a.sum())
+    assert dist > 0.05, dist
 
 
 def test_dispersion_collapse_preserves_brightness(ctx):

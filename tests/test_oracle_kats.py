@@ -112,6 +112,63 @@ def test_d65_white_point():
     assert abs(out[0] / s - 0.3127) <= 2e-3 and abs(out[1] / s - 0.3290) <= 2e-3
 
 
+# ---- core/tests/rayleigh.rs: 1/lambda^4 through the shipped sensor tables ---
+def _integrate_d65(weight):
+    """sum over 380..730 nm in 5 nm steps of D65 * weight * cmf * 5 (f32, as rayleigh.rs:10-23)."""
+    x = y = z = np.float32(0.0)
+    c = np.zeros(3, np.float32)
+    nm = np.float32(380.0)
+    while nm <= np.float32(730.0):
+        sv = np.float32(O.or_illuminant(0, float(nm))) * np.float32(weight(nm))
+        O.or_cmf(float(nm), fp(c))
+        x += sv * c[0] * np.float32(5.0)
+        y += sv * c[1] * np.float32(5.0)
+        z += sv * c[2] * np.float32(5.0)
+        nm += np.float32(5.0)
+    xyz = np.array([x, y, z], np.float32)
+    rgb = np.zeros(3, np.float32)
+    O.or_xyz_to_linear_srgb(fp(xyz), fp(rgb))
+    return xyz / xyz.sum(), rgb
+
+
+def test_scattered_sky_is_blue():
+    ch, rgb = _integrate_d65(lambda nm: np.float32(550.0 / nm) ** 4)
+    assert ch[0] < 0.28 and ch[1] < 0.33 and rgb[2] > rgb[0]
+
+
+def test_sunset_transmitted_is_red():
+    ch, rgb = _integrate_d65(lambda nm: np.exp(np.float32(-1.5) * np.float32(550.0 / nm) ** 4))
+    assert ch[0] > 0.40 and rgb[0] > rgb[2]
+
+
+# ---- core/tests/scene_b_metamerism.rs:16-66: illuminant-dependent colour ------
+def _chroma_under(refl, ill):
+    x = y = z = np.float32(0.0)
+    c = np.zeros(3, np.float32)
+    nm = np.float32(380.0)
+    while nm <= np.float32(730.0):
+        sv = np.float32(O.or_illuminant(ill, float(nm))) * np.float32(refl(nm))
+        O.or_cmf(float(nm), fp(c))
+        x += sv * c[0] * np.float32(5.0)
+        y += sv * c[1] * np.float32(5.0)
+        z += sv * c[2] * np.float32(5.0)
+        nm += np.float32(5.0)
+    s = x + y + z
+    return x / s, y / s
+
+
+def test_illuminant_swap_changes_color_relationship():
+    smooth = lambda nm: 0.5 + 0.3 * math.cos((nm - 555.0) / 120.0)  # noqa: E731
+    g = lambda nm, c, w: math.exp(-(((nm - c) / w) ** 2))  # noqa: E731
+    bumpy = lambda nm: min(max(0.55 * g(nm, 450, 25) + 0.75 * g(nm, 540, 25) + 0.65 * g(nm, 610, 25), 0.0), 1.0)  # noqa: E731
+    assert sum(abs(smooth(n) - bumpy(n)) for n in range(400, 700, 20)) > 0.5
+
+    def gap(ill):
+        a, b = _chroma_under(smooth, ill), _chroma_under(bumpy, ill)
+        return math.hypot(a[0] - b[0], a[1] - b[1])
+    assert abs(gap(1) - gap(0)) > 1e-3  # illuminant A vs D65
+
+
 def test_cmf_in_band_and_tables():
     c = np.zeros(3, np.float32)
     O.or_cmf(555.0, fp(c))
