@@ -187,6 +187,15 @@ class GpuContext:
         self.h = C.c_void_p()
         check(lib.sc_ctx_create(int(device), self.tables.ctypes.data_as(C.POINTER(C.c_float)), C.byref(self.h)))
 
+    @classmethod
+    def new(cls, device=0, tables=None):
+        """GpuContext::new (spectral-gpu/src/lib.rs:29-41): the context, or None
+        when no usable sm_100 device is present (the reference's Option)."""
+        try:
+            return cls(device, tables)
+        except _lib.SpectralError:
+            return None
+
     def synchronize(self):
         check(lib.sc_ctx_synchronize(self.h))
 

@@ -130,6 +130,13 @@ def test_null_arguments_fail_with_status():
     assert _lib.lib.sc_glass_n_many(0, C.byref(n), 0, None) == _lib.SC_OK  # nothing to do
 
 
+def test_context_new_is_none_without_a_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    assert sb.GpuContext.new() is None  # GpuContext::new() -> None, as the reference's Option
+
+
 def test_no_gpu_means_error_not_fallback():
     try:
         import torch
