@@ -31,7 +31,8 @@ __device__ __forceinline__ void flush_mask(uint32_t* mask, uint32_t words, uint3
     __syncwarp();
 }
 
-template <int AGG, int MINB, bool SPLIT>
+// FF: built with free-flight sampling (estimator 3) as well; jobs choose per job.
+template <int AGG, int MINB, bool SPLIT, bool FF>
 __global__ void __launch_bounds__(256, MINB) batch_kernel(const BatchJobDev* __restrict__ jobs,
                                                           const WorkItem* __restrict__ items, uint32_t n_items,
                                                           uint32_t* counter, const float* __restrict__ cmf_g,
@@ -71,11 +72,11 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(const BatchJobDev* __r
         S.prims = slot.prims; S.planes = slot.planes; S.mats = slot.mats; S.n_prims = slot.p.n_prims;
         if (SPLIT) {
             for (uint32_t b0 = 0; b0 < item.count; b0 += 32u)
-                trace_warp_split<true, AGG>(slot.p, S, cmf, item.begin + b0 + lane, b0 + lane < item.count,
+                trace_warp_split<true, AGG, FF>(slot.p, S, cmf, item.begin + b0 + lane, b0 + lane < item.count,
                                             cur_words ? mask : nullptr, split[warp]);
         } else {
             for (uint32_t i = lane; i < item.count; i += 32u)
-                trace_photon<true, AGG, false>(slot.p, S, cmf, item.begin + i, cur_words ? mask : nullptr);
+                trace_photon<true, AGG, false, false, FF>(slot.p, S, cmf, item.begin + i, cur_words ? mask : nullptr);
         }
         __syncwarp();
     }
@@ -85,11 +86,14 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(const BatchJobDev* __r
 using BatchFn = void (*)(const BatchJobDev*, const WorkItem*, uint32_t, uint32_t*, const float*, uint32_t);
 
 template <bool SPLIT>
-BatchFn batch_fn_t(int agg, int minb) {
-    if (minb >= 5) return agg ? batch_kernel<1, 5, SPLIT> : batch_kernel<0, 5, SPLIT>;
-    return agg ? batch_kernel<1, 4, SPLIT> : batch_kernel<0, 4, SPLIT>;
+BatchFn batch_fn_t(int agg, int minb, bool ff) {
+    if (ff) return batch_kernel<0, 4, SPLIT, true>;  // batches with free-flight jobs: plain atomics, 4 CTAs per SM
+    if (minb >= 5) return agg ? batch_kernel<1, 5, SPLIT, false> : batch_kernel<0, 5, SPLIT, false>;
+    return agg ? batch_kernel<1, 4, SPLIT, false> : batch_kernel<0, 4, SPLIT, false>;
 }
-BatchFn batch_fn(int agg, int minb, int split) { return split ? batch_fn_t<true>(agg, minb) : batch_fn_t<false>(agg, minb); }
+BatchFn batch_fn(int agg, int minb, int split, bool ff) {
+    return split ? batch_fn_t<true>(agg, minb, ff) : batch_fn_t<false>(agg, minb, ff);
+}
 
 }  // namespace
 
@@ -102,9 +106,9 @@ size_t batch_smem(uint32_t mask_words_max, int split, uint32_t block) {
            (split ? warps * sizeof(WarpSplitSmem) : 0);
 }
 
-int batch_occupancy(int agg, int minb, int split, uint32_t mask_words_max, uint32_t block) {
+int batch_occupancy(int agg, int minb, int split, uint32_t mask_words_max, uint32_t block, bool ff) {
     int n = 0;
-    const void* fn = reinterpret_cast<const void*>(batch_fn(agg, minb, split));
+    const void* fn = reinterpret_cast<const void*>(batch_fn(agg, minb, split, ff));
     const size_t smem = batch_smem(mask_words_max, split, block);
     if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)block, smem) != cudaSuccess) return 1;
@@ -113,12 +117,12 @@ int batch_occupancy(int agg, int minb, int split, uint32_t mask_words_max, uint3
 
 cudaError_t launch_batch(const BatchJobDev* jobs, const WorkItem* items, uint32_t n_items, uint32_t* counter,
                          const float* cmf, uint32_t mask_words_max, int agg, int minb, int split, uint32_t grid,
-                         cudaStream_t s, uint32_t block) {
+                         cudaStream_t s, uint32_t block, bool ff) {
     // the shared-memory attribute was raised by batch_occupancy before any capture
     const size_t smem = batch_smem(mask_words_max, split, block);
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
-    batch_fn(agg, minb, split)<<<grid, block, smem, s>>>(jobs, items, n_items, counter, cmf, mask_words_max);
+    batch_fn(agg, minb, split, ff)<<<grid, block, smem, s>>>(jobs, items, n_items, counter, cmf, mask_words_max);
     return cudaGetLastError();
 }
 

@@ -28,10 +28,11 @@ struct alignas(16) BatchJobDev {
 struct WorkItem { uint32_t job, begin, count; };
 
 // `block`: threads per CTA, 128 or 256 (one shared-memory job slot per warp).
+// `ff`: some job uses free-flight sampling (the kernel built with it).
 size_t batch_smem(uint32_t mask_words_max, int split, uint32_t block = 256);
-int batch_occupancy(int agg, int minb, int split, uint32_t mask_words_max, uint32_t block = 256);
+int batch_occupancy(int agg, int minb, int split, uint32_t mask_words_max, uint32_t block = 256, bool ff = false);
 cudaError_t launch_batch(const BatchJobDev* jobs, const WorkItem* items, uint32_t n_items, uint32_t* counter,
                          const float* cmf, uint32_t mask_words_max, int agg, int minb, int split, uint32_t grid,
-                         cudaStream_t s, uint32_t block = 256);
+                         cudaStream_t s, uint32_t block = 256, bool ff = false);
 
 }  // namespace sc

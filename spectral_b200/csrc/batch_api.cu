@@ -74,6 +74,13 @@ struct sc_batch {
     uint64_t total_photons = 0;
     sc_batch_tuning tuning{};
     uint32_t grid = 0;
+    bool ff = false;  // some job samples free-flight distances: the kernel built with them
+
+    bool any_free_flight() const {
+        for (const sc_scene_job& j : jobs)
+            if (j.opts.estimator == 3u && j.weights.sigma_t > 0.0f) return true;
+        return false;
+    }
     cudaGraphExec_t graph = nullptr;
     cudaStream_t graph_stream = nullptr;
 
@@ -153,7 +160,9 @@ struct sc_batch {
         n.aggregate = n.aggregate ? 1 : 0;
         n.per_photon = n.per_photon ? 1 : 0;
         n.block = n.block == 128u ? 128u : 256u;
-        const int occ = batch_occupancy((int)n.aggregate, (int)n.minb, n.per_photon ? 0 : 1, kBatchMaskWords, n.block);
+        ff = any_free_flight();
+        const int occ = batch_occupancy((int)n.aggregate, (int)n.minb, n.per_photon ? 0 : 1, kBatchMaskWords, n.block,
+                                        ff);
         grid = n.grid ? n.grid : (uint32_t)(ctx->sms * occ);
         if (n.chunk_photons != tuning.chunk_photons || n_items == 0) {
             int rc = build_items(n.chunk_photons);
@@ -168,7 +177,7 @@ struct sc_batch {
     int enqueue_batch(cudaStream_t s) {
         SC_CUDA(launch_batch(d_jobs.p, d_items.p, n_items, counter.p, ctx->cmf.p, kBatchMaskWords,
                              (int)tuning.aggregate, (int)tuning.minb, tuning.per_photon ? 0 : 1, grid, s,
-                             tuning.block));
+                             tuning.block, ff));
         // the drain rewrites the images: wait for the last asynchronous copy of them
         SC_CUDA(cudaStreamWaitEvent(s, copied, cudaEventWaitExternal));
         SC_CUDA(launch_reduce_many(d_descs.p, (uint32_t)jobs.size(), total_words, true, max_channels, dirty_list.p,
@@ -422,6 +431,10 @@ int sc_batch_update_jobs(sc_batch* b, const sc_scene_job* jobs, uint32_t n) {
                    SC_E_STATE, "job %u changes its film or photon budget; create a new batch", i);
     }
     b->jobs.assign(jobs, jobs + n);
+    if (b->any_free_flight() != b->ff) {  // another kernel: new grid and graph
+        const int rc = b->apply_tuning(b->tuning);
+        if (rc != SC_OK) return rc;
+    }
     return b->upload_jobs();  // stream-ordered before the next run on the same stream
     SC_GUARD_END
 }
@@ -522,7 +535,7 @@ int sc_batch_stats(sc_batch* b, uint64_t out[6]) {
     // dirty tiles of one pass: trace only, count the set bits, then drain
     SC_CUDA(launch_batch(b->d_jobs.p, b->d_items.p, b->n_items, b->counter.p, b->ctx->cmf.p, kBatchMaskWords,
                          (int)b->tuning.aggregate, (int)b->tuning.minb, b->tuning.per_photon ? 0 : 1, b->grid,
-                         b->stream, b->tuning.block));
+                         b->stream, b->tuning.block, b->ff));
     std::vector<uint32_t> fl(b->flags.n);
     SC_CUDA(cudaMemcpyAsync(fl.data(), b->flags.p, b->flags.bytes(), cudaMemcpyDeviceToHost, b->stream));
     SC_CUDA(cudaStreamSynchronize(b->stream));

@@ -31,7 +31,8 @@ __host__ __device__ __forceinline__ size_t split_offset(const PhotonParams& p, u
 
 // 256 threads per CTA; MINB CTAs per SM bound the registers (4: 63 registers,
 // no spills; 5: 48 registers, a few spills, more warps in flight).
-template <bool SPEC, int AGG, int MINB, bool SPLIT>
+// FF: built with free-flight sampling (estimator 3) as well.
+template <bool SPEC, int AGG, int MINB, bool SPLIT, bool FF>
 __global__ void __launch_bounds__(256, MINB) photon_kernel(const PhotonParams p, uint32_t mask_words) {
     extern __shared__ __align__(16) unsigned char smem[];
     const float* cmf;
@@ -45,12 +46,12 @@ __global__ void __launch_bounds__(256, MINB) photon_kernel(const PhotonParams p,
             const uint32_t i = base + lane;
             const bool valid = i < p.photon_count;
             const uint32_t k = p.order && valid ? p.order[i] : i;
-            trace_warp_split<SPEC, AGG>(p, S, cmf, p.photon_base + k, valid, smask, ws[warp]);
+            trace_warp_split<SPEC, AGG, FF>(p, S, cmf, p.photon_base + k, valid, smask, ws[warp]);
         }
     } else {
         const uint32_t stride = gridDim.x * blockDim.x;
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += stride)
-            trace_photon<SPEC, AGG, false>(p, S, cmf, p.photon_base + (p.order ? p.order[i] : i), smask);
+            trace_photon<SPEC, AGG, false, false, FF>(p, S, cmf, p.photon_base + (p.order ? p.order[i] : i), smask);
     }
     if (smask) {  // publish this CTA's dirty tiles
         __syncthreads();
@@ -262,16 +263,19 @@ size_t scene_smem_bytes(uint32_t n_prims, uint32_t n_planes, uint32_t n_mats) {
 using PhotonKernelFn = void (*)(const PhotonParams, uint32_t);
 
 template <bool SPLIT>
-static PhotonKernelFn photon_fn_t(bool spec, int agg, int minb) {
+static PhotonKernelFn photon_fn_t(bool spec, int agg, int minb, bool ff) {
+    // free-flight launches: plain atomics, 4 CTAs per SM
+    if (ff) return spec ? photon_kernel<true, 0, 4, SPLIT, true> : photon_kernel<false, 0, 4, SPLIT, true>;
     if (minb >= 5) {
-        if (spec) return agg ? photon_kernel<true, 1, 5, SPLIT> : photon_kernel<true, 0, 5, SPLIT>;
-        return agg ? photon_kernel<false, 1, 5, SPLIT> : photon_kernel<false, 0, 5, SPLIT>;
+        if (spec) return agg ? photon_kernel<true, 1, 5, SPLIT, false> : photon_kernel<true, 0, 5, SPLIT, false>;
+        return agg ? photon_kernel<false, 1, 5, SPLIT, false> : photon_kernel<false, 0, 5, SPLIT, false>;
     }
-    if (spec) return agg ? photon_kernel<true, 1, 4, SPLIT> : photon_kernel<true, 0, 4, SPLIT>;
-    return agg ? photon_kernel<false, 1, 4, SPLIT> : photon_kernel<false, 0, 4, SPLIT>;
+    if (spec) return agg ? photon_kernel<true, 1, 4, SPLIT, false> : photon_kernel<true, 0, 4, SPLIT, false>;
+    return agg ? photon_kernel<false, 1, 4, SPLIT, false> : photon_kernel<false, 0, 4, SPLIT, false>;
 }
-static PhotonKernelFn photon_fn(const LaunchShape& s, bool spec) {
-    return s.split ? photon_fn_t<true>(spec, s.aggregate, s.minb) : photon_fn_t<false>(spec, s.aggregate, s.minb);
+static PhotonKernelFn photon_fn(const LaunchShape& s, bool spec, bool ff) {
+    return s.split ? photon_fn_t<true>(spec, s.aggregate, s.minb, ff)
+                   : photon_fn_t<false>(spec, s.aggregate, s.minb, ff);
 }
 // Shared memory beyond scene + mask: one segment buffer per warp (8 warps).
 static size_t split_bytes(const LaunchShape& s) { return s.split ? 16 + 8 * sizeof(WarpSplitSmem) : 0; }
@@ -294,7 +298,7 @@ int occupancy_blocks(const void* fn, int block, size_t smem) {
 }
 
 int photon_occupancy_blocks(const LaunchShape& shape, bool spectral, size_t smem) {
-    return occupancy_blocks(reinterpret_cast<const void*>(photon_fn(shape, spectral)), (int)shape.block,
+    return occupancy_blocks(reinterpret_cast<const void*>(photon_fn(shape, spectral, false)), (int)shape.block,
                             smem + split_bytes(shape));
 }
 
@@ -370,7 +374,7 @@ static cudaError_t launch_photons_in(const PhotonParams& p, const LaunchShape& s
     const bool spec = p.channels != 3u || p.bins != 0u;
     const uint32_t need = (p.photon_count + 255u) / 256u;
     const uint32_t grid = need < shape.grid ? need : shape.grid;
-    photon_fn(shape, spec)<<<grid, 256, smem, s>>>(p, mw);
+    photon_fn(shape, spec, free_flight(p))<<<grid, 256, smem, s>>>(p, mw);
     return cudaGetLastError();
 }
 

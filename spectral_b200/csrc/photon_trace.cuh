@@ -119,12 +119,20 @@ struct PhotonCounts { uint32_t segments, splats, scatters; };
 // (sigma_t exp(-sigma_t t)) instead of the uniform estimator's seg: the same
 // single-scatter integral, with samples denser where the beam enters.  With
 // sigma_t = 0 it is the uniform estimator.
+// FF: free-flight distances (estimator 3 with sigma_t > 0).  Kernels are built
+// with or without free-flight support (FFOK); launches of the uniform
+// estimators take the kernels without it, whose code is the uniform path only.
+__host__ __device__ __forceinline__ bool free_flight(const PhotonParams& p) {
+    return p.estimator == 3u && p.sigma_t > 0.0f;
+}
+template <bool FF>
 __device__ __forceinline__ float haze_distance(const PhotonParams& p, float u, float seg) {
-    if (p.estimator != 3u || !(p.sigma_t > 0.0f)) return u * seg;
+    if (!FF) return u * seg;
     return -log1pf(u * expm1f(-p.sigma_t * seg)) / p.sigma_t;
 }
+template <bool FF>
 __device__ __forceinline__ float haze_span(const PhotonParams& p, float dist, float seg) {
-    if (p.estimator != 3u || !(p.sigma_t > 0.0f)) return seg;
+    if (!FF) return seg;
     return -expm1f(-p.sigma_t * seg) / (p.sigma_t * expf(-p.sigma_t * dist));
 }
 
@@ -132,6 +140,7 @@ __device__ __forceinline__ float haze_span(const PhotonParams& p, float dist, fl
 // (spectral-core/src/volume.rs:130-150): camera projection, z-test, HG phase x
 // transmittance / d^2 x seg/4 (x 1/pdf / 4 for free-flight samples).  Returns
 // whether the sample lands in frame; `contrib`, px, py are its weight and pixel.
+template <bool FF>
 __device__ __forceinline__ bool haze_sample(const PhotonParams& p, f3 o, f3 d, float dist, float seg, float power,
                                             uint32_t& px, uint32_t& py, float& contrib) {
     const f3 q = add(o, mul(d, dist));
@@ -142,7 +151,7 @@ __device__ __forceinline__ bool haze_sample(const PhotonParams& p, f3 o, f3 d, f
     if (ok) {
         px = min((uint32_t)(s * (float)p.width), p.width - 1u);
         py = min((uint32_t)((1.0f - t) * (float)p.height), p.height - 1u);
-        if (p.estimator == 0u || p.estimator == 3u) {
+        if (FF || p.estimator != 1u) {  // point estimators (the beam estimator has its own kernel)
             const f3 to = sub(p.proj.o, q);
             const float dd = fmaxf(length(to), 1e-3f);
             if (p.zbuf && !(dd < p.zbuf[py * p.width + px])) {
@@ -152,7 +161,7 @@ __device__ __forceinline__ bool haze_sample(const PhotonParams& p, f3 o, f3 d, f
                 // direction to the camera is not needed.
                 const float phase = p.g == 0.0f ? kInv4Pi : phase_hg(p.g, dot(d, vdiv(to, dd)));
                 const float trans = expf(-p.sigma_t * dd);
-                contrib = power * p.sigma_s * phase * trans / (dd * dd) * haze_span(p, dist, seg) / 4.0f;
+                contrib = power * p.sigma_s * phase * trans / (dd * dd) * haze_span<FF>(p, dist, seg) / 4.0f;
             }
         } else {
             contrib = power * p.sigma_s * seg / 4.0f * kInv4Pi;
@@ -175,7 +184,7 @@ __device__ __forceinline__ void photon_payload(const PhotonParams& p, const floa
     }
 }
 
-template <bool SPEC, int AGG, bool DEBUG, bool COUNT = false>
+template <bool SPEC, int AGG, bool DEBUG, bool COUNT = false, bool FFOK = true>
 __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneView& S, const float* cmf,
                                              uint32_t idx, uint32_t* smask, PhotonCounts* cnt = nullptr) {
     Rng r = Rng::make(idx, p.seed);
@@ -206,11 +215,14 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
         if (COUNT) ++cnt->segments;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            const float dist = haze_distance(p, r.f32(), seg);
+            const bool ff = FFOK && free_flight(p);
+            const float u = r.f32();
+            const float dist = ff ? haze_distance<true>(p, u, seg) : haze_distance<false>(p, u, seg);
             if (DEBUG) continue;
             uint32_t px, py;
             float contrib;
-            const bool ok = haze_sample(p, o, d, dist, seg, power, px, py, contrib);
+            const bool ok = ff ? haze_sample<true>(p, o, d, dist, seg, power, px, py, contrib)
+                               : haze_sample<false>(p, o, d, dist, seg, power, px, py, contrib);
             if (COUNT) { if (ok) ++cnt->splats; continue; }
             deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, cx, cy, cz, bin);
         }
@@ -252,26 +264,33 @@ struct alignas(16) WarpSplitSmem {
 };
 static_assert(sizeof(SegRec) == 40, "segment record layout");
 
-template <bool SPEC, int AGG>
-__device__ __forceinline__ void flush_segments(const PhotonParams& p, WarpSplitSmem& ws, uint32_t n, uint32_t* smask,
-                                               uint32_t lane) {
-    __syncwarp();
-    const uint32_t total = 4u * n;
+template <bool SPEC, int AGG, bool FF>
+__device__ __forceinline__ void flush_loop(const PhotonParams& p, WarpSplitSmem& ws, uint32_t total, uint32_t* smask,
+                                           uint32_t lane) {
     for (uint32_t t = lane; t < total; t += 32u) {
         const SegRec R = ws.seg[t >> 2];
         const float u = (float)(pcg32(R.rng + (t & 3u) + 1u) >> 8) * (1.0f / 16777216.0f);
         uint32_t px, py;
         float contrib;
-        const bool ok = haze_sample(p, R.o, R.d, haze_distance(p, u, R.seg), R.seg, R.power, px, py, contrib);
+        const bool ok = haze_sample<FF>(p, R.o, R.d, haze_distance<FF>(p, u, R.seg), R.seg, R.power, px, py, contrib);
         const float4 pl = ws.payload[R.lane];
         deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, pl.x, pl.y, pl.z, __float_as_uint(pl.w));
     }
+}
+
+// The estimator is fixed per job: one uniform branch picks the loop.
+template <bool SPEC, int AGG, bool FFOK>
+__device__ __forceinline__ void flush_segments(const PhotonParams& p, WarpSplitSmem& ws, uint32_t n, uint32_t* smask,
+                                               uint32_t lane) {
+    __syncwarp();
+    if (FFOK && free_flight(p)) flush_loop<SPEC, AGG, true>(p, ws, 4u * n, smask, lane);
+    else flush_loop<SPEC, AGG, false>(p, ws, 4u * n, smask, lane);
     __syncwarp();
 }
 
 // All 32 lanes of the warp must call this together; lanes without a photon pass
 // valid = false.
-template <bool SPEC, int AGG>
+template <bool SPEC, int AGG, bool FFOK>
 __device__ __forceinline__ void trace_warp_split(const PhotonParams& p, const SceneView& S, const float* cmf,
                                                  uint32_t idx, bool valid, uint32_t* smask, WarpSplitSmem& ws) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -299,7 +318,7 @@ __device__ __forceinline__ void trace_warp_split(const PhotonParams& p, const Sc
         // one flush site (keeps the inlined haze code single): when this bounce's
         // segments do not fit, and once when every photon is done
         if (n + cnt > kWarpSegs || (m == 0u && n)) {
-            flush_segments<SPEC, AGG>(p, ws, n, smask, lane);
+            flush_segments<SPEC, AGG, FFOK>(p, ws, n, smask, lane);
             n = 0;
         }
         if (m == 0u) break;

@@ -400,8 +400,10 @@ struct sc_server {
         SC_CUDA(cudaMemcpyAsync(d_items.p, h->items, h_items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
                                 stream));
         SC_CUDA(cudaEventRecord(h->used, stream));
+        bool ff = false;  // some request samples free-flight distances: the kernel built with them
+        for (const Request* q : active) ff = ff || (q->r.job.opts.estimator == 3u && q->r.job.weights.sigma_t > 0.0f);
         SC_CUDA(launch_batch(d_jobs.p, d_items.p, (uint32_t)h_items.size(), counter.p, ctx->cmf.p, kBatchMaskWords, 0,
-                             4, 1, grid, stream));
+                             4, 1, grid, stream, 256, ff));
         SC_CUDA(launch_reduce_many(d_descs.p, n, words, true, maxc, dirty_list.p, dirty_count.p, stream));
         photons += step_photons;
         StepRecord rec;
