@@ -4,7 +4,7 @@ Every kernel is compiled for ``sm_100a`` only, with ``-fmad=false`` so no
 multiply-add is contracted (transport arithmetic must match the CPU crate
 operation by operation) and IEEE division / square root (the nvcc default).
 
-    python -m spectral_b200.build [--verbose-ptxas] [--force]
+    python spectral_b200/build.py [--verbose-ptxas] [--force]
 """
 import argparse
 import concurrent.futures as cf
