@@ -113,6 +113,58 @@ def build_scene(wl):
     return rainbow_workload(cfg["width"], cfg["height"])
 
 
+def load_specs():
+    """spectral_b200/specs.py loaded by file path: the workload descriptions in
+    plain Python, so that the CPU legs never load the CUDA library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("spectral_specs", os.path.join(ROOT, "spectral_b200", "specs.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def oracle_scene(d, aspect):
+    """(OScene, or_beam or None, or_camera) of a specs scene dict, in the record
+    order the library's Scene flattens it (solids, then spheres)."""
+    import oracle
+    prims, planes, mats = [], [], []
+
+    def mat(m):
+        mats.append(oracle.or_mat(0.0, m[1], 1, 0) if m[0] == "glass" else oracle.or_mat(m[1], 0, 0, 0))
+        return len(mats) - 1
+    for pl, m in d["solids"]:
+        start = len(planes)
+        planes.extend(oracle.or_plane(oracle.F3(*n), dd) for n, dd in pl)
+        prims.append(oracle.or_prim(oracle.F3(0.0, 0.0, 0.0), 0.0, start, len(pl), 1, mat(m)))
+    for c, r, m in d["spheres"]:
+        prims.append(oracle.or_prim(oracle.F3(*c), r, 0, 0, 0, mat(m)))
+    sc = oracle.OScene(b"".join(bytes(x) for x in prims), len(prims), b"".join(bytes(x) for x in planes), len(planes),
+                       b"".join(bytes(x) for x in mats), len(mats), 0.0)
+    beam = oracle.or_beam(*[oracle.F3(*v) for v in d["beam"]]) if "beam" in d else None
+    o, t, up, vfov = d["camera"]
+    return sc, beam, oracle.camera_look_at(o, t, up, vfov, aspect)
+
+
+def oracle_scene_of(wl):
+    cfg = WORKLOADS[wl]
+    specs = load_specs()
+    d = {"prism": specs.prism_scene, "beam": specs.dsotm_scene, "rainbow": specs.rainbow_scene}[wl]()
+    return oracle_scene(d, cfg["width"] / cfg["height"])
+
+
+def oracle_prism_job(spec):
+    """(OScene, or_camera, or_beam, or_vol_params) of a prism job dict (the
+    sc_scene_job that spectral_b200.batch.job_from_spec makes of it)."""
+    import oracle
+    specs = load_specs()
+    d = dict(solids=[(specs.prism_planes(spec["apex_deg"], 1.0, 1.0), ("glass", spec["glass"]))], spheres=[],
+             beam=specs.prism_beam(spec["apex_deg"], 1.0, spec["incidence_deg"], 0.02), camera=specs.PRISM_CAMERA)
+    sc, beam, cam = oracle_scene(d, spec["width"] / spec["height"])
+    p = oracle.vol_params(spec["width"], spec["height"], spec["seed"], spec["sigma_s"], spec["sigma_t"], spec["g"],
+                          6.0, 8, spec["lambda_min"], spec["lambda_max"], bins=spec["bins"])
+    return sc, cam, beam, p
+
+
 # ----------------------------------------------------------------------------
 # CPU reference arm / baseline: the oracle's point estimator on all host cores
 # ----------------------------------------------------------------------------
@@ -120,11 +172,7 @@ def run_cpu(wl, seconds, threads=None):
     """Photons/s of the CPU restatement on a bounded sample of the workload."""
     import oracle
     cfg = WORKLOADS[wl]
-    scene, beam, cam = build_scene(wl)
-    prims, np_, planes, npl, mats, nm = scene.arrays()
-    osc = oracle.OScene(bytes(prims), np_, bytes(planes), npl, bytes(mats), nm, scene.background)
-    ob = oracle.or_beam.from_buffer_copy(bytes(beam.c))
-    oc = oracle.or_camera.from_buffer_copy(bytes(cam.c))
+    osc, ob, oc = oracle_scene_of(wl)
     # the reference's XYZ film (per-thread int64 XYZ films merged exactly): a
     # 64-bin film per host thread would cost more to clear and merge than to trace
     p = oracle.vol_params(cfg["width"], cfg["height"], cfg["seed"], cfg["sigma_s"], cfg["sigma_t"], cfg["g"],
@@ -473,12 +521,10 @@ def run_cpu_tracer(seconds, threads=None):
     the reference's rayon loop) with the emitter / roulette extensions, on
     whole frames at 1 spp until ~`seconds` of work."""
     import oracle
-    from spectral_b200.scenes import tracer_workload
     W, H = TRACER["width"], TRACER["height"]
-    scene, cam, kw = tracer_workload(W, H)
-    prims, np_, planes, npl, mats, nm = scene.arrays()
-    osc = oracle.OScene(bytes(prims), np_, bytes(planes), npl, bytes(mats), nm, scene.background)
-    oc = oracle.or_camera.from_buffer_copy(bytes(cam.c))
+    d = load_specs().tracer_scene()
+    osc, _, oc = oracle_scene(d, W / H)
+    kw = d["tracer"]
     c, r, sc = kw["emitter"]
     ext = oracle.or_tracer_ext(oracle.F3(*c), r, sc, kw["rr_start"])
     threads = threads or os.cpu_count() or 1
@@ -800,23 +846,22 @@ def run_gpu_serve(args, rank, world, local_rank):
 BATCH = dict(n_jobs=256, seed=0xB200, bins=32, lambda_min=380.0, lambda_max=780.0)
 
 
-def batch_jobs(rank, n_jobs=0):
-    from spectral_b200.batch import prism_jobs
-    from spectral_b200.scenes import random_prism_jobs
-    return random_prism_jobs(n_jobs or BATCH["n_jobs"], seed=BATCH["seed"] + rank, bins=BATCH["bins"],
-                             lambda_min=BATCH["lambda_min"], lambda_max=BATCH["lambda_max"]), prism_jobs
+def batch_specs(rank, n_jobs=0):
+    """The batch's job dicts (spectral_b200.specs.random_prism_jobs) of `rank`."""
+    return load_specs().random_prism_jobs(n_jobs or BATCH["n_jobs"], seed=BATCH["seed"] + rank, bins=BATCH["bins"],
+                                          lambda_min=BATCH["lambda_min"], lambda_max=BATCH["lambda_max"])
 
 
-def run_cpu_batch(seconds, threads=None, rank=0, jobs=None):
+def run_cpu_batch(seconds, threads=None, rank=0, specs=None):
     """Photons/s of the CPU restatement over a bounded sample of the batch (or
-    of `jobs`).  Scenes are rendered in parallel, one host thread per scene with
-    its own film (the CPU oracle releases the GIL), taking scenes in job order
-    and the first 2^18 photons of each, until `seconds` of wall time are used."""
+    of the job dicts `specs`).  Scenes are rendered in parallel, one host thread
+    per scene with its own film (the CPU oracle releases the GIL), taking scenes
+    in job order and the first 2^18 photons of each, until `seconds` of wall
+    time are used."""
     import threading
     import oracle
-    if jobs is None:
-        specs, prism_jobs = batch_jobs(rank)
-        jobs = prism_jobs(specs)
+    if specs is None:
+        specs = batch_specs(rank)
     threads = threads or os.cpu_count() or 1
     per_job = 1 << 18
     lock = threading.Lock()
@@ -827,19 +872,12 @@ def run_cpu_batch(seconds, threads=None, rank=0, jobs=None):
         while True:
             with lock:
                 i = state["next"]
-                if i >= len(jobs) or time.perf_counter() - t0 >= seconds:
+                if i >= len(specs) or time.perf_counter() - t0 >= seconds:
                     return
                 state["next"] += 1
-            j = jobs[i]
-            o = j.opts
-            sc = oracle.OScene(bytes(j.prims)[:32 * j.n_prims], j.n_prims, bytes(j.planes)[:16 * j.n_planes],
-                               j.n_planes, bytes(j.mats)[:16 * j.n_mats], j.n_mats, 0.0)
-            cam = oracle.or_camera.from_buffer_copy(bytes(j.cam))
-            beam = oracle.or_beam.from_buffer_copy(bytes(j.beam))
-            p = oracle.vol_params(j.width, j.height, j.seed, j.weights.sigma_s, j.weights.sigma_t, j.weights.g,
-                                  j.max_dist, o.max_bounces, o.lambda_min, o.lambda_max, bins=o.bins)
-            film = np.zeros(j.width * j.height * o.bins, np.int64)
-            n = min(j.n_photons, per_job)
+            sc, cam, beam, p = oracle_prism_job(specs[i])
+            film = np.zeros(p.width * p.height * p.bins, np.int64)
+            n = min(specs[i]["n_photons"], per_job)
             oracle.lib.or_render_point(C.byref(sc.c), C.byref(cam), C.byref(beam), C.byref(p), None, 0, n, None,
                                        None, film.ctypes.data_as(C.POINTER(C.c_int64)))
             with lock:
@@ -865,7 +903,8 @@ def run_gpu_batch(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     ctx = sb.GpuContext(local_rank)
-    specs, prism_jobs = batch_jobs(rank, args.scenes)  # weak scaling: every rank renders its own scenes
+    from spectral_b200.batch import prism_jobs
+    specs = batch_specs(rank, args.scenes)  # weak scaling: every rank renders its own scenes
     jobs = prism_jobs(specs)
     b = Batch(ctx, jobs)
     tuning = b.autotune()  # untimed: picks chunk size, register bound, splat aggregation
@@ -1035,11 +1074,11 @@ def main():
             metric = "L2 atomic throughput, u32 atomicAdd (AtomicFilm synthetic splat)"
             cfg_line = {"workload": "atomics (see the GPU arm)", "splats_per_step": ATOMICS["splats"]}
         elif args.workload == "serve":
-            from spectral_b200.serve import poisson_requests
-            reqs = [r[1] for r in poisson_requests(SERVE["rate"], SERVE["seconds"], SERVE["seed"])]
-            run_cpu_batch(0.5, jobs=reqs)
+            reqs = [r[1] for r in load_specs().poisson_request_specs(SERVE["rate"], SERVE["seconds"],
+                                                                       SERVE["seed"])]
+            run_cpu_batch(0.5, specs=reqs)
             for _ in range(args.steps):
-                rate, n_s, dt, th, sc = run_cpu_batch(per_step, jobs=reqs)
+                rate, n_s, dt, th, sc = run_cpu_batch(per_step, specs=reqs)
                 rates.append((n_s, dt))
             sample = ("per step the first frame (up to 2^18 photons) of the stream's requests in arrival order, "
                       "one host thread per request, for ~%.1f s" % per_step)

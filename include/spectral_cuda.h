@@ -12,7 +12,7 @@
  *   - host buffers are caller-allocated; sizes are in elements unless stated;
  *   - no C++ exception crosses the ABI;
  *   - the library never falls back to a CPU path: without a usable sm_100 device
- *     sc_ctx_create fails with SC_E_CUDA.
+ *     sc_ctx_create fails with SC_E_NODEVICE.
  *
  * Films are 64-bit fixed point (value = count / 2^scale_log2): exact and
  * independent of the order in which splats land.
@@ -35,6 +35,7 @@ extern "C" {
 #define SC_E_LIMIT (-4)     /* scene or film exceeds a documented compile-time limit */
 #define SC_E_TIMEOUT (-5)   /* a bounded device-side wait gave up */
 #define SC_E_STATE (-6)     /* call not valid in the handle's current state */
+#define SC_E_NODEVICE (-7)  /* no usable device: none present, none at that index, or not sm_100 */
 
 /* ---- limits ------------------------------------------------------------ */
 #define SC_MAX_PRIMS 64
@@ -310,15 +311,18 @@ int sc_sensor_reduce_device(sc_ctx* ctx, uint32_t width, uint32_t height, uint32
  * the scene in `desc` (scene records in device memory, as for
  * sc_trace_photons_device) and writes the f32 XYZ image (3*w*h floats) to the
  * caller's device buffer `xyz_dev` on `stream`.  It calls no cudaMalloc /
- * cudaFree: its scratch (64-bit film, tile mask, sensor table, bin weights)
- * lives in static device arrays that every GPU loading this library holds
- * until the process exits.  Limit: (width padded to 8) * (height padded to 8)
- * * channels <= SC_NOALLOC_MAX_FILM_CELLS (16 MiB of int64 cells; e.g.
- * 640x360 XYZ, or 256x256 with 32 bins); larger films return SC_E_LIMIT.
- * The first call on a device looks up the arrays' device addresses (once per
- * device); make that first call before any stream capture.  Every call
- * clears the scratch it reads, but all calls share it: calls that overlap on
- * the GPU (other streams, other threads) race and must be serialised. */
+ * cudaFree: its scratch (64-bit film, tile mask, colour-matching table, bin
+ * weights) lives in static device arrays that every GPU loading this library
+ * holds until the process exits; the table and bin weights travel as a kernel
+ * parameter, so `tables_5x71` is read only during the call.  Estimators 0
+ * (point), 1 (isotropic) and 3 (free-flight); others return SC_E_INVALID.
+ * Limit: (width padded to 8) * (height padded to 8) * channels <=
+ * SC_NOALLOC_MAX_FILM_CELLS (16 MiB of int64 cells; e.g. 640x360 XYZ, or
+ * 256x256 with 32 bins); larger films return SC_E_LIMIT.  The first call on a
+ * device looks up the arrays' device addresses (once per device); make that
+ * first call before any stream capture.  Every call clears the scratch it
+ * reads, but all calls share it: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialised. */
 #define SC_NOALLOC_MAX_FILM_CELLS (1u << 21)
 #define SC_NOALLOC_MAX_MASK_WORDS 4096u
 int sc_trace_xyz_noalloc(const float* tables_5x71, const sc_trace_desc* desc, uint32_t photon_base,

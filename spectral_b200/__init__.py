@@ -190,11 +190,14 @@ class GpuContext:
     @classmethod
     def new(cls, device=0, tables=None):
         """GpuContext::new (spectral-gpu/src/lib.rs:29-41): the context, or None
-        when no usable sm_100 device is present (the reference's Option)."""
+        when no usable sm_100 device is present (the reference's Option).  Any
+        other failure (a bad device index or table, a CUDA error) raises."""
         try:
             return cls(device, tables)
-        except _lib.SpectralError:
-            return None
+        except _lib.SpectralError as e:
+            if e.code == _lib.SC_E_NODEVICE:
+                return None
+            raise
 
     def synchronize(self):
         check(lib.sc_ctx_synchronize(self.h))

@@ -17,6 +17,7 @@ SC_E_NOMEM = -3
 SC_E_LIMIT = -4
 SC_E_TIMEOUT = -5
 SC_E_STATE = -6
+SC_E_NODEVICE = -7
 SC_MAX_PRIMS = 64
 SC_MAX_PLANES = 256
 SC_MAX_BINS = 256

@@ -10,6 +10,7 @@ import numpy as np
 from . import _lib, Camera
 from ._lib import check, lib
 from .scenes import prism_beam, prism_planes
+from .specs import PRISM_CAMERA
 
 
 def prism_job(glass, apex_deg, incidence_deg, n_photons, width, height, sigma_s, sigma_t, g, seed, bins,
@@ -24,7 +25,8 @@ def prism_job(glass, apex_deg, incidence_deg, n_photons, width, height, sigma_s,
         j.planes[k].d = d
     j.prims[0].plane_start, j.prims[0].plane_count, j.prims[0].kind, j.prims[0].material = 0, len(planes), 1, 0
     j.mats[0].kind, j.mats[0].glass = 1, int(glass)
-    j.cam = Camera.look_at((0.6, -0.4, 6.0), (0.6, -0.4, 0.0), (0.0, 1.0, 0.0), 42.0, width / height).c
+    o, t, up, vfov = PRISM_CAMERA
+    j.cam = Camera.look_at(o, t, up, vfov, width / height).c
     j.beam = prism_beam(apex_deg, 1.0, incidence_deg, beam_width).c
     j.weights = _lib.sc_vol_weights(sigma_s, sigma_t, g)
     j.width, j.height, j.n_photons, j.seed, j.max_dist = int(width), int(height), int(n_photons), int(seed), max_dist
@@ -32,13 +34,17 @@ def prism_job(glass, apex_deg, incidence_deg, n_photons, width, height, sigma_s,
     return j
 
 
+def job_from_spec(s):
+    """sc_scene_job of one prism job dict (spectral_b200.specs)."""
+    return prism_job(s["glass"], s["apex_deg"], s["incidence_deg"], s["n_photons"], s["width"], s["height"],
+                     s["sigma_s"], s["sigma_t"], s["g"], s["seed"], s["bins"], s["lambda_min"], s["lambda_max"])
+
+
 def prism_jobs(specs):
-    """sc_scene_job array from dicts of spectral_b200.scenes.random_prism_jobs."""
+    """sc_scene_job array from dicts of spectral_b200.specs.random_prism_jobs."""
     arr = (_lib.sc_scene_job * len(specs))()
     for i, s in enumerate(specs):
-        arr[i] = prism_job(s["glass"], s["apex_deg"], s["incidence_deg"], s["n_photons"], s["width"], s["height"],
-                           s["sigma_s"], s["sigma_t"], s["g"], s["seed"], s["bins"], s["lambda_min"],
-                           s["lambda_max"])
+        arr[i] = job_from_spec(s)
     return arr
 
 

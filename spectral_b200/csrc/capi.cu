@@ -192,13 +192,19 @@ int sc_load_sensor_tables(const char* path, float* out) {
 int sc_ctx_create(int device, const float* tables, sc_ctx** out) {
     SC_GUARD_BEGIN
     SC_REQUIRE(out && tables, SC_E_INVALID, "null argument");
+    SC_REQUIRE(device >= 0, SC_E_INVALID, "device index %d", device);
     *out = nullptr;
     int count = 0;
-    SC_CUDA(cudaGetDeviceCount(&count));
-    SC_REQUIRE(device >= 0 && device < count, SC_E_INVALID, "device %d not present (%d devices)", device, count);
+    const cudaError_t ce = cudaGetDeviceCount(&count);
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        set_error("no CUDA device: %s", cudaGetErrorString(ce));
+        return SC_E_NODEVICE;
+    }
+    SC_REQUIRE(device < count, SC_E_NODEVICE, "device %d not present (%d devices)", device, count);
     cudaDeviceProp prop;
     SC_CUDA(cudaGetDeviceProperties(&prop, device));
-    SC_REQUIRE(prop.major == 10, SC_E_CUDA, "device %d is sm_%d%d; this library is built for sm_100a only",
+    SC_REQUIRE(prop.major == 10, SC_E_NODEVICE, "device %d is sm_%d%d; this library is built for sm_100a only",
                device, prop.major, prop.minor);
     sc_ctx* c = new sc_ctx();
     c->device = device;

@@ -6,8 +6,11 @@
 // never block on an allocation.  The caller passes the inputs (scene records
 // in device memory, camera, beam, weights, film options) and the output image;
 // the scratch this path needs -- the 64-bit film, its dirty-tile mask, the
-// sensor table and the bin weights -- lives in the file-scope device arrays
-// below, which every GPU that loads the library holds until the process exits.
+// colour-matching table and the bin weights -- lives in the file-scope device
+// arrays below, which every GPU that loads the library holds until the process
+// exits.  The table and the bin weights reach the device as the by-value
+// parameter of a small staging kernel, so no copy reads host memory after the
+// call has returned.
 //
 // Host code must not use the arrays' names as device addresses: on the host
 // they are stand-ins.  The addresses are looked up with cudaGetSymbolAddress
@@ -22,7 +25,7 @@ namespace {
 
 static __device__ __align__(256) unsigned long long g_noalloc_film[SC_NOALLOC_MAX_FILM_CELLS];
 static __device__ __align__(256) uint32_t g_noalloc_mask[SC_NOALLOC_MAX_MASK_WORDS];
-static __device__ __align__(256) float g_noalloc_tables[5 * sc::kTableN];
+static __device__ __align__(256) float g_noalloc_tables[3 * sc::kTableN];  // xbar, ybar, zbar
 static __device__ __align__(256) float g_noalloc_binw[3 * SC_MAX_BINS];
 
 struct ScratchPtrs {
@@ -33,6 +36,19 @@ struct ScratchPtrs {
     int sms = 0;
     bool ready = false;
 };
+
+// What a call needs from the host, carried by the staging launch itself
+// (3928 bytes of kernel parameter).  Device code names the arrays directly.
+struct NoallocStage {
+    float cmf[3 * sc::kTableN];
+    float binw[3 * SC_MAX_BINS];
+    uint32_t bins;
+};
+
+__global__ void noalloc_stage_kernel(const NoallocStage st) {
+    for (uint32_t i = threadIdx.x; i < 3u * sc::kTableN; i += blockDim.x) g_noalloc_tables[i] = st.cmf[i];
+    for (uint32_t i = threadIdx.x; i < 3u * st.bins; i += blockDim.x) g_noalloc_binw[i] = st.binw[i];
+}
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
@@ -76,9 +92,11 @@ extern "C" int sc_trace_xyz_noalloc(const float* tables_5x71, const sc_trace_des
     if (o.lambda_max == 0.0f) o.lambda_max = 730.0f;
     if (o.max_bounces == 0u) o.max_bounces = 8u;
     if (o.scale_log2 == 0u) o.scale_log2 = 32u;
-    SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min && o.scale_log2 <= 50u && o.max_bounces <= 64u &&
-                   o.estimator <= 1u,
+    SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min && o.scale_log2 <= 50u && o.max_bounces <= 64u,
                SC_E_INVALID, "bad film options");
+    SC_REQUIRE(o.estimator <= 1u || o.estimator == 3u, SC_E_INVALID,
+               "estimator %u: the allocation-free path takes the point (0), isotropic (1) and free-flight (3) "
+               "estimators", o.estimator);
     const uint32_t channels = o.bins ? o.bins : 3u;
     const uint32_t tiles_x = (d->width + 7u) / 8u, tiles_y = (d->height + 7u) / 8u;
     const uint64_t cells = (uint64_t)tiles_x * tiles_y * kTilePixels * channels;
@@ -95,10 +113,12 @@ extern "C" int sc_trace_xyz_noalloc(const float* tables_5x71, const sc_trace_des
 
     // Calls share the scratch arrays: everything read before it is written is
     // reset here, on the caller's stream.  Calls that overlap on the GPU race.
-    float binw[3 * SC_MAX_BINS];
-    if (o.bins) bin_weights(tables_5x71, o.bins, o.lambda_min, o.lambda_max, binw);
-    SC_CUDA(cudaMemcpyAsync(sp.tables, tables_5x71, 5 * kTableN * sizeof(float), cudaMemcpyHostToDevice, s));
-    if (o.bins) SC_CUDA(cudaMemcpyAsync(sp.binw, binw, 3 * o.bins * sizeof(float), cudaMemcpyHostToDevice, s));
+    NoallocStage st;
+    std::memcpy(st.cmf, tables_5x71, sizeof st.cmf);  // rows 0..2 of the sensor table
+    st.bins = o.bins;
+    if (o.bins) bin_weights(tables_5x71, o.bins, o.lambda_min, o.lambda_max, st.binw);
+    noalloc_stage_kernel<<<1, 256, 0, s>>>(st);
+    SC_CUDA(cudaGetLastError());
     SC_CUDA(cudaMemsetAsync(sp.film, 0, cells * sizeof(unsigned long long), s));
     SC_CUDA(cudaMemsetAsync(sp.mask, 0, words * sizeof(uint32_t), s));
 
@@ -116,7 +136,7 @@ extern "C" int sc_trace_xyz_noalloc(const float* tables_5x71, const sc_trace_des
     p.zbuf = d->zbuffer; p.film = sp.film; p.flags = sp.mask;
     p.prims = d->prims; p.planes = d->planes; p.mats = d->mats;
     p.n_prims = d->n_prims; p.n_planes = d->n_planes; p.n_mats = d->n_mats;
-    p.cmf = sp.tables;  // rows 0..2 of the sensor table are xbar, ybar, zbar
+    p.cmf = sp.tables;  // xbar, ybar, zbar
 
     LaunchShape shape;
     shape.block = 256; shape.aggregate = 0; shape.minb = 4;

@@ -44,4 +44,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python spectral_b200/data/make_sensor_tables.py <reference-root>")
+    main(sys.argv[1])

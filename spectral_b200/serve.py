@@ -13,8 +13,8 @@ import numpy as np
 
 from . import _lib
 from ._lib import check, lib
-from .batch import prism_job
-from .scenes import Pcg
+from . import specs
+from .batch import job_from_spec
 
 ORBIT_TARGET = (0.6, -0.4, 0.0)
 
@@ -80,28 +80,11 @@ class Server:
             pass
 
 
-def poisson_requests(rate=200.0, seconds=60.0, seed=0x5E7E, session_share=0.3, frames=(16, 128),
-                     photons=(2 ** 16, 2 ** 20), side=(128, 1024), bins=32, orbit_deg=2.0):
-    """Seeded request stream: list of (arrival_s, job, frames, orbit_deg)."""
-    g = Pcg(0, seed)
-    out, t, i = [], 0.0, 0
-    while True:
-        t += -math.log(1.0 - g.f()) / rate
-        if t >= seconds:
-            break
-        r = Pcg(i, seed ^ 0x9E3779B9)
-        glass = (0, 1, 3)[r.u32() % 3]
-        apex, inc = r.uniform(30.0, 75.0), r.uniform(30.0, 60.0)
-        n = int(round(r.log_uniform(*photons)))
-        s = int(round(r.log_uniform(*side)))
-        sig = r.uniform(0.01, 0.1)
-        sess = r.f() < session_share
-        nf = (frames[0] + r.u32() % (frames[1] - frames[0] + 1)) if sess else 1
-        job = prism_job(glass, apex, inc, n, s, s, sig, sig, 0.0, (seed * 2654435761 + i) & 0xFFFFFFFF, bins,
-                        380.0, 780.0)
-        out.append((t, job, nf, orbit_deg if sess else 0.0))
-        i += 1
-    return out
+def poisson_requests(rate=200.0, seconds=60.0, seed=0x5E7E, **kw):
+    """Seeded request stream: list of (arrival_s, job, frames, orbit_deg), the
+    request dicts of specs.poisson_request_specs as sc_scene_job records."""
+    return [(t, job_from_spec(spec), nf, orbit) for t, spec, nf, orbit in
+            specs.poisson_request_specs(rate, seconds, seed, **kw)]
 
 
 def orbit_camera(job, frame, deg, target=ORBIT_TARGET, up=(0.0, 1.0, 0.0), vfov=42.0):

@@ -1,7 +1,7 @@
 """bench.py's output contract, checked on CPU: the reference arm (the CPU
 restatement on the host cores) prints one JSON line with the keys the bench
-contract names, and the GPU arm without a GPU fails instead of falling back to
-a CPU path."""
+contract names and never loads the CUDA library, and the GPU arm without a GPU
+fails instead of falling back to a CPU path."""
 import json
 import os
 import subprocess
@@ -12,15 +12,30 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+# bench.py run in-process, then the libraries the process mapped are listed
+_WRAP = ("import runpy, sys\n"
+         "sys.argv = ['bench.py'] + sys.argv[1:]\n"
+         "rc = 0\n"
+         "try:\n"
+         "    runpy.run_path('bench.py', run_name='__main__')\n"
+         "except SystemExit as e:\n"
+         "    rc = e.code or 0\n"
+         "maps = open('/proc/self/maps').read()\n"
+         "print('MAPPED ' + ('product' if 'libspectral_cuda' in maps else 'none'))\n"
+         "sys.exit(rc)\n")
+
+
 def _run(*args):
-    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], capture_output=True, text=True,
-                          cwd=ROOT, timeout=600)
+    return subprocess.run([sys.executable, "-c", _WRAP, *args], capture_output=True, text=True, cwd=ROOT,
+                          timeout=600)
 
 
-@pytest.mark.parametrize("workload", ["prism", "tracer"])
+@pytest.mark.parametrize("workload", ["prism", "tracer", "batch", "serve"])
 def test_reference_arm_prints_one_contract_line(workload):
     r = _run("--impl", "reference", "--workload", workload, "--steps", "1", "--warmup", "1", "--cpu-seconds", "0.5")
     assert r.returncode == 0, r.stderr[-2000:]
+    # the reference arm times the CPU restatement only: the product library stays unloaded
+    assert "MAPPED none" in r.stdout, r.stdout[-500:]
     lines = [ln for ln in r.stdout.splitlines() if ln.strip().startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])

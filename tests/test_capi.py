@@ -135,6 +135,10 @@ def test_context_new_is_none_without_a_gpu():
     if torch.cuda.is_available():
         pytest.skip("a GPU is present")
     assert sb.GpuContext.new() is None  # GpuContext::new() -> None, as the reference's Option
+    # an argument error is not "no GPU": it raises
+    with pytest.raises(_lib.SpectralError) as e:
+        sb.GpuContext.new(-1)
+    assert e.value.code == _lib.SC_E_INVALID
 
 
 def test_no_gpu_means_error_not_fallback():
@@ -147,4 +151,4 @@ def test_no_gpu_means_error_not_fallback():
         pytest.skip("a GPU is present")
     with pytest.raises(_lib.SpectralError) as e:
         sb.GpuContext(0)
-    assert e.value.code in (_lib.SC_E_CUDA, _lib.SC_E_INVALID)
+    assert e.value.code == _lib.SC_E_NODEVICE
