@@ -301,6 +301,45 @@ def measured_peaks():
 # ----------------------------------------------------------------------------
 # GPU arm
 # ----------------------------------------------------------------------------
+# Photons of the film-error sample per workload (the oracle's share of the run)
+FILM_ERR_PHOTONS = {"prism": 1 << 20, "rainbow": 1 << 22, "beam": 1 << 12}
+
+
+def rel_l1(got, ref):
+    got, ref = np.asarray(got, np.float64), np.asarray(ref, np.float64)
+    den = float(np.abs(ref).sum())
+    return float(np.abs(got - ref).sum() / den) if den > 0 else 0.0
+
+
+def oracle_xyz_from_spectral(fs, bins, lambda_min, lambda_max, scale_log2=32):
+    """The library's sensor reduction on the host: spectral int64 film times the
+    bin-averaged CMF (f64), / 2^scale."""
+    import oracle
+    w = oracle.bin_weights(bins, lambda_min, lambda_max).astype(np.float64)
+    return (fs.reshape(-1, bins).astype(np.float64) @ w.T).reshape(-1) * 2.0 ** -scale_log2
+
+
+def single_scene_film_err(wl, scene, beam, cam, cfg, n, gpu_xyz):
+    """Relative L1 of a GPU XYZ image of photons [0, n) against the oracle's
+    image of the same photons (the checker; never timed)."""
+    import oracle
+    prims, np_, planes, npl, mats, nm = scene.arrays()
+    osc = oracle.OScene(bytes(prims), np_, bytes(planes), npl, bytes(mats), nm, scene.background)
+    ob = oracle.or_beam.from_buffer_copy(bytes(beam.c))
+    oc = oracle.or_camera.from_buffer_copy(bytes(cam.c))
+    W, H, B = cfg["width"], cfg["height"], cfg["bins"]
+    p = oracle.vol_params(W, H, cfg["seed"], cfg["sigma_s"], cfg["sigma_t"], cfg["g"], cfg["max_dist"],
+                          cfg["max_bounces"], cfg["lambda_min"], cfg["lambda_max"], bins=B,
+                          scale_log2=cfg.get("scale_log2", 32), estimator=cfg.get("estimator", 0))
+    if cfg.get("estimator", 0) == 2:
+        ref = oracle.render_beam(osc, oc, ob, p, 0, n)
+    else:
+        threads = max(1, min(os.cpu_count() or 1, 16 if W * H * max(B, 3) <= (1 << 24) else 4))
+        _, _, fs = oracle.render_point(osc, oc, ob, p, 0, n, f32=False, xyz=False, spec=True, threads=threads)
+        ref = oracle_xyz_from_spectral(fs, B, cfg["lambda_min"], cfg["lambda_max"], cfg.get("scale_log2", 32))
+    return rel_l1(gpu_xyz, ref)
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     import spectral_b200 as sb
@@ -390,6 +429,23 @@ def run_gpu(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     value = N * world * args.steps / (total_ms / 1e3)
+
+    # film error against the oracle (outside the timed region): a prefix of
+    # the workload's photons through the same device path, trace + reduce
+    n_chk = min(N, FILM_ERR_PHOTONS[args.workload])
+    film.zero_()
+    flags.zero_()
+    _lib.check(_lib.lib.sc_trace_photons_device(ctx.h, C.byref(desc), 0, n_chk, C.c_void_p(film.data_ptr()),
+                                                C.c_void_p(flags.data_ptr()), sp))
+    reduce()
+    torch.cuda.synchronize()
+    film_err = None
+    if rank == 0:
+        err = single_scene_film_err(args.workload, scene, beam, cam, cfg, n_chk, xyz.cpu().numpy())
+        film_err = {"value": err, "bar": 5e-3, "photons": n_chk,
+                    "sample": "photons [0, %d) of the workload (%s), GPU XYZ image vs the oracle's film%s"
+                              % (n_chk, "all of them" if n_chk == N else "a prefix",
+                                 " reduced by the bin-averaged CMF on the host" if B else "")}
 
     # end to end through the GpuPhotonFilm-shaped ABI object with host buffers
     e2e_steps = args.e2e_steps or args.steps
@@ -495,6 +551,7 @@ def run_gpu(args, rank, world, local_rank):
                             "frac": (2 * lit_bytes + 12 * W * H) / reduce_s / 1e9 / hbm,
                             "algorithmic": "read + zero the %d lit 8x8 tiles (%d B) + 12 B XYZ per pixel"
                                            % (dirty_tiles, lit_bytes)},
+        "film_err": film_err,
         "work": ({"photons": photons, "segments": segments, "march_steps": steps, "in_frame_steps": in_frame,
                   "footprint_deposits": deposits} if EST == 2 else
                  {"photons": photons, "segments": segments, "in_frame_samples": splats, "scatters": scatters}),
@@ -893,6 +950,36 @@ def run_cpu_batch(seconds, threads=None, rank=0, specs=None):
     return state["done"] / dt, state["done"], dt, threads, state["scenes"]
 
 
+def batch_film_err(ctx, specs, cap=1 << 16):
+    """Relative L1 of batch images against the oracle (the checker; never
+    timed) on a sample: every scene of the batch with its own film, traced by
+    the same batched launch on photons [0, cap) of its stream."""
+    import concurrent.futures as cf
+    import oracle
+    from spectral_b200.batch import Batch, prism_jobs
+    capped = [dict(s, n_photons=min(s["n_photons"], cap)) for s in specs]
+    b = Batch(ctx, prism_jobs(capped))
+    b.run()
+    imgs = [b.read_xyz(i) for i in range(len(capped))]
+    b.close()
+
+    def ref(s):
+        sc, cam, beam, p = oracle_prism_job(s)
+        fs = np.zeros(p.width * p.height * p.bins, np.int64)
+        oracle.lib.or_render_point(C.byref(sc.c), C.byref(cam), C.byref(beam), C.byref(p), None, 0, s["n_photons"],
+                                   None, None, fs.ctypes.data_as(C.POINTER(C.c_int64)))
+        return oracle_xyz_from_spectral(fs, s["bins"], s["lambda_min"], s["lambda_max"])
+    with cf.ThreadPoolExecutor(max(1, min(16, os.cpu_count() or 1))) as ex:  # the oracle releases the GIL
+        refs = list(ex.map(ref, capped))
+    num = sum(float(np.abs(g.astype(np.float64) - r).sum()) for g, r in zip(imgs, refs))
+    den = sum(float(np.abs(r).sum()) for r in refs)
+    worst = max(rel_l1(g, r) for g, r in zip(imgs, refs))
+    return {"value": num / den, "worst_scene": worst, "bar": 5e-3, "photons": sum(s["n_photons"] for s in capped),
+            "sample": "every scene of the batch with its film, photons [0, %d) of each through one batched launch; "
+                      "GPU XYZ images vs the oracle's spectral films reduced by the bin-averaged CMF on the host; "
+                      "value = sum |diff| / sum |ref| over all scenes" % cap}
+
+
 def run_gpu_batch(args, rank, world, local_rank):
     import torch
     import spectral_b200 as sb
@@ -995,6 +1082,7 @@ def run_gpu_batch(args, rank, world, local_rank):
     e2e_value = job_photons * e2e_steps / e2e_s
     if rank != 0:
         return None
+    film_err = batch_film_err(ctx, specs)
 
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs") or 6650.0
@@ -1027,6 +1115,7 @@ def run_gpu_batch(args, rank, world, local_rank):
                 "path": "sc_batch_update_jobs + sc_batch_run + sc_batch_read_all_xyz_async (pinned host; the "
                         "copy of a pass overlaps the next pass's tracing), all steps synchronised at the end"},
         "gpu_launches": args.steps * 3,  # per pass: batch_kernel, reduce_scan, reduce_list
+        "film_err": film_err,
         "work": stats,
         "roofline": {"bound": "hbm", "kernel": "batch_kernel + reduce_scan + reduce_list (one pass)",
                      "achieved": (stats["in_frame_samples"] * 8 + 2 * stats["dirty_tile_bytes"] +

@@ -10,7 +10,7 @@ from spectral_b200 import _lib
 from spectral_b200.batch import Batch, prism_job, prism_jobs
 from spectral_b200.scenes import random_prism_jobs
 
-from helpers import rel_l1
+from helpers import oracle_job_xyz, rel_l1
 
 pytestmark = pytest.mark.gpu
 
@@ -24,20 +24,7 @@ def small_specs(n=12, seed=0x5EED):
 
 
 def oracle_xyz(job):
-    """Spectral film of one job on the CPU, sensor-reduced like the library."""
-    prims = bytes(job.prims)[:32 * job.n_prims]
-    planes = bytes(job.planes)[:16 * job.n_planes]
-    mats = bytes(job.mats)[:16 * job.n_mats]
-    sc = oracle.OScene(prims, job.n_prims, planes, job.n_planes, mats, job.n_mats, 0.0)
-    cam = oracle.or_camera.from_buffer_copy(bytes(job.cam))
-    beam = oracle.or_beam.from_buffer_copy(bytes(job.beam))
-    o = job.opts
-    p = oracle.vol_params(job.width, job.height, job.seed, job.weights.sigma_s, job.weights.sigma_t, job.weights.g,
-                          job.max_dist, o.max_bounces, o.lambda_min, o.lambda_max, spectral=job.spectral,
-                          bins=o.bins)
-    _, _, fs = oracle.render_point(sc, cam, beam, p, 0, job.n_photons, f32=False, xyz=False, spec=True)
-    w = oracle.bin_weights(o.bins, o.lambda_min, o.lambda_max).astype(np.float64)
-    return (fs.reshape(-1, o.bins).astype(np.float64) @ w.T).reshape(-1) * 2.0 ** -32
+    return oracle_job_xyz(job)
 
 
 def test_batched_equals_plain_and_oracle(ctx):
