@@ -59,7 +59,8 @@ typedef struct { float sigma_s, sigma_t, g; } sc_vol_weights;
 typedef struct { uint32_t num_states; float lambda; uint32_t pad0, pad1; float states[18][4]; } sc_debug_photon;
 
 /* Film options beyond the reference: spectral binning and band.  Zero-initialise
- * and set what you need; zeros select the reference's defaults. */
+ * and set what you need; zeros select the reference's film (XYZ, 380-730 nm,
+ * 8 bounces, the point estimator). */
 typedef struct {
     uint32_t bins;          /* 0: XYZ film (3 channels, the reference film); N>0: N spectral bins */
     float lambda_min;       /* emission band start, nm (0 -> 380) */
@@ -72,6 +73,13 @@ typedef struct {
                                3 point estimator with free-flight sampling (no counterpart in the
                                reference): the 4 distances of a segment follow sigma_t exp(-sigma_t t)
                                restricted to the segment, weighted by 1/pdf: the same integral */
+    uint32_t haze_exact;    /* 0: haze samples (camera projection, distance, transmittance, phase) in
+                               fast f32 arithmetic, within 1e-3 relative L1 of the CPU crate's film;
+                               1: in the CPU crate's operation order (volume.rs:130-150), film cells
+                               within a few fixed-point quanta of it, slower.  Photon paths, the RNG
+                               stream and the film's integer sums are the same either way.  Photon
+                               films and the device-pointer and allocation-free traces only: batches
+                               and the server run the fast samples. */
 } sc_film_options;
 
 typedef struct sc_batch sc_batch;
@@ -400,7 +408,13 @@ typedef struct {
 } sc_server_config;
 typedef struct {
     sc_scene_job job;           /* scene, film (bins >= 1), photons per frame (n_photons), seed, camera */
-    uint32_t frames;            /* 1: a single render; F > 1: an orbit session of F frames */
+    uint32_t frames;            /* 1: a single render; F > 1: a session of F frames.  Frame f traces
+                                   photons [f*N, (f+1)*N) of the request's stream.  With orbit_deg == 0
+                                   the session is progressive (spectral-viewer/src/main.rs:395-419): the
+                                   frames add into the request's film on the device and its image is
+                                   that film over all frames so far times 1/frames (one frame's
+                                   brightness); with orbit_deg != 0 the camera moves every frame, the
+                                   film restarts, and the image is the last frame's */
     float orbit_deg;            /* camera azimuth step per frame around orbit_target (about +y) */
     float orbit_target[3];
     float orbit_up[3];
@@ -424,6 +438,12 @@ int sc_server_step(sc_server* s, uint32_t* active);
  * last two as seen by the host).  SC_E_STATE when nothing is finished. */
 int sc_server_poll(sc_server* s, uint64_t* id, float* xyz_out, size_t capacity, uint32_t* width,
                    uint32_t* height, double times[4]);
+/* The current image of an active request (3*w*h floats): for a progressive
+ * session the accumulated film so far (times 1/frames_done), for an orbit
+ * session its latest frame.  Waits for the frames already queued on the
+ * server's stream; *frames_done = frames in that image.  SC_E_STATE when the
+ * request is not on the device or has no frame yet (a finished one is polled). */
+int sc_server_peek(sc_server* s, uint64_t id, float* xyz_out, size_t capacity, uint32_t* frames_done);
 /* Drop a queued or active request (frames of it already queued still run;
  * its device memory is reused only behind them). */
 int sc_server_cancel(sc_server* s, uint64_t id);

@@ -230,11 +230,14 @@ class GpuPhotonFilm:
     ``estimator``: POINT (render_volumetric_scene_point, the GPU path of the
     reference), ISOTROPIC (render_volumetric), BEAM (render_volumetric_scene,
     spectral-core/src/volume.rs:170-329) or FREE_FLIGHT (the point estimator
-    with free-flight distances and 1/pdf weights; no reference counterpart)."""
+    with free-flight distances and 1/pdf weights; no reference counterpart).
+    ``haze_exact=True`` runs the haze samples in the CPU crate's operation
+    order (films within a few fixed-point quanta of it, slower); by default
+    they run in fast f32 arithmetic (the same photon paths and RNG stream)."""
 
     def __init__(self, ctx, scene, camera, beam, width, height, n_photons, seed, max_dist, weights=None,
                  zbuffer=None, bins=0, lambda_min=380.0, lambda_max=730.0, max_bounces=8, scale_log2=None,
-                 estimator=0):
+                 estimator=0, haze_exact=False):
         if scale_log2 is None:
             scale_log2 = 40 if estimator == BEAM else 32
         self.ctx = ctx
@@ -242,7 +245,7 @@ class GpuPhotonFilm:
         weights = weights or VolWeights()
         prims, np_, planes, npl, mats, nm = scene.arrays()
         opts = _lib.sc_film_options(int(bins), float(lambda_min), float(lambda_max), int(max_bounces),
-                                    int(scale_log2), int(estimator))
+                                    int(scale_log2), int(estimator), int(bool(haze_exact)))
         z = None
         if zbuffer is not None:
             z = np.ascontiguousarray(zbuffer, dtype=np.float32)

@@ -61,7 +61,8 @@ class sc_debug_photon(C.Structure):
 
 class sc_film_options(C.Structure):
     _fields_ = [("bins", C.c_uint32), ("lambda_min", C.c_float), ("lambda_max", C.c_float),
-                ("max_bounces", C.c_uint32), ("scale_log2", C.c_uint32), ("estimator", C.c_uint32)]
+                ("max_bounces", C.c_uint32), ("scale_log2", C.c_uint32), ("estimator", C.c_uint32),
+                ("haze_exact", C.c_uint32)]
 
 
 class sc_tracer_options(C.Structure):
@@ -196,6 +197,7 @@ PROTOTYPES = {
     "sc_server_step": (_i32, [_vp, P(_u32)]),
     "sc_server_poll": (_i32, [_vp, P(_u64), P(_f32), _sz, P(_u32), P(_u32), P(C.c_double)]),
     "sc_server_cancel": (_i32, [_vp, _u64]),
+    "sc_server_peek": (_i32, [_vp, _u64, P(_f32), _sz, P(_u32)]),
     "sc_server_stats": (_i32, [_vp, P(_u64), P(_u64), P(_u32), P(_u32), P(_u32)]),
     "sc_trace_xyz_noalloc": (_i32, [P(_f32), P(sc_trace_desc), _u32, _u32, _vp, _vp]),
     "sc_film_bytes": (_sz, [_u32, _u32, _u32]),

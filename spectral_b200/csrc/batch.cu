@@ -41,7 +41,8 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(const BatchJobDev* __r
     float* cmf = reinterpret_cast<float*>(smem);
     WarpSlot* slots = reinterpret_cast<WarpSlot*>(smem + kCmfBytes16);
     uint32_t* masks = reinterpret_cast<uint32_t*>(slots + blockDim.x / 32);
-    WarpSplitSmem* split = reinterpret_cast<WarpSplitSmem*>(masks + (blockDim.x / 32) * mask_words_max);
+    using WS = WarpSplitSmem<kBatchWarpSegs>;
+    WS* split = reinterpret_cast<WS*>(masks + (blockDim.x / 32) * mask_words_max);
     for (uint32_t i = threadIdx.x; i < 3u * kTableN; i += blockDim.x) cmf[i] = cmf_g[i];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     uint32_t* mask = masks + warp * mask_words_max;
@@ -72,8 +73,9 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(const BatchJobDev* __r
         S.prims = slot.prims; S.planes = slot.planes; S.mats = slot.mats; S.n_prims = slot.p.n_prims;
         if (SPLIT) {
             for (uint32_t b0 = 0; b0 < item.count; b0 += 32u)
-                trace_warp_split<true, AGG, FF>(slot.p, S, cmf, item.begin + b0 + lane, b0 + lane < item.count,
-                                            cur_words ? mask : nullptr, split[warp]);
+                trace_warp_split<true, AGG, FF, kBatchWarpSegs>(slot.p, S, cmf, item.begin + b0 + lane,
+                                                                b0 + lane < item.count, cur_words ? mask : nullptr,
+                                                                split[warp]);
         } else {
             for (uint32_t i = lane; i < item.count; i += 32u)
                 trace_photon<true, AGG, false, false, FF>(slot.p, S, cmf, item.begin + i, cur_words ? mask : nullptr);
@@ -103,7 +105,7 @@ static_assert(sizeof(WarpSlot) == sizeof(BatchSlotImage), "slot image layout");
 size_t batch_smem(uint32_t mask_words_max, int split, uint32_t block) {
     const size_t warps = block / 32u;
     return kCmfBytes16 + warps * sizeof(WarpSlot) + warps * mask_words_max * sizeof(uint32_t) +
-           (split ? warps * sizeof(WarpSplitSmem) : 0);
+           (split ? warps * sizeof(WarpSplitSmem<kBatchWarpSegs>) : 0);
 }
 
 int batch_occupancy(int agg, int minb, int split, uint32_t mask_words_max, uint32_t block, bool ff) {

@@ -41,6 +41,7 @@ int check_job(const sc_scene_job& j, uint32_t i) {
     SC_REQUIRE(lmax > lmin, SC_E_INVALID, "job %u band", i);
     SC_REQUIRE(j.opts.max_bounces <= 64 && j.opts.scale_log2 <= 50 && (j.opts.estimator <= 1 || j.opts.estimator == 3), SC_E_INVALID,
                "job %u options", i);
+    SC_REQUIRE(j.opts.haze_exact == 0u, SC_E_INVALID, "job %u: batches run the fast haze samples (haze_exact 0)", i);
     return SC_OK;
 }
 
@@ -112,6 +113,7 @@ struct sc_batch {
         p.flags = flags.p + flag_off[j];
         p.n_prims = J.n_prims; p.n_planes = J.n_planes; p.n_mats = J.n_mats;
         p.cmf = ctx->cmf.p;
+        set_haze_consts(p);
         return p;
     }
 

@@ -133,7 +133,7 @@ struct sc_photon_film {
         p.bins = opts.bins; p.bin_min = opts.lambda_min;
         p.bin_inv_width = opts.bins ? (float)opts.bins / p.lambda_range : 0.0f;
         p.scale = std::ldexp(1.0f, (int)opts.scale_log2);
-        p.spectral = spectral; p.estimator = opts.estimator;
+        p.spectral = spectral; p.estimator = opts.estimator; p.haze_exact = opts.haze_exact;
         p.zbuf = zbuf.p; p.film = film.p; p.flags = flags.p;
         p.prims = prims.p; p.planes = planes.p; p.mats = mats.p;
         p.n_prims = n_prims; p.n_planes = n_planes; p.n_mats = n_mats;
@@ -382,6 +382,7 @@ int sc_photon_film_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_pri
     SC_REQUIRE(o.scale_log2 <= 50u, SC_E_INVALID, "scale_log2 %u > 50", o.scale_log2);
     SC_REQUIRE(o.max_bounces <= 64u, SC_E_LIMIT, "max_bounces %u > 64", o.max_bounces);
     SC_REQUIRE(o.estimator <= 3u, SC_E_INVALID, "estimator %u", o.estimator);
+    SC_REQUIRE(o.haze_exact <= 1u, SC_E_INVALID, "haze_exact %u", o.haze_exact);
     SC_REQUIRE(o.estimator != 2u || (width < 65536u && height < 65536u), SC_E_LIMIT,
                "beam estimator films are below 65536 pixels per side");
     (void)background;
@@ -743,8 +744,8 @@ int sc_trace_photons_device(sc_ctx* ctx, const sc_trace_desc* d, uint32_t base, 
     SC_REQUIRE(d->width > 0 && d->height > 0, SC_E_INVALID, "empty film");
     sc_film_options o;
     resolve_options(&d->opts, o);
-    SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min && o.estimator <= 3u, SC_E_INVALID,
-               "bad film options");
+    SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min && o.estimator <= 3u && o.haze_exact <= 1u,
+               SC_E_INVALID, "bad film options");
     SC_REQUIRE(o.estimator != 2u || (d->width < 65536u && d->height < 65536u), SC_E_LIMIT,
                "beam estimator films are below 65536 pixels per side");
     DeviceGuard g(ctx->device);

@@ -26,14 +26,15 @@ constexpr int kReduceThreads = 256;
 struct TileRef {
     ReduceParams p;
     uint32_t tile;
-    bool valid, dirty;
+    bool valid, dirty, keep;  // keep: never drained (an accumulating film)
 };
 
-__device__ __forceinline__ TileRef tile_ref(const ReduceParams& p, uint32_t tile, bool valid) {
+__device__ __forceinline__ TileRef tile_ref(const ReduceParams& p, uint32_t tile, bool valid, bool keep = false) {
     TileRef t;
     t.p = p;
     t.tile = tile;
     t.valid = valid;
+    t.keep = keep;
     t.dirty = valid && (p.flags == nullptr || ((p.flags[tile >> 5] >> (tile & 31u)) & 1u));
     return t;
 }
@@ -129,11 +130,11 @@ __device__ __forceinline__ void reduce_walk(At at, unsigned long long* sm, doubl
     TileRef cur = at(0u);
     prefetch_tile(cur, v);
     for (uint32_t k = 0; cur.valid; ++k) {
-        stage_tile(cur, v, DRAIN, sm);
+        stage_tile(cur, v, DRAIN && !cur.keep, sm);
         __syncthreads();
         const TileRef nxt = at(k + 1u);
         prefetch_tile(nxt, v);  // in flight while this tile is reduced
-        reduce_staged(cur, DRAIN, sm, part);
+        reduce_staged(cur, DRAIN && !cur.keep, sm, part);
         __syncthreads();
         cur = nxt;
     }
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(256) reduce_scan_kernel(const FilmDesc* __rest
             if (lane == 0) base = atomicAdd(count, (uint32_t)__popc(dm));
             base = __shfl_sync(0xffffffffu, base, 0);
             if (dirty) list[base + __popc(dm & ((1u << lane) - 1u))] = DirtyTile{lo, tile};
-            if (DRAIN && lane == 0) d.flags[wl] = 0u;
+            if (DRAIN && !d.keep && lane == 0) d.flags[wl] = 0u;
         }
         // zeros for the clean tiles: 8 rows x 24 floats each, 6 coalesced stores per lane
         for (unsigned cm = __ballot_sync(0xffffffffu, valid && !dirty); cm; cm &= cm - 1u) {
@@ -219,7 +220,7 @@ __global__ void __launch_bounds__(kReduceThreads, 3) reduce_list_kernel(const Fi
             p.film = d.film; p.flags = nullptr; p.xyz = d.xyz; p.width = d.width; p.height = d.height;
             p.tiles_x = d.tiles_x; p.tiles_y = d.tiles_y; p.channels = d.channels; p.binw = d.binw;
             p.inv_scale = d.inv_scale;
-            return tile_ref(p, e.tile, true);
+            return tile_ref(p, e.tile, true, d.keep != 0u);
         },
         sm, part);
 }

@@ -27,7 +27,18 @@ struct PhotonParams {
     const float* cmf;                 // device 3x71 (xbar, ybar, zbar)
     sc_debug_photon* debug;           // debug launches only
     const uint32_t* order;            // nullable: photon i of the launch is photon_base + order[i]
+    uint32_t haze_exact;              // 1: haze samples in the CPU crate's operation order (per-photon kernel)
+    // Launch constants of the fast haze samples, filled by set_haze_consts()
+    // from the fields above just before a launch.
+    float hz_w, hz_h;                 // film width and height
+    float hz_sx, hz_sy;               // W / |horizontal|, -H / |vertical|
+    float hz_k, hz_kiso;              // sigma_s * 2^scale / 4 * HG numerator / (4 pi); isotropic estimator's
+    float hz_kexp, hz_inv_sigma_t;    // -sigma_t * log2(e), 1 / sigma_t
+    float hz_g2, hz_m2g;              // 1 + g^2, -2 g (HG denominator)
 };
+
+// Fills the hz_* launch constants of `p` (host side, before every launch).
+void set_haze_consts(PhotonParams& p);
 
 // Photon launch: CTAs of 256 threads, `grid` CTAs (grid-stride), warp
 // aggregation on/off, register bound (minimum CTAs per SM: 4 or 5), the
@@ -102,13 +113,14 @@ struct FilmDesc {
     unsigned long long* film; uint32_t* flags; float* xyz; const float* binw;
     uint32_t width, height, tiles_x, tiles_y, channels;
     uint32_t word_begin;  // prefix over films of their dirty-mask words
+    uint32_t keep;        // 1: a draining pass leaves this film and its mask as they are (it accumulates)
     double inv_scale;
 };
 struct DirtyTile { uint32_t film, tile; };
 // Two launches after zeroing `count`: a scan of every film's dirty-mask words
 // that writes zeros into the images of clean tiles and lists the dirty ones
-// (clearing their mask words when draining), then the pipelined reduction of
-// the listed tiles only.  Scratch: `list` with room for every tile of the
+// (clearing their mask words when draining, except for films marked `keep`),
+// then the pipelined reduction of the listed tiles only.  Scratch: `list` with room for every tile of the
 // films, one counter.
 cudaError_t launch_reduce_many(const FilmDesc* descs, uint32_t n_films, uint32_t total_words, bool drain,
                                uint32_t max_channels, DirtyTile* list, uint32_t* count, cudaStream_t s);

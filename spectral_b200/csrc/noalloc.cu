@@ -92,7 +92,8 @@ extern "C" int sc_trace_xyz_noalloc(const float* tables_5x71, const sc_trace_des
     if (o.lambda_max == 0.0f) o.lambda_max = 730.0f;
     if (o.max_bounces == 0u) o.max_bounces = 8u;
     if (o.scale_log2 == 0u) o.scale_log2 = 32u;
-    SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min && o.scale_log2 <= 50u && o.max_bounces <= 64u,
+    SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min && o.scale_log2 <= 50u && o.max_bounces <= 64u &&
+                   o.haze_exact <= 1u,
                SC_E_INVALID, "bad film options");
     SC_REQUIRE(o.estimator <= 1u || o.estimator == 3u, SC_E_INVALID,
                "estimator %u: the allocation-free path takes the point (0), isotropic (1) and free-flight (3) "
@@ -132,7 +133,7 @@ extern "C" int sc_trace_xyz_noalloc(const float* tables_5x71, const sc_trace_des
     p.lambda_min = o.lambda_min; p.lambda_range = o.lambda_max - o.lambda_min;
     p.bins = o.bins; p.bin_min = o.lambda_min; p.bin_inv_width = o.bins ? (float)o.bins / p.lambda_range : 0.0f;
     p.scale = std::ldexp(1.0f, (int)o.scale_log2);
-    p.spectral = d->spectral; p.estimator = o.estimator;
+    p.spectral = d->spectral; p.estimator = o.estimator; p.haze_exact = o.haze_exact;
     p.zbuf = d->zbuffer; p.film = sp.film; p.flags = sp.mask;
     p.prims = d->prims; p.planes = d->planes; p.mats = d->mats;
     p.n_prims = d->n_prims; p.n_planes = d->n_planes; p.n_mats = d->n_mats;

@@ -31,27 +31,30 @@ __host__ __device__ __forceinline__ size_t split_offset(const PhotonParams& p, u
 
 // 256 threads per CTA; MINB CTAs per SM bound the registers (4: 63 registers,
 // no spills; 5: 48 registers, a few spills, more warps in flight).
-// FF: built with free-flight sampling (estimator 3) as well.
-template <bool SPEC, int AGG, int MINB, bool SPLIT, bool FF>
+// FF: built with free-flight sampling (estimator 3) as well.  EXACT: haze
+// samples in the CPU crate's operation order (per-photon transport only).
+template <bool SPEC, int AGG, int MINB, bool SPLIT, bool FF, bool EXACT = false>
 __global__ void __launch_bounds__(256, MINB) photon_kernel(const PhotonParams p, uint32_t mask_words) {
     extern __shared__ __align__(16) unsigned char smem[];
     const float* cmf;
     uint32_t* smask;
     const SceneView S = load_scene(p, smem, &cmf, &smask, mask_words);
     if (SPLIT) {  // warp-split transport: per-warp segment buffers after the scene
-        WarpSplitSmem* ws = reinterpret_cast<WarpSplitSmem*>(smem + split_offset(p, mask_words));
+        using WS = WarpSplitSmem<kWarpSegs>;
+        WS* ws = reinterpret_cast<WS*>(smem + split_offset(p, mask_words));
         const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
         const uint32_t warps = gridDim.x * (blockDim.x >> 5);
         for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < p.photon_count; base += warps * 32u) {
             const uint32_t i = base + lane;
             const bool valid = i < p.photon_count;
             const uint32_t k = p.order && valid ? p.order[i] : i;
-            trace_warp_split<SPEC, AGG, FF>(p, S, cmf, p.photon_base + k, valid, smask, ws[warp]);
+            trace_warp_split<SPEC, AGG, FF, kWarpSegs>(p, S, cmf, p.photon_base + k, valid, smask, ws[warp]);
         }
     } else {
         const uint32_t stride = gridDim.x * blockDim.x;
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += stride)
-            trace_photon<SPEC, AGG, false, false, FF>(p, S, cmf, p.photon_base + (p.order ? p.order[i] : i), smask);
+            trace_photon<SPEC, AGG, false, false, FF, EXACT>(p, S, cmf, p.photon_base + (p.order ? p.order[i] : i),
+                                                              smask);
     }
     if (smask) {  // publish this CTA's dirty tiles
         __syncthreads();
@@ -263,7 +266,13 @@ size_t scene_smem_bytes(uint32_t n_prims, uint32_t n_planes, uint32_t n_mats) {
 using PhotonKernelFn = void (*)(const PhotonParams, uint32_t);
 
 template <bool SPLIT>
-static PhotonKernelFn photon_fn_t(bool spec, int agg, int minb, bool ff) {
+static PhotonKernelFn photon_fn_t(bool spec, int agg, int minb, bool ff, bool exact) {
+    // haze samples in the reference's operation order: per-photon transport,
+    // plain atomics, 4 CTAs per SM
+    if (exact && !SPLIT) {
+        if (ff) return spec ? photon_kernel<true, 0, 4, false, true, true> : photon_kernel<false, 0, 4, false, true, true>;
+        return spec ? photon_kernel<true, 0, 4, false, false, true> : photon_kernel<false, 0, 4, false, false, true>;
+    }
     // free-flight launches: plain atomics, 4 CTAs per SM
     if (ff) return spec ? photon_kernel<true, 0, 4, SPLIT, true> : photon_kernel<false, 0, 4, SPLIT, true>;
     if (minb >= 5) {
@@ -273,12 +282,29 @@ static PhotonKernelFn photon_fn_t(bool spec, int agg, int minb, bool ff) {
     if (spec) return agg ? photon_kernel<true, 1, 4, SPLIT, false> : photon_kernel<true, 0, 4, SPLIT, false>;
     return agg ? photon_kernel<false, 1, 4, SPLIT, false> : photon_kernel<false, 0, 4, SPLIT, false>;
 }
-static PhotonKernelFn photon_fn(const LaunchShape& s, bool spec, bool ff) {
-    return s.split ? photon_fn_t<true>(spec, s.aggregate, s.minb, ff)
-                   : photon_fn_t<false>(spec, s.aggregate, s.minb, ff);
+static PhotonKernelFn photon_fn(const LaunchShape& s, bool spec, bool ff, bool exact = false) {
+    return s.split && !exact ? photon_fn_t<true>(spec, s.aggregate, s.minb, ff, false)
+                             : photon_fn_t<false>(spec, s.aggregate, s.minb, ff, exact);
 }
 // Shared memory beyond scene + mask: one segment buffer per warp (8 warps).
-static size_t split_bytes(const LaunchShape& s) { return s.split ? 16 + 8 * sizeof(WarpSplitSmem) : 0; }
+static size_t split_bytes(const LaunchShape& s) {
+    return s.split ? 16 + 8 * sizeof(WarpSplitSmem<kWarpSegs>) : 0;
+}
+
+void set_haze_consts(PhotonParams& p) {
+    const double pi = 3.14159265358979323846;
+    const double g = p.g;
+    p.hz_w = (float)p.width;
+    p.hz_h = (float)p.height;
+    p.hz_sx = (float)((double)p.width / (double)p.proj.vw);
+    p.hz_sy = (float)(-(double)p.height / (double)p.proj.vh);
+    p.hz_k = (float)((double)p.sigma_s * (double)p.scale * 0.25 * (1.0 - g * g) / (4.0 * pi));
+    p.hz_kiso = (float)((double)p.sigma_s * (double)p.scale * 0.25 / (4.0 * pi));
+    p.hz_kexp = (float)(-(double)p.sigma_t * 1.4426950408889634);  // -sigma_t log2(e)
+    p.hz_inv_sigma_t = p.sigma_t > 0.0f ? (float)(1.0 / (double)p.sigma_t) : 0.0f;
+    p.hz_g2 = (float)(1.0 + g * g);
+    p.hz_m2g = (float)(-2.0 * g);
+}
 
 int occupancy_blocks(const void* fn, int block, size_t smem) {
     static std::mutex mu;
@@ -367,14 +393,20 @@ cudaError_t launch_photons(const PhotonParams& p, const LaunchShape& shape, cuda
     return e != cudaSuccess ? e : f;
 }
 
-static cudaError_t launch_photons_in(const PhotonParams& p, const LaunchShape& shape, cudaStream_t s) {
+static cudaError_t launch_photons_in(const PhotonParams& p0, const LaunchShape& shape, cudaStream_t s) {
+    PhotonParams p = p0;
+    set_haze_consts(p);
+    const bool exact = p.haze_exact != 0u;
     const uint32_t mw = photon_mask_words(p);
-    const size_t smem = shape.split ? split_offset(p, mw) + 8 * sizeof(WarpSplitSmem)
-                                    : scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats) + mw * sizeof(uint32_t);
+    const size_t smem = shape.split && !exact
+                            ? split_offset(p, mw) + 8 * sizeof(WarpSplitSmem<kWarpSegs>)
+                            : scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats) + mw * sizeof(uint32_t);
     const bool spec = p.channels != 3u || p.bins != 0u;
     const uint32_t need = (p.photon_count + 255u) / 256u;
     const uint32_t grid = need < shape.grid ? need : shape.grid;
-    photon_fn(shape, spec, free_flight(p))<<<grid, 256, smem, s>>>(p, mw);
+    const PhotonKernelFn fn = photon_fn(shape, spec, free_flight(p), exact);
+    if (smem > 48 * 1024) occupancy_blocks(reinterpret_cast<const void*>(fn), 256, smem);  // raises its limit once
+    fn<<<grid, 256, smem, s>>>(p, mw);
     return cudaGetLastError();
 }
 
@@ -385,8 +417,10 @@ cudaError_t launch_photon_debug(const PhotonParams& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_photon_count(const PhotonParams& p, unsigned long long* out, uint32_t grid, cudaStream_t s) {
-    if (p.photon_count == 0) return cudaSuccess;
+cudaError_t launch_photon_count(const PhotonParams& p0, unsigned long long* out, uint32_t grid, cudaStream_t s) {
+    if (p0.photon_count == 0) return cudaSuccess;
+    PhotonParams p = p0;
+    set_haze_consts(p);
     const size_t smem = scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats);
     const uint32_t need = (p.photon_count + 255) / 256;
     photon_count_kernel<<<need < grid ? need : grid, 256, smem, s>>>(p, out);

@@ -61,9 +61,10 @@ __device__ __forceinline__ void mark_tile(const PhotonParams& p, uint32_t* smask
 
 // Deposit one haze sample.  AGG=1 merges lanes of the warp that hit the same
 // film cell before issuing the atomic.
+// `scale`: the film's 2^k, or 1 when `contrib` carries it already.
 template <bool SPEC, int AGG>
 __device__ __forceinline__ void deposit(const PhotonParams& p, uint32_t* smask, bool ok, uint32_t px, uint32_t py,
-                                        float contrib, float cx, float cy, float cz, uint32_t bin) {
+                                        float contrib, float cx, float cy, float cz, uint32_t bin, float scale) {
     size_t cell = 0;
     uint32_t tile = 0;
     unsigned long long v0 = 0, v1 = 0, v2 = 0;
@@ -71,11 +72,11 @@ __device__ __forceinline__ void deposit(const PhotonParams& p, uint32_t* smask, 
         tile = film_tile(px, py, p.tiles_x);
         cell = film_cell(px, py, p.tiles_x, p.channels) + (SPEC ? bin : 0u);
         if (SPEC) {
-            v0 = to_fixed(contrib, p.scale);
+            v0 = to_fixed(contrib, scale);
         } else {
-            v0 = to_fixed(cx * contrib, p.scale);
-            v1 = to_fixed(cy * contrib, p.scale);
-            v2 = to_fixed(cz * contrib, p.scale);
+            v0 = to_fixed(cx * contrib, scale);
+            v1 = to_fixed(cy * contrib, scale);
+            v2 = to_fixed(cz * contrib, scale);
         }
     }
     if (AGG == 0) {
@@ -170,6 +171,109 @@ __device__ __forceinline__ bool haze_sample(const PhotonParams& p, f3 o, f3 d, f
     return ok;
 }
 
+// ---------------------------------------------------------------------------
+// Fast haze samples.  Only the transport (intersection, Fresnel / refract /
+// TIR, Sellmeier) decides a photon's path; the haze samples only weight film
+// deposits, so they need the film's accuracy (0.5 % relative L1), not the CPU
+// crate's operation order.  Along a segment q(t) = o + d t, with D = o - o_cam
+// and the camera basis (u, v, w, |horizontal|, |vertical|):
+//   depth  c(t)     = D.w + (d.w) t                  (in front: c < -1e-6)
+//   column s(t) * W = W/2 + (a0 + a1 t) / -c(t),  a = (D.u, d.u) * W / |horizontal|
+//   row (1-t') * H  = H/2 + (b0 + b1 t) / -c(t),  b = (D.v, d.v) * -H / |vertical|
+//   distance^2      = h2 + (s0 + s1 t)^2,  s1 = |d|, s0 = -|d| t*, t* = -D.d / |d|^2,
+//                     h2 = |D + d t*|^2 (squared distance of closest approach: a sum of
+//                     two non-negative terms, so no cancellation near the camera)
+//   d . (to camera) / distance = -s1 (s0 + s1 t) / distance
+// so a sample costs three fused multiply-adds for the projection, one
+// reciprocal, one reciprocal square root and one exp2 (PTX approximations),
+// and the constant factor k = power sigma_s seg / 4 * 2^scale * HG numerator
+// is formed once per segment.  The HG denominator power 1.5 is r^3 with
+// r = rsqrt(max(1 + g^2 - 2 g cos, 1e-6)).
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Per-segment constants.  `segs` is seg * 2^-24 for the uniform estimator
+// (t = (draw >> 8) * segs, the same product the reference rounds) and
+// expm1(-sigma_t seg) for free-flight distances.
+struct HazeSeg { float c0, c1, a0, a1, b0, b1, s0, s1, h2, k, segs; };
+
+template <bool FF>
+__device__ __forceinline__ HazeSeg haze_setup(const PhotonParams& p, f3 o, f3 d, float seg, float power) {
+    const Proj& P = p.proj;
+    const f3 D = sub(o, P.o);
+    HazeSeg h;
+    h.c0 = dot(D, P.w);
+    h.c1 = dot(d, P.w);
+    h.a0 = dot(D, P.u) * p.hz_sx;
+    h.a1 = dot(d, P.u) * p.hz_sx;
+    h.b0 = dot(D, P.v) * p.hz_sy;
+    h.b1 = dot(d, P.v) * p.hz_sy;
+    const float e2 = dot(d, d);
+    const float tstar = -dot(D, d) / e2;
+    const f3 m = add(D, mul(d, tstar));
+    h.h2 = dot(m, m);
+    h.s1 = sqrtf(e2);
+    h.s0 = -h.s1 * tstar;
+    if (FF) {
+        const float em = expm1f(-p.sigma_t * seg);
+        h.segs = em;
+        h.k = power * (-em * p.hz_inv_sigma_t) * p.hz_k;  // 1/pdf numerator (1 - e^-sigma_t seg) / sigma_t
+    } else {
+        h.segs = seg * (1.0f / 16777216.0f);
+        h.k = power * seg * (p.estimator == 1u ? p.hz_kiso : p.hz_k);
+    }
+    return h;
+}
+
+// One haze sample of a segment from its 24-bit draw; returns whether it lands
+// in frame (and is not occluded), with its pixel and its scaled weight.
+template <bool FF>
+__device__ __forceinline__ bool haze_fast(const PhotonParams& p, const HazeSeg& h, uint32_t draw24, uint32_t& px,
+                                          uint32_t& py, float& contrib) {
+    float t;
+    if (FF) t = -log1pf((float)draw24 * (1.0f / 16777216.0f) * h.segs) * p.hz_inv_sigma_t;
+    else t = (float)draw24 * h.segs;
+    const float c = __fmaf_rn(h.c1, t, h.c0);
+    const float rc = rcp_approx(-c);
+    const float x = __fmaf_rn(__fmaf_rn(h.a1, t, h.a0), rc, 0.5f * p.hz_w);
+    const float y = __fmaf_rn(__fmaf_rn(h.b1, t, h.b0), rc, 0.5f * p.hz_h);
+    contrib = 0.0f;
+    px = py = 0u;
+    if (!(c < -1e-6f && x >= 0.0f && x < p.hz_w && y > 0.0f && y <= p.hz_h)) return false;
+    px = min((uint32_t)x, p.width - 1u);
+    py = min((uint32_t)y, p.height - 1u);
+    if (!FF && p.estimator == 1u) {  // isotropic estimator: no transmittance, no 1/d^2, no z-test
+        contrib = h.k;
+        return true;
+    }
+    const float q = __fmaf_rn(h.s1, t, h.s0);
+    const float dd2 = fmaxf(__fmaf_rn(q, q, h.h2), 1e-6f);
+    const float r = rsqrt_approx(dd2);
+    const float dd = dd2 * r;
+    if (p.zbuf && !(dd < p.zbuf[py * p.width + px])) return false;
+    float w = h.k * ex2_approx(p.hz_kexp * (FF ? dd - t : dd)) * (r * r);
+    if (p.g != 0.0f) {
+        const float den = fmaxf(__fmaf_rn(p.hz_m2g, -(h.s1 * q) * r, p.hz_g2), 1e-6f);
+        const float rr = rsqrt_approx(den);
+        w *= rr * rr * rr;
+    }
+    contrib = w;
+    return true;
+}
+
 // Photon-level splat payload: CMF of the photon's wavelength (XYZ film) or its bin.
 __device__ __forceinline__ void photon_payload(const PhotonParams& p, const float* cmf, float lambda, float& cx,
                                                float& cy, float& cz, uint32_t& bin, bool spec) {
@@ -184,7 +288,9 @@ __device__ __forceinline__ void photon_payload(const PhotonParams& p, const floa
     }
 }
 
-template <bool SPEC, int AGG, bool DEBUG, bool COUNT = false, bool FFOK = true>
+// EXACT: haze samples in the CPU crate's operation order (haze_sample);
+// otherwise the fast haze samples, as the warp-split transport runs them.
+template <bool SPEC, int AGG, bool DEBUG, bool COUNT = false, bool FFOK = true, bool EXACT = false>
 __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneView& S, const float* cmf,
                                              uint32_t idx, uint32_t* smask, PhotonCounts* cnt = nullptr) {
     Rng r = Rng::make(idx, p.seed);
@@ -213,18 +319,33 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
         const bool any = scene_hit(S, o, d, h, mi);
         const float seg = any ? h.t : p.max_dist;
         if (COUNT) ++cnt->segments;
+        const bool ff = FFOK && free_flight(p);
+        if (DEBUG) {
+            r.state += 4u;  // the segment's 4 distance draws
+        } else if (EXACT) {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const bool ff = FFOK && free_flight(p);
-            const float u = r.f32();
-            const float dist = ff ? haze_distance<true>(p, u, seg) : haze_distance<false>(p, u, seg);
-            if (DEBUG) continue;
-            uint32_t px, py;
-            float contrib;
-            const bool ok = ff ? haze_sample<true>(p, o, d, dist, seg, power, px, py, contrib)
-                               : haze_sample<false>(p, o, d, dist, seg, power, px, py, contrib);
-            if (COUNT) { if (ok) ++cnt->splats; continue; }
-            deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, cx, cy, cz, bin);
+            for (int k = 0; k < 4; ++k) {
+                const float u = r.f32();
+                const float dist = ff ? haze_distance<true>(p, u, seg) : haze_distance<false>(p, u, seg);
+                uint32_t px, py;
+                float contrib;
+                const bool ok = ff ? haze_sample<true>(p, o, d, dist, seg, power, px, py, contrib)
+                                   : haze_sample<false>(p, o, d, dist, seg, power, px, py, contrib);
+                if (COUNT) { if (ok) ++cnt->splats; continue; }
+                deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, cx, cy, cz, bin, p.scale);
+            }
+        } else {
+            const HazeSeg hz = ff ? haze_setup<true>(p, o, d, seg, power) : haze_setup<false>(p, o, d, seg, power);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t draw24 = r.u32() >> 8;
+                uint32_t px, py;
+                float contrib;
+                const bool ok = ff ? haze_fast<true>(p, hz, draw24, px, py, contrib)
+                                   : haze_fast<false>(p, hz, draw24, px, py, contrib);
+                if (COUNT) { if (ok) ++cnt->splats; continue; }
+                deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, cx, cy, cz, bin, 1.0f);
+            }
         }
         if (!any) break;
         const sc_material& m = S.mats[mi];
@@ -256,32 +377,48 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
 // different numbers of segments.  PCG is counter based: sample k of a segment
 // uses draw pcg32(state_before + k + 1), exactly the draw the per-photon loop
 // makes, so paths and films are bit-identical to trace_photon's.
-struct SegRec { f3 o, d; float seg, power; uint32_t rng, lane; };
-constexpr uint32_t kWarpSegs = 64;
-struct alignas(16) WarpSplitSmem {
-    SegRec seg[kWarpSegs];
-    float4 payload[32];  // per lane: CMF x, y, z of the photon (XYZ film) or its bin in .w
+// Segment record: the fast haze constants of the segment, the RNG state
+// before its 4 distance draws, and the photon's bin (spectral films) or lane
+// (XYZ films, whose CMF payload sits in the warp's payload table).
+struct alignas(16) SegRec {
+    HazeSeg hz;
+    uint32_t rng, tag;
+    uint32_t pad[3];
 };
-static_assert(sizeof(SegRec) == 40, "segment record layout");
+static_assert(sizeof(SegRec) == 64, "segment record layout");
+template <uint32_t SEGS>
+struct alignas(16) WarpSplitSmem {
+    SegRec seg[SEGS];
+    float4 payload[32];  // per lane: CMF x, y, z of the photon (XYZ film)
+};
+// Segments buffered per warp: 64 in the plain photon kernel, 48 in the batch
+// kernel (whose warps also hold a job slot and a dirty mask).
+constexpr uint32_t kWarpSegs = 64;
+constexpr uint32_t kBatchWarpSegs = 48;
 
-template <bool SPEC, int AGG, bool FF>
-__device__ __forceinline__ void flush_loop(const PhotonParams& p, WarpSplitSmem& ws, uint32_t total, uint32_t* smask,
-                                           uint32_t lane) {
+template <bool SPEC, int AGG, bool FF, uint32_t SEGS>
+__device__ __forceinline__ void flush_loop(const PhotonParams& p, WarpSplitSmem<SEGS>& ws, uint32_t total,
+                                           uint32_t* smask, uint32_t lane) {
     for (uint32_t t = lane; t < total; t += 32u) {
-        const SegRec R = ws.seg[t >> 2];
-        const float u = (float)(pcg32(R.rng + (t & 3u) + 1u) >> 8) * (1.0f / 16777216.0f);
+        const SegRec& R = ws.seg[t >> 2];
+        const HazeSeg hz = R.hz;
+        const uint32_t draw24 = pcg32(R.rng + (t & 3u) + 1u) >> 8;
         uint32_t px, py;
         float contrib;
-        const bool ok = haze_sample<FF>(p, R.o, R.d, haze_distance<FF>(p, u, R.seg), R.seg, R.power, px, py, contrib);
-        const float4 pl = ws.payload[R.lane];
-        deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, pl.x, pl.y, pl.z, __float_as_uint(pl.w));
+        const bool ok = haze_fast<FF>(p, hz, draw24, px, py, contrib);
+        if (SPEC) {
+            deposit<true, AGG>(p, smask, ok, px, py, contrib, 0.f, 0.f, 0.f, R.tag, 1.0f);
+        } else {
+            const float4 pl = ws.payload[R.tag];
+            deposit<false, AGG>(p, smask, ok, px, py, contrib, pl.x, pl.y, pl.z, 0u, 1.0f);
+        }
     }
 }
 
 // The estimator is fixed per job: one uniform branch picks the loop.
-template <bool SPEC, int AGG, bool FFOK>
-__device__ __forceinline__ void flush_segments(const PhotonParams& p, WarpSplitSmem& ws, uint32_t n, uint32_t* smask,
-                                               uint32_t lane) {
+template <bool SPEC, int AGG, bool FFOK, uint32_t SEGS>
+__device__ __forceinline__ void flush_segments(const PhotonParams& p, WarpSplitSmem<SEGS>& ws, uint32_t n,
+                                               uint32_t* smask, uint32_t lane) {
     __syncwarp();
     if (FFOK && free_flight(p)) flush_loop<SPEC, AGG, true>(p, ws, 4u * n, smask, lane);
     else flush_loop<SPEC, AGG, false>(p, ws, 4u * n, smask, lane);
@@ -290,14 +427,15 @@ __device__ __forceinline__ void flush_segments(const PhotonParams& p, WarpSplitS
 
 // All 32 lanes of the warp must call this together; lanes without a photon pass
 // valid = false.
-template <bool SPEC, int AGG, bool FFOK>
+template <bool SPEC, int AGG, bool FFOK, uint32_t SEGS>
 __device__ __forceinline__ void trace_warp_split(const PhotonParams& p, const SceneView& S, const float* cmf,
-                                                 uint32_t idx, bool valid, uint32_t* smask, WarpSplitSmem& ws) {
+                                                 uint32_t idx, bool valid, uint32_t* smask, WarpSplitSmem<SEGS>& ws) {
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
     Rng r = Rng::make(idx, p.seed);
     f3 o = mk(0.f, 0.f, 0.f), d = p.bdir;
     float lambda = 0.0f, power = 1.0f;
+    uint32_t tag = lane;  // spectral films: the photon's bin
     if (valid) {
         const float r1 = r.f32();
         const float r2 = r.f32();
@@ -306,8 +444,10 @@ __device__ __forceinline__ void trace_warp_split(const PhotonParams& p, const Sc
         float cx = 0.f, cy = 0.f, cz = 0.f;
         uint32_t bin = 0;
         photon_payload(p, cmf, lambda, cx, cy, cz, bin, SPEC);
-        ws.payload[lane] = make_float4(cx, cy, cz, __uint_as_float(bin));
+        if (SPEC) tag = bin;
+        else ws.payload[lane] = make_float4(cx, cy, cz, 0.0f);
     }
+    const bool ff = FFOK && free_flight(p);
     bool alive = valid;
     uint32_t n = 0;  // buffered segments, the same in every lane
     uint32_t n_glass = 0xFFFFFFFFu;
@@ -317,8 +457,8 @@ __device__ __forceinline__ void trace_warp_split(const PhotonParams& p, const Sc
         const uint32_t cnt = __popc(m);
         // one flush site (keeps the inlined haze code single): when this bounce's
         // segments do not fit, and once when every photon is done
-        if (n + cnt > kWarpSegs || (m == 0u && n)) {
-            flush_segments<SPEC, AGG, FFOK>(p, ws, n, smask, lane);
+        if (n + cnt > SEGS || (m == 0u && n)) {
+            flush_segments<SPEC, AGG, FFOK, SEGS>(p, ws, n, smask, lane);
             n = 0;
         }
         if (m == 0u) break;
@@ -332,7 +472,9 @@ __device__ __forceinline__ void trace_warp_split(const PhotonParams& p, const Sc
         }
         if (alive) {
             SegRec& R = ws.seg[n + __popc(m & below)];
-            R.o = o; R.d = d; R.seg = seg; R.power = power; R.rng = r.state; R.lane = lane;
+            R.hz = ff ? haze_setup<true>(p, o, d, seg, power) : haze_setup<false>(p, o, d, seg, power);
+            R.rng = r.state;
+            R.tag = tag;
             r.state += 4u;  // this segment's 4 distance draws, made by the flush
             if (!any) {
                 alive = false;

@@ -22,7 +22,13 @@
 //   state of a request is its photon index: frame f traces photons
 //   [f*N, (f+1)*N) of the request's own stream, so a request's result does not
 //   depend on what else is in the batch.
-// * Orbit sessions move the camera by a fixed azimuth step around their target
+// * Progressive sessions (several frames, a fixed camera) add every frame into
+//   the request's resident film, as the reference viewer accumulates frame
+//   after frame (spectral-viewer/src/main.rs:395-419): that film is never
+//   drained, and each frame's image is the accumulated film over the frames so
+//   far, scaled by 1 / frames (the viewer's normalisation by total photons, at
+//   the per-frame photon count), so it keeps the brightness of one frame.
+//   Orbit sessions move the camera by a fixed azimuth step around their target
 //   every frame (the film restarts each frame, as the reference viewer resets
 //   its accumulation on a camera move); the last frame's image is returned.
 #include <algorithm>
@@ -256,6 +262,9 @@ struct sc_server {
         q->image = nullptr;
     }
 
+    // Several frames on a fixed camera: the frames accumulate.
+    static bool progressive(const Request* q) { return q->r.frames > 1u && q->r.orbit_deg == 0.0f; }
+
     sc_camera frame_camera(const Request* q) const {
         const sc_request& r = q->r;
         if (r.orbit_deg == 0.0f || q->frame == 0) return r.job.cam;
@@ -372,6 +381,7 @@ struct sc_server {
             p.film = film_ptr(q); p.flags = flags_ptr(q);
             p.n_prims = J.n_prims; p.n_planes = J.n_planes; p.n_mats = J.n_mats;
             p.cmf = ctx->cmf.p;
+            set_haze_consts(p);
             BatchJobDev& d = h->jobs[i];
             std::memset(&d, 0, sizeof d);
             d.slot_image.p = p;
@@ -384,7 +394,9 @@ struct sc_server {
             fd.film = p.film; fd.flags = p.flags; fd.xyz = xyz_ptr(q); fd.binw = q->binw;
             fd.width = J.width; fd.height = J.height; fd.tiles_x = q->tiles_x; fd.tiles_y = q->tiles_y;
             fd.channels = J.opts.bins; fd.word_begin = words;
-            fd.inv_scale = std::ldexp(1.0, -(int)(J.opts.scale_log2 ? J.opts.scale_log2 : 32u));
+            fd.keep = progressive(q) ? 1u : 0u;
+            fd.inv_scale = std::ldexp(1.0, -(int)(J.opts.scale_log2 ? J.opts.scale_log2 : 32u)) /
+                           (progressive(q) ? (double)(q->frame + 1u) : 1.0);
             tiles += q->tiles_x * q->tiles_y;
             words += q->words;
             maxc = std::max(maxc, J.opts.bins);
@@ -525,6 +537,7 @@ int sc_server_submit(sc_server* s, const sc_request* r, uint64_t* id) {
     SC_REQUIRE(j.opts.estimator <= 1u || j.opts.estimator == 3u, SC_E_INVALID,
                "estimator %u: requests take the point, isotropic or free-flight estimator", j.opts.estimator);
     SC_REQUIRE(j.opts.lambda_max > j.opts.lambda_min && j.opts.lambda_min > 0.0f, SC_E_INVALID, "band");
+    SC_REQUIRE(j.opts.haze_exact == 0u, SC_E_INVALID, "requests run the fast haze samples (haze_exact 0)");
     SC_REQUIRE(r->frames >= 1 && (uint64_t)r->frames * j.n_photons <= 0xFFFFFFFFull, SC_E_INVALID,
                "frames x photons must fit 32-bit photon indices");
     Request* q = new Request();
@@ -573,6 +586,27 @@ int sc_server_poll(sc_server* s, uint64_t* id, float* xyz_out, size_t capacity, 
     s->finished.pop_front();
     delete q;
     return SC_OK;
+    SC_GUARD_END
+}
+
+int sc_server_peek(sc_server* s, uint64_t id, float* xyz_out, size_t capacity, uint32_t* frames_done) {
+    SC_GUARD_BEGIN
+    SERVER_LOCK(s);
+    SC_REQUIRE(xyz_out, SC_E_INVALID, "null output");
+    Request* q = nullptr;
+    for (Request* a : s->active)
+        if (a->id == id) q = a;
+    if (!q || q->frame == 0) {
+        set_error("request %llu has no frame on the device (queued, finished or unknown)", (unsigned long long)id);
+        return SC_E_STATE;
+    }
+    const size_t nf = 3ull * q->r.job.width * q->r.job.height;
+    SC_REQUIRE(capacity >= nf, SC_E_INVALID, "output holds %zu floats, need %zu", capacity, nf);
+    // behind every queued frame of the request: its image after q->frame frames
+    SC_CUDA(cudaMemcpyAsync(xyz_out, s->xyz_ptr(q), nf * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    SC_CUDA(cudaStreamSynchronize(s->stream));
+    if (frames_done) *frames_done = q->frame;
+    return s->collect(false);
     SC_GUARD_END
 }
 

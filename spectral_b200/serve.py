@@ -28,6 +28,9 @@ class Server:
         self._buf = None
 
     def submit(self, job, frames=1, orbit_deg=0.0, target=ORBIT_TARGET, up=(0.0, 1.0, 0.0), vfov=42.0):
+        """Queue a render of `frames` frames of job.n_photons photons each:
+        with orbit_deg == 0 the frames accumulate (a progressive session), else
+        the camera orbits by orbit_deg per frame and the last frame is kept."""
         r = _lib.sc_request()
         r.job, r.frames, r.orbit_deg = job, int(frames), float(orbit_deg)
         r.orbit_target, r.orbit_up, r.vfov_deg = _lib.F3(*target), _lib.F3(*up), float(vfov)
@@ -57,6 +60,21 @@ class Server:
         check(rc)
         n = self._dims.pop(rid.value, 0)
         return rid.value, (buf[:n].copy() if cap else None), tuple(times)
+
+    def peek(self, rid):
+        """(frames done, current XYZ image) of an active request, or None when
+        it has no frame on the device: a progressive session's accumulated
+        image so far, an orbit session's latest frame."""
+        n = self._dims.get(rid)
+        if n is None:
+            return None
+        out = np.empty(n, np.float32)
+        fr = C.c_uint32()
+        rc = lib.sc_server_peek(self.h, int(rid), out.ctypes.data_as(C.POINTER(C.c_float)), n, C.byref(fr))
+        if rc == _lib.SC_E_STATE:
+            return None
+        check(rc)
+        return fr.value, out
 
     def cancel(self, rid):
         check(lib.sc_server_cancel(self.h, int(rid)))

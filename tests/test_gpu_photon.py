@@ -7,6 +7,11 @@ tolerances of this library:
   * per-photon states: exact bounce count, origin/direction within PATH_TOL
     (the reference asserts 1e-4, its README claims ~1e-6);
   * films: relative L1 within FILM_TOL of the oracle (reference gate 5 %).
+Films traced with haze_exact=True (haze samples in the CPU crate's operation
+order) must also agree with the oracle's int64 films cell by cell to a few
+fixed-point quanta (only expf/powf last bits differ); films with the default
+fast haze samples must stay within FAST_TOL of them (rare pixel-boundary
+moves of single samples and ulp-level weight differences).
 """
 import ctypes as C
 import json
@@ -25,6 +30,7 @@ pytestmark = pytest.mark.gpu
 
 PATH_TOL = 1e-6      # per-photon origin / direction (the required bound)
 FILM_TOL = 5e-3      # relative L1 of films / XYZ images (the required bound, 0.5 %)
+FAST_TOL = 2e-3      # relative L1 of fast-haze films against the oracle
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
@@ -128,7 +134,7 @@ def dsotm_film(ctx, w, h, n, seed, **kw):
 def test_vol_diff_gate(ctx):
     w, h, n, seed = 200, 200, 200_000, 7
     zbuf = np.full(w * h, np.inf, np.float32)
-    film, scene, beam, cam = dsotm_film(ctx, w, h, n, seed, zbuffer=zbuf)
+    film, scene, beam, cam = dsotm_film(ctx, w, h, n, seed, zbuffer=zbuf, haze_exact=True)
     film.trace_and_resolve(n, seed)
     gpu = film.accum()
     raw = film.read_raw().reshape(-1)
@@ -143,14 +149,23 @@ def test_vol_diff_gate(ctx):
     # the 64-bit films agree to a few quanta (expf/powf last-bit differences only)
     assert diff.max() <= 64 and rel_l1(raw, fx) < 1e-6
     assert ((gpu > 0).reshape(-1, 3).any(1) == (img > 0).reshape(-1, 3).any(1)).mean() > 0.999
+    # the default fast haze samples: the same photons, within FAST_TOL
+    fast, *_ = dsotm_film(ctx, w, h, n, seed, zbuffer=zbuf)
+    fast.trace_and_resolve(n, seed)
+    lf = rel_l1(fast.read_raw().reshape(-1), fx)
+    print("vol_diff_gate fast haze: rel L1 %.3e" % lf)
+    assert lf < FAST_TOL and energy_delta(fast.accum(), img) < FAST_TOL
 
 
 def test_film_against_golden_fixture(ctx):
     g = np.load(os.path.join(GOLDEN, "dsotm_film_64.npz"))
-    film, *_ = dsotm_film(ctx, 64, 64, 4096, 7)
+    film, *_ = dsotm_film(ctx, 64, 64, 4096, 7, haze_exact=True)
     film.trace_and_resolve(4096, 7)
     raw = film.read_raw().reshape(-1)
     assert rel_l1(raw, g["film_xyz"]) < 1e-6 and rel_l1(film.accum(), g["img_f32"]) < FILM_TOL
+    fast, *_ = dsotm_film(ctx, 64, 64, 4096, 7)
+    fast.trace_and_resolve(4096, 7)
+    assert rel_l1(fast.read_raw().reshape(-1), g["film_xyz"]) < FAST_TOL
 
 
 def test_forward_gpu_determinism_and_chunking(ctx):
@@ -210,7 +225,7 @@ def test_free_flight_estimator_matches_oracle(ctx, bins):
     pixel; films agree far inside the 0.5 % bar."""
     w, h, n, seed = 80, 64, 60_000, 19
     film, scene, beam, cam = dsotm_film(ctx, w, h, n, seed, bins=bins, weights=sb.VolWeights(0.5, 0.3, 0.5),
-                                        estimator=sb.FREE_FLIGHT)
+                                        estimator=sb.FREE_FLIGHT, haze_exact=True)
     film.trace_and_resolve(n, seed)
     p = oracle.vol_params(w, h, seed, 0.5, 0.3, 0.5, 14.0, bins=bins, estimator=3)
     img, fx, fs = oracle.render_point(oscene(scene), ocam(cam), obeam(beam), p, 0, n, f32=False, xyz=not bins,
@@ -218,6 +233,10 @@ def test_free_flight_estimator_matches_oracle(ctx, bins):
     ref = (fs if bins else fx).reshape(-1)
     raw = film.read_raw().reshape(-1)
     assert ref.sum() > 0 and rel_l1(raw, ref) < 1e-4
+    fast, *_ = dsotm_film(ctx, w, h, n, seed, bins=bins, weights=sb.VolWeights(0.5, 0.3, 0.5),
+                          estimator=sb.FREE_FLIGHT)
+    fast.trace_and_resolve(n, seed)
+    assert rel_l1(fast.read_raw().reshape(-1), ref) < FAST_TOL
     uni, *_ = dsotm_film(ctx, w, h, n, seed, bins=bins, weights=sb.VolWeights(0.5, 0.3, 0.5))
     uni.trace_and_resolve(n, seed)
     assert raw.tobytes() != uni.read_raw().tobytes()  # a different estimator of the same image
@@ -226,7 +245,8 @@ def test_free_flight_estimator_matches_oracle(ctx, bins):
 @pytest.mark.parametrize("bins,band", [(64, (380.0, 730.0)), (32, (380.0, 780.0)), (7, (400.0, 700.0))])
 def test_spectral_film_parity(ctx, bins, band):
     w, h, n, seed = 72, 41, 60_000, 11
-    film, scene, beam, cam = dsotm_film(ctx, w, h, n, seed, bins=bins, lambda_min=band[0], lambda_max=band[1])
+    film, scene, beam, cam = dsotm_film(ctx, w, h, n, seed, bins=bins, lambda_min=band[0], lambda_max=band[1],
+                                        haze_exact=True)
     film.trace_and_resolve(n, seed)
     raw = film.read_raw()
     p = oracle.vol_params(w, h, seed, 0.5, 0.06, 0.5, 14.0, bins=bins, lambda_min=band[0], lambda_max=band[1])
@@ -238,22 +258,28 @@ def test_spectral_film_parity(ctx, bins, band):
     expect = (fs.reshape(-1, bins).astype(np.float64) @ wts.T) * 2.0 ** -32
     got = film.accum().reshape(-1, 3)
     assert rel_l1(got, expect) < 1e-6
+    fast, *_ = dsotm_film(ctx, w, h, n, seed, bins=bins, lambda_min=band[0], lambda_max=band[1])
+    fast.trace_and_resolve(n, seed)
+    assert rel_l1(fast.read_raw(), fs) < FAST_TOL and rel_l1(fast.accum().reshape(-1, 3), expect) < FAST_TOL
 
 
 def test_zbuffer_occlusion_and_legacy_estimator(ctx):
     w, h, n, seed = 80, 60, 40_000, 21
     zb = np.full(w * h, np.inf, np.float32)
     zb[: w * h // 2] = 11.5  # occlude the top half behind depth 11.5
-    film, scene, beam, cam = dsotm_film(ctx, w, h, n, seed, zbuffer=zb)
-    film.trace_and_resolve(n, seed)
+    scene, beam, cam = sb.dsotm_scene(1.0)
     p = oracle.vol_params(w, h, seed, 0.5, 0.06, 0.5, 14.0)
     _, fx, _ = oracle.render_point(oscene(scene), ocam(cam), obeam(beam), p, 0, n, zbuf=zb, f32=False)
-    assert rel_l1(film.read_raw().reshape(-1), fx) < 1e-6
-    film2, *_ = dsotm_film(ctx, w, h, n, seed, estimator=1, weights=sb.VolWeights(0.05, 0.05, 0.0))
-    film2.trace_and_resolve(n, seed)
     p2 = oracle.vol_params(w, h, seed, 0.05, 0.05, 0.0, 14.0, estimator=1)
     _, fx2, _ = oracle.render_point(oscene(scene), ocam(cam), obeam(beam), p2, 0, n, f32=False)
-    assert rel_l1(film2.read_raw().reshape(-1), fx2) < 1e-6
+    for exact, tol in ((True, 1e-6), (False, FAST_TOL)):
+        film, *_ = dsotm_film(ctx, w, h, n, seed, zbuffer=zb, haze_exact=exact)
+        film.trace_and_resolve(n, seed)
+        assert rel_l1(film.read_raw().reshape(-1), fx) < tol, exact
+        film2, *_ = dsotm_film(ctx, w, h, n, seed, estimator=1, weights=sb.VolWeights(0.05, 0.05, 0.0),
+                               haze_exact=exact)
+        film2.trace_and_resolve(n, seed)
+        assert rel_l1(film2.read_raw().reshape(-1), fx2) < tol, exact
 
 
 def test_surface_rim_matches_cpu(ctx):
@@ -301,21 +327,21 @@ def test_edge_cases(ctx):
     scene, beam, cam = sb.dsotm_scene(1.0)
     # odd film sizes, a single pixel, zero photons, photon ranges with an offset
     for w, h in [(1, 1), (9, 7), (17, 33)]:
-        f = sb.GpuPhotonFilm(ctx, scene, cam, beam, w, h, 10, 1, 14.0)
+        f = sb.GpuPhotonFilm(ctx, scene, cam, beam, w, h, 10, 1, 14.0, haze_exact=True)
         f.trace_and_resolve(0, 1)
         assert not f.accum().any()
         f.trace_and_resolve(5000, 1)
         p = oracle.vol_params(w, h, 1, 0.5, 0.06, 0.5, 14.0)
         _, fx, _ = oracle.render_point(oscene(scene), ocam(cam), obeam(beam), p, 0, 5000, f32=False)
         assert rel_l1(f.read_raw().reshape(-1), fx) < 1e-6
-    f = sb.GpuPhotonFilm(ctx, scene, cam, beam, 40, 40, 10, 1, 14.0)
+    f = sb.GpuPhotonFilm(ctx, scene, cam, beam, 40, 40, 10, 1, 14.0, haze_exact=True)
     f.dispatch_photons(1000, 3000, 5)
     p = oracle.vol_params(40, 40, 5, 0.5, 0.06, 0.5, 14.0)
     _, fx, _ = oracle.render_point(oscene(scene), ocam(cam), obeam(beam), p, 1000, 3000, f32=False)
     assert rel_l1(f.read_raw().reshape(-1), fx) < 1e-6
     # empty scene: photons stream straight through the haze
     empty = sb.Scene(background=0.0)
-    f = sb.GpuPhotonFilm(ctx, empty, cam, beam, 32, 32, 10, 1, 14.0)
+    f = sb.GpuPhotonFilm(ctx, empty, cam, beam, 32, 32, 10, 1, 14.0, haze_exact=True)
     f.trace_and_resolve(2000, 2)
     p = oracle.vol_params(32, 32, 2, 0.5, 0.06, 0.5, 14.0)
     _, fx, _ = oracle.render_point(oscene(empty), ocam(cam), obeam(beam), p, 0, 2000, f32=False)

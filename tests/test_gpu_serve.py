@@ -1,7 +1,8 @@
 """Serving loop (continuous batching): a request's image is the same alone and
 in any mix of concurrent requests (bit-identical: its photons are keyed by its
-own index), single renders and orbit frames match the CPU oracle, admission
-respects the device-memory budget, and a real-time Poisson stream completes."""
+own index), single renders, orbit frames and progressive sessions match the
+CPU oracle, admission respects the device-memory budget, and a real-time
+Poisson stream completes."""
 import math
 
 import numpy as np
@@ -16,6 +17,8 @@ from spectral_b200.serve import ORBIT_TARGET, Server, orbit_camera, poisson_requ
 from helpers import rel_l1
 
 pytestmark = pytest.mark.gpu
+
+FAST_TOL = 2e-3  # relative L1 against the oracle: batched films run the fast haze samples
 
 
 def job(i, n=20_000, side=48, bins=16):
@@ -74,7 +77,7 @@ def test_same_alone_and_in_the_mix(ctx):
             exp = oracle_image(j, 0, j.n_photons)
         else:
             exp = oracle_image(j, 2 * j.n_photons, 3 * j.n_photons, orbit_camera(j, 2, 2.0))
-        assert exp.sum() > 0 and rel_l1(alone[i], exp) < 1e-6, i
+        assert exp.sum() > 0 and rel_l1(alone[i], exp) < FAST_TOL, i
 
 
 def test_budget_admission_and_cancel(ctx):
@@ -145,3 +148,82 @@ def test_realtime_stream_completes(ctx):
     plain = run_plain_stream(ctx, stream)
     assert plain["requests"] == len(stream) and plain["photons"] == m["photons"]
     assert 0 < plain["p50_ms"] <= plain["p99_ms"]
+
+
+def plain_image(ctx, j, begin, end):
+    """XYZ image of photons [begin, end) of a job through the plain film object."""
+    import ctypes as C
+    f = C.c_void_p()
+    _lib.check(_lib.lib.sc_photon_film_create(ctx.h, j.prims, j.n_prims, j.planes, j.n_planes, j.mats, j.n_mats,
+                                              0.0, C.byref(j.cam), C.byref(j.beam), j.width, j.height, j.n_photons,
+                                              j.seed, j.max_dist, C.byref(j.weights), None, C.byref(j.opts),
+                                              C.byref(f)))
+    try:
+        _lib.check(_lib.lib.sc_photon_film_set_spectral(f, int(j.spectral)))
+        _lib.check(_lib.lib.sc_photon_film_dispatch(f, begin, end, j.seed))
+        out = np.empty(3 * j.width * j.height, np.float32)
+        _lib.check(_lib.lib.sc_photon_film_read_accum(f, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+    finally:
+        _lib.lib.sc_photon_film_destroy(f)
+
+
+def test_progressive_session_accumulates(ctx):
+    """A session of 4 frames on a fixed camera adds photons [0, 4N) into one
+    film on the device: its image is the film of those photons times 1/4 (the
+    same bits as the plain film object's image of [0, 4N), scaled by 2^-2),
+    within FAST_TOL of the oracle, and the same alone and in a mix.  Midway,
+    peek shows the image of the frames done so far."""
+    j = job(2, n=15_000)
+    n = j.n_photons
+    s = Server(ctx, budget_bytes=1 << 30)
+    rid = s.submit(j, frames=4)
+    s.step()
+    s.step()
+    fr, mid = s.peek(rid)
+    assert fr == 2
+    assert mid.tobytes() == (plain_image(ctx, j, 0, 2 * n) * np.float32(0.5)).tobytes()
+    alone = drain(s)[rid]
+    out = np.empty(3 * j.width * j.height, np.float32)
+    import ctypes as C
+    assert _lib.lib.sc_server_peek(s.h, rid, out.ctypes.data_as(C.POINTER(C.c_float)), out.size,
+                                   None) == _lib.SC_E_STATE  # finished: polled, not peeked
+    s.close()
+    plain = plain_image(ctx, j, 0, 4 * n)
+    assert alone.tobytes() == (plain * np.float32(0.25)).tobytes()
+    exp = oracle_image(j, 0, 4 * n) * 0.25
+    assert exp.sum() > 0 and rel_l1(alone, exp) < FAST_TOL
+    # in a mix with single renders, an orbit session and another progressive session
+    m = Server(ctx, budget_bytes=1 << 30)
+    others = [m.submit(job(0)), m.submit(job(1), frames=3, orbit_deg=2.0)]
+    m.step()
+    mine = m.submit(j, frames=4)
+    others.append(m.submit(job(3), frames=2))
+    got = drain(m)
+    m.close()
+    assert sorted(got) == sorted(others + [mine])
+    assert got[mine].tobytes() == alone.tobytes()
+    exp3 = oracle_image(job(3), 0, 2 * job(3).n_photons) * 0.5
+    assert rel_l1(got[others[2]], exp3) < FAST_TOL
+
+
+def test_mixed_free_flight_and_uniform_requests(ctx):
+    """A server step that holds a free-flight request and uniform ones runs
+    the kernel built with free-flight sampling: every image is the same as
+    the request's image alone (run by the kernel without it)."""
+    reqs = [job(0), job(1), job(4)]
+    reqs[1].opts.estimator = 3
+    reqs[1].weights.sigma_t = 0.3
+    alone = {}
+    for i, r in enumerate(reqs):
+        a = Server(ctx, budget_bytes=1 << 30)
+        rid = a.submit(r)
+        alone[i] = drain(a)[rid]
+        a.close()
+    m = Server(ctx, budget_bytes=1 << 30)
+    ids = {m.submit(r): i for i, r in enumerate(reqs)}
+    got = drain(m)
+    m.close()
+    for rid, img in got.items():
+        assert img.tobytes() == alone[ids[rid]].tobytes(), ids[rid]
+    assert alone[1].tobytes() != plain_image(ctx, job(1), 0, job(1).n_photons).tobytes()
