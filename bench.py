@@ -90,7 +90,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["atomics", "batch", "serve", "tracer"],
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["atomics", "batch", "serve", "split", "tracer"],
                     default="batch")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -99,6 +99,9 @@ def parse():
                     help="scenes of the batch workload (0: 256; the first N of the same seeded draw)")
     ap.add_argument("--photons", type=int, default=0,
                     help="photons per step for prism/rainbow/beam (0: the workload's; smaller for profiling)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
+                    help="window of the 200 req/s Poisson stream replayed in real time for the served numbers "
+                         "(batch and serve workloads; 0: none)")
     return ap.parse_args()
 
 
@@ -834,33 +837,61 @@ def run_cpu_atomics(seconds):
 # the 60 s stream by default), prism scenes of the batch workload's distribution,
 # 2^16-2^20 photons per frame, 30 % orbit sessions of 16-128 frames at 2 deg
 # per frame, 40 GB HBM budget.
-SERVE = dict(rate=200.0, seconds=15.0, budget_gb=40.0, seed=0x5E7E)
+SERVE = dict(rate=200.0, budget_gb=40.0, seed=0x5E7E, sample_s=3.0)
+
+
+def served_summary(ctx, seconds, rank, clk=None):
+    """The serving numbers of the config-5 stream: a `seconds` window of the
+    200 req/s Poisson stream replayed in real time against the continuous-
+    batching server (latency from arrival to the XYZ image in host memory),
+    then the stream's first SERVE["sample_s"] seconds of requests submitted at
+    once to the server (capacity) and to the plain per-request path (a film
+    object per request, frames traced and read back one by one), whose
+    throughput ratio is served_over_plain."""
+    from spectral_b200.serve import Server, poisson_requests, run_plain_stream, run_stream
+    budget = int(SERVE["budget_gb"] * (1 << 30))
+    warm = poisson_requests(SERVE["rate"], 0.5, SERVE["seed"] ^ 0xA5A5 ^ rank)
+    srv = Server(ctx, budget_bytes=budget)
+    run_stream(srv, warm, want_image=True)
+    srv.close()
+    run_plain_stream(ctx, warm[:20], time_scale=0.0)
+    stream = poisson_requests(SERVE["rate"], seconds, SERVE["seed"] + rank)
+    srv = Server(ctx, budget_bytes=budget)
+    served = run_stream(srv, stream, want_image=True)
+    srv.close()
+    sample = [r for r in stream if r[0] < SERVE["sample_s"]]
+    srv = Server(ctx, budget_bytes=budget)
+    capacity = run_stream(srv, sample, time_scale=0.0, want_image=True)
+    srv.close()
+    plain = run_plain_stream(ctx, sample, time_scale=0.0)
+    return {
+        "window_s": seconds, "rate_per_s": SERVE["rate"], "requests": len(stream),
+        "sessions": sum(1 for r in stream if r[2] > 1), "frames": sum(r[2] for r in stream),
+        "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
+        "p50_first_frame_ms": served["p50_first_frame_ms"], "p99_first_frame_ms": served["p99_first_frame_ms"],
+        "photons_per_s": served["photons_per_s"], "photons": served["photons"], "wall_s": served["wall_s"],
+        "steps": served["steps"],
+        "capacity_photons_per_s": capacity["photons_per_s"],
+        "plain_per_request_photons_per_s": plain["photons_per_s"],
+        "served_over_plain": capacity["photons_per_s"] / plain["photons_per_s"],
+        "sample": "latency: the first %.0f s of the stream (seed 0x%X) replayed in real time; capacity and plain: "
+                  "its first %.0f s (%d requests, %d frames) submitted at once to the server and to a film object "
+                  "per request" % (seconds, SERVE["seed"] + rank, SERVE["sample_s"], len(sample),
+                                   sum(r[2] for r in sample)),
+        "what": "latency from arrival to the XYZ image in host memory; served_over_plain = capacity / plain on "
+                "the same requests",
+    }
 
 
 def run_gpu_serve(args, rank, world, local_rank):
     import torch
     import spectral_b200 as sb
-    from spectral_b200.serve import Server, poisson_requests, run_plain_stream, run_stream
     torch.cuda.set_device(local_rank)
     ctx = sb.GpuContext(local_rank)
-    budget = int(SERVE["budget_gb"] * (1 << 30))
-    # warm-up: a short stream of other requests through both paths
-    warm = poisson_requests(SERVE["rate"], 0.5 * max(1, args.warmup), SERVE["seed"] ^ 0xA5A5 ^ rank)
-    srv = Server(ctx, budget_bytes=budget)
-    run_stream(srv, warm, want_image=True)
-    srv.close()
-    run_plain_stream(ctx, warm[:20])
-    stream = poisson_requests(SERVE["rate"], SERVE["seconds"], SERVE["seed"] + rank)
-    srv = Server(ctx, budget_bytes=budget)
+    seconds = args.serve_seconds or 15.0
     uuid = "GPU-" + str(torch.cuda.get_device_properties(torch.device("cuda", local_rank)).uuid)
     with ClockSampler(uuid) as clk, torch.cuda.nvtx.range("timed"):  # nvtx range for ncu --nvtx-include
-        served = run_stream(srv, stream, want_image=True)
-    srv.close()
-    # capacity: the same requests all submitted at once, served until drained
-    srv = Server(ctx, budget_bytes=budget)
-    capacity = run_stream(srv, stream, time_scale=0.0, want_image=True)
-    srv.close()
-    plain = run_plain_stream(ctx, stream)
+        served = served_summary(ctx, seconds, rank)
     total_rate = served["photons_per_s"]
     if world > 1:  # every rank served its own stream: total photons over the longest replay
         import torch.distributed as dist
@@ -872,9 +903,10 @@ def run_gpu_serve(args, rank, world, local_rank):
         total_rate = float(ph.item()) / float(wall.item())
     if rank != 0:
         return None
-    frames = sum(s[2] for s in stream)
-    in_bytes = sum(C.sizeof(s[1]) for s in stream)
-    out_bytes = sum(3 * s[1].width * s[1].height * 4 for s in stream)
+    from spectral_b200.serve import poisson_requests
+    stream = poisson_requests(SERVE["rate"], seconds, SERVE["seed"] + rank)
+    in_bytes = sum(C.sizeof(r[1]) for r in stream)
+    out_bytes = sum(3 * r[1].width * r[1].height * 4 for r in stream)
     return {
         "metric": "served photons/s with p50/p99 request latency (continuous batching vs plain per-request launch)",
         "value": total_rate, "unit": "photons/s", "n_gpus": world, "steps": 1,
@@ -882,22 +914,159 @@ def run_gpu_serve(args, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f32 transport, int64 fixed-point film", "data": "synthetic (seeded stream)",
         "config": {"workload": "serve: Poisson %.0f req/s for %.0f s (%d requests, %d frames), prism scenes of the "
                                "batch distribution, 2^16-2^20 photons per frame, 30%% orbit sessions of 16-128 "
-                               "frames at 2 deg, %.0f GB budget" % (SERVE["rate"], SERVE["seconds"], len(stream),
-                                                                     frames, SERVE["budget_gb"]),
+                               "frames at 2 deg, %.0f GB budget" % (SERVE["rate"], seconds, len(stream),
+                                                                     served["frames"], SERVE["budget_gb"]),
                    "parallelism": "own request stream per rank, no collective",
                    "timing": "host clock over the whole stream replayed in real time (one step = the stream)"},
-        "served": served, "plain_per_request": plain,
-        "served_over_plain": served["photons_per_s"] / plain["photons_per_s"],
-        # the replay serves the offered load; the burst shows how far above it the server goes
-        "capacity": dict(capacity, what="the same requests submitted at once (arrival time 0), served to the "
-                                        "last image"),
-        "capacity_over_plain": capacity["photons_per_s"] / plain["photons_per_s"],
+        "served": served,
         "e2e": {"value": total_rate, "unit": "photons/s", "h2d_bytes_per_step": in_bytes,
                 "d2h_bytes_per_step": out_bytes,
                 "path": "sc_server_submit per request, sc_server_step, sc_server_poll with the XYZ image to host"},
         "gpu_launches": served["steps"] * 3,  # per server step: batch_kernel, reduce_scan, reduce_list
         "clocks": clk.summary(),
     }
+
+
+def run_gpu_split(args, rank, world, local_rank):
+    """One scene split across the ranks (strong scaling): the rainbow workload's
+    2^26 photons in contiguous ranges, one per rank, each traced into the rank's
+    own int64 film, then ONE all-reduce (sum) of the 1.06 GB films over NCCL and
+    the sensor reduction of the summed film on every rank.  The film of any
+    number of ranks is bit-identical to one GPU's."""
+    import torch
+    import spectral_b200 as sb
+    from spectral_b200 import _lib
+    from spectral_b200.shard import photon_range, trace_sharded
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    wl = "rainbow"
+    cfg = dict(WORKLOADS[wl])
+    if args.photons:
+        cfg["photons"] = args.photons
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ctx = sb.GpuContext(local_rank)
+    scene, beam, cam = build_scene(wl)
+    W, H, B, N = cfg["width"], cfg["height"], cfg["bins"], cfg["photons"]
+    b0, b1 = photon_range(rank, world, N)
+    prims, np_, planes, npl, mats, nm = scene.arrays()
+
+    def dev_bytes(obj, n):
+        return torch.frombuffer(bytearray(bytes(obj)[: n * C.sizeof(obj._type_)] or b"\0"), dtype=torch.uint8).to(dev)
+
+    d_prims, d_planes, d_mats = dev_bytes(prims, np_), dev_bytes(planes, npl), dev_bytes(mats, nm)
+    opts = _lib.sc_film_options(B, cfg["lambda_min"], cfg["lambda_max"], cfg["max_bounces"], 32, 0)
+    desc = _lib.sc_trace_desc(d_prims.data_ptr(), np_, d_planes.data_ptr(), npl, d_mats.data_ptr(), nm, cam.c, beam.c,
+                              _lib.sc_vol_weights(cfg["sigma_s"], cfg["sigma_t"], cfg["g"]), W, H, cfg["seed"], 1,
+                              cfg["max_dist"], opts, None)
+    film = torch.zeros(_lib.lib.sc_film_bytes(W, H, B) // 8, dtype=torch.int64, device=dev)
+    flags = torch.zeros(_lib.lib.sc_film_flag_bytes(W, H) // 4, dtype=torch.int32, device=dev)
+    xyz = torch.empty(3 * W * H, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = C.c_void_p(stream.cuda_stream)
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        _lib.check(_lib.lib.sc_trace_photons_device(ctx.h, C.byref(desc), b0, b1 - b0, C.c_void_p(film.data_ptr()),
+                                                    C.c_void_p(flags.data_ptr()), sp))
+        if ev:
+            ev[1].record(stream)
+        if dist:
+            dist.all_reduce(film, op=dist.ReduceOp.SUM)  # int64: exact
+            flags.fill_(-1)                               # other ranks lit tiles too
+        if ev:
+            ev[2].record(stream)
+        _lib.check(_lib.lib.sc_sensor_reduce_device(ctx.h, W, H, B, cfg["lambda_min"], cfg["lambda_max"], 32,
+                                                    C.c_void_p(film.data_ptr()), C.c_void_p(flags.data_ptr()),
+                                                    C.c_void_p(xyz.data_ptr()), 1, sp))
+        if ev:
+            ev[3].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    with ClockSampler(uuid) as clk:
+        for k in range(args.steps):
+            step(ev[k])
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    parts = [[ev[k][i].elapsed_time(ev[k][i + 1]) for k in range(args.steps)] for i in range(3)]
+    total_ms = sum(ev[k][0].elapsed_time(ev[k][3]) for k in range(args.steps))
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = N * args.steps / (total_ms / 1e3)
+
+    # end to end through the film object: trace_sharded (own range + the film
+    # all-reduce) and the XYZ image back to the host, every step
+    pf = sb.GpuPhotonFilm(ctx, scene, cam, beam, W, H, N, cfg["seed"], cfg["max_dist"],
+                          sb.VolWeights(cfg["sigma_s"], cfg["sigma_t"], cfg["g"]), bins=B,
+                          lambda_min=cfg["lambda_min"], lambda_max=cfg["lambda_max"], max_bounces=cfg["max_bounces"])
+    host_xyz = torch.empty(3 * W * H, dtype=torch.float32, pin_memory=True).numpy()
+
+    def e2e_step():
+        if dist:
+            trace_sharded(pf, N, cfg["seed"])
+        else:
+            pf.dispatch_photons(0, N, cfg["seed"])
+        _lib.check(_lib.lib.sc_photon_film_read_accum(pf.h, host_xyz.ctypes.data_as(C.POINTER(C.c_float))))
+        _lib.check(_lib.lib.sc_photon_film_clear(pf.h))
+
+    e2e_steps = args.e2e_steps or max(3, args.steps // 2)
+    e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    pf.close()
+    if rank != 0:
+        return None
+    film_bytes = film.numel() * 8
+    ar_ms = statistics.mean(parts[1])
+    line = {
+        "metric": METRIC_POINT + "; one scene split across GPUs",
+        "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32 transport, int64 fixed-point film", "data": "synthetic (seeded scene)",
+        "config": {"workload": "split: the rainbow scene (water sphere r=1, beam 2.2, 1920x1080x64 bins), %d photons "
+                               "split into contiguous ranges over %d rank(s)" % (N, world),
+                   "photons_per_step": N, "film": [W, H, B],
+                   "parallelism": "photon ranges per rank + one int64 NCCL all-reduce of the film per step"},
+        "kernels": {"trace_ms": statistics.mean(parts[0]), "allreduce_ms": ar_ms,
+                    "reduce_ms": statistics.mean(parts[2])},
+        "allreduce": {"bytes": film_bytes, "ms": ar_ms,
+                      "bus_gbs": (film_bytes * 2 * (world - 1) / world / (ar_ms / 1e3) / 1e9) if world > 1 and ar_ms > 0
+                      else None},
+        "e2e": {"value": N * e2e_steps / e2e_s, "unit": "photons/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 3 * W * H * 4,
+                "path": "shard.trace_sharded (own range + film all-reduce) + read_accum (host f32 XYZ) + clear"},
+        "gpu_launches": args.steps * (2 + 3),  # per step: sort (3) + photon kernel, drain
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        rate, n_s, dt, th = run_cpu(wl, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": rate, "unit": "photons/s", "cores": th, "kind": "port",
+                                "sample": "%d photons of the rainbow workload from photon 0, %.1f s, %s"
+                                          % (n_s, dt, cpu_model())}
+    return line
 
 
 BATCH = dict(n_jobs=256, seed=0xB200, bins=32, lambda_min=380.0, lambda_max=780.0)
@@ -1024,8 +1193,8 @@ def run_gpu_batch(args, rank, world, local_rank):
     plain_ms = timed(b.run_plain, max(2, args.steps // 2))
     # plain per-scene launches through the drop-in object API (what a caller of
     # the reference's GpuPhotonFilm does per scene): create, trace, read back,
-    # free.  Host-bound by the film allocations (cudaMalloc / cudaFree of up to
-    # 268 MB per scene), whose cost varies from pass to pass: best of two passes.
+    # free.  The film's buffers come from the context's memory pool, so after
+    # the first pass no pass allocates; best of two passes.
     plain_api_s = float("inf")
     for _ in range(2):
         t0 = time.perf_counter()
@@ -1081,8 +1250,12 @@ def run_gpu_batch(args, rank, world, local_rank):
         e2e_s = float(t.item())
     e2e_value = job_photons * e2e_steps / e2e_s
     if rank != 0:
+        served = None
+        if args.serve_seconds > 0:  # every rank serves its own stream (the same work as rank 0)
+            served_summary(ctx, args.serve_seconds, rank)
         return None
     film_err = batch_film_err(ctx, specs)
+    served = served_summary(ctx, args.serve_seconds, rank) if args.serve_seconds > 0 else None
 
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs") or 6650.0
@@ -1116,6 +1289,7 @@ def run_gpu_batch(args, rank, world, local_rank):
                         "copy of a pass overlaps the next pass's tracing), all steps synchronised at the end"},
         "gpu_launches": args.steps * 3,  # per pass: batch_kernel, reduce_scan, reduce_list
         "film_err": film_err,
+        "served": served,
         "work": stats,
         "roofline": {"bound": "hbm", "kernel": "batch_kernel + reduce_scan + reduce_list (one pass)",
                      "achieved": (stats["in_frame_samples"] * 8 + 2 * stats["dirty_tile_bytes"] +
@@ -1163,7 +1337,7 @@ def main():
             metric = "L2 atomic throughput, u32 atomicAdd (AtomicFilm synthetic splat)"
             cfg_line = {"workload": "atomics (see the GPU arm)", "splats_per_step": ATOMICS["splats"]}
         elif args.workload == "serve":
-            reqs = [r[1] for r in load_specs().poisson_request_specs(SERVE["rate"], SERVE["seconds"],
+            reqs = [r[1] for r in load_specs().poisson_request_specs(SERVE["rate"], args.serve_seconds or 15.0,
                                                                        SERVE["seed"])]
             run_cpu_batch(0.5, specs=reqs)
             for _ in range(args.steps):
@@ -1174,7 +1348,7 @@ def main():
             metric = ("served photons/s with p50/p99 request latency (continuous batching vs plain per-request "
                       "launch)")
             cfg_line = {"workload": "serve (see the GPU arm)", "rate_per_s": SERVE["rate"],
-                        "seconds": SERVE["seconds"]}
+                        "seconds": args.serve_seconds or 15.0}
         elif args.workload == "tracer":
             run_cpu_tracer(0.5)
             for _ in range(args.steps):
@@ -1229,7 +1403,7 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     line = {"atomics": run_gpu_atomics, "batch": run_gpu_batch, "serve": run_gpu_serve,
-            "tracer": run_gpu_tracer}.get(
+            "split": run_gpu_split, "tracer": run_gpu_tracer}.get(
         args.workload, run_gpu)(args, rank, world, local_rank)
     if world > 1:
         import torch.distributed as dist

@@ -121,6 +121,14 @@ struct sc_photon_film {
     LaunchShape shape{};
     uint64_t film_version = 1, xyz_version = 0;
 
+    void bind_pool() {
+        if (!ctx->pool) return;  // no pool: plain cudaMalloc buffers
+        prims.bind(ctx->pool, stream); planes.bind(ctx->pool, stream); mats.bind(ctx->pool, stream);
+        zbuf.bind(ctx->pool, stream); film.bind(ctx->pool, stream); flags.bind(ctx->pool, stream);
+        xyz.bind(ctx->pool, stream); surface.bind(ctx->pool, stream); binw.bind(ctx->pool, stream);
+        work.bind(ctx->pool, stream); rgb.bind(ctx->pool, stream); debug.bind(ctx->pool, stream);
+    }
+
     PhotonParams params(uint32_t base, uint32_t count, uint32_t s) const {
         PhotonParams p;
         std::memset(&p, 0, sizeof p);
@@ -395,11 +403,16 @@ int sc_photon_film_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_pri
     DeviceGuard g(ctx->device);
     auto fail = [&](cudaError_t e) {
         set_error("photon film setup failed: %s", cudaGetErrorString(e));
-        delete f;
+        cudaStream_t st = f->stream;
+        delete f;  // buffers go back on the film's stream, which is destroyed after them
+        if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
         return e == cudaErrorMemoryAllocation ? SC_E_NOMEM : SC_E_CUDA;
     };
     cudaError_t e = cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(e);
+    // every buffer of the film from the context's pool, on the film's stream:
+    // creating and destroying films allocates nothing once the pool holds enough
+    f->bind_pool();
     const size_t npx = (size_t)width * height;
     if ((e = f->prims.alloc(n_prims)) != cudaSuccess) return fail(e);
     if ((e = f->planes.alloc(n_planes)) != cudaSuccess) return fail(e);
@@ -409,18 +422,18 @@ int sc_photon_film_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_pri
     if ((e = f->xyz.alloc(3 * npx)) != cudaSuccess) return fail(e);
     if ((e = f->surface.alloc(3 * npx)) != cudaSuccess) return fail(e);
     if ((e = f->work.alloc(264)) != cudaSuccess) return fail(e);
-    if (n_prims && (e = cudaMemcpy(f->prims.p, prims, n_prims * sizeof(sc_primitive), cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
-    if (n_planes && (e = cudaMemcpy(f->planes.p, planes, n_planes * sizeof(sc_plane), cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
-    if (n_mats && (e = cudaMemcpy(f->mats.p, mats, n_mats * sizeof(sc_material), cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
+    if (n_prims && (e = cudaMemcpyAsync(f->prims.p, prims, n_prims * sizeof(sc_primitive), cudaMemcpyHostToDevice, f->stream)) != cudaSuccess) return fail(e);
+    if (n_planes && (e = cudaMemcpyAsync(f->planes.p, planes, n_planes * sizeof(sc_plane), cudaMemcpyHostToDevice, f->stream)) != cudaSuccess) return fail(e);
+    if (n_mats && (e = cudaMemcpyAsync(f->mats.p, mats, n_mats * sizeof(sc_material), cudaMemcpyHostToDevice, f->stream)) != cudaSuccess) return fail(e);
     if (zbuffer) {
         if ((e = f->zbuf.alloc(npx)) != cudaSuccess) return fail(e);
-        if ((e = cudaMemcpy(f->zbuf.p, zbuffer, npx * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
+        if ((e = cudaMemcpyAsync(f->zbuf.p, zbuffer, npx * sizeof(float), cudaMemcpyHostToDevice, f->stream)) != cudaSuccess) return fail(e);
     }
     if (o.bins) {
         std::vector<float> w(3 * o.bins);
         bin_weights(ctx->tables, o.bins, o.lambda_min, o.lambda_max, w.data());
         if ((e = f->binw.alloc(w.size())) != cudaSuccess) return fail(e);
-        if ((e = cudaMemcpy(f->binw.p, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
+        if ((e = cudaMemcpyAsync(f->binw.p, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, f->stream)) != cudaSuccess) return fail(e);
     }
     if ((e = cudaMemsetAsync(f->film.p, 0, f->film.bytes(), f->stream)) != cudaSuccess) return fail(e);
     if ((e = cudaMemsetAsync(f->flags.p, 0, f->flags.bytes(), f->stream)) != cudaSuccess) return fail(e);
@@ -441,7 +454,8 @@ int sc_photon_film_destroy(sc_photon_film* f) {
         if (f->stream) cudaStreamSynchronize(f->stream);
         f->prims.reset(); f->planes.reset(); f->mats.reset(); f->zbuf.reset(); f->film.reset(); f->flags.reset();
         f->xyz.reset(); f->surface.reset(); f->binw.reset(); f->work.reset(); f->rgb.reset(); f->debug.reset();
-        if (f->stream) cudaStreamDestroy(f->stream);
+        // the frees are stream-ordered: let them complete, so the next film can take the memory at once
+        if (f->stream) { cudaStreamSynchronize(f->stream); cudaStreamDestroy(f->stream); }
     }
     delete f;
     return SC_OK;

@@ -59,23 +59,38 @@ struct DeviceGuard {
     ~DeviceGuard() { int cur = 0; cudaGetDevice(&cur); if (cur != prev) cudaSetDevice(prev); }
 };
 
+// Device buffer.  Unbound, it holds cudaMalloc memory.  Bound to a memory pool
+// and a stream (bind), it takes stream-ordered memory from the pool on that
+// stream and gives it back there: a pool that keeps its memory reserved turns
+// repeated create / destroy of same-sized objects into no allocation at all.
 template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { reset(); }
+    void bind(cudaMemPool_t mp, cudaStream_t s) { pool = mp; stream = s; }
     cudaError_t alloc(size_t count) {
         reset();
         if (count == 0) return cudaSuccess;
-        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+        cudaError_t e = pool ? cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), pool, stream)
+                             : cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
         if (e != cudaSuccess) { p = nullptr; return e; }
         n = count;
         return cudaSuccess;
     }
-    void reset() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    void reset() {
+        if (p) {
+            if (pool) cudaFreeAsync(p, stream);
+            else cudaFree(p);
+        }
+        p = nullptr;
+        n = 0;
+    }
     size_t bytes() const { return n * sizeof(T); }
 };
 

@@ -97,15 +97,23 @@ def trace_rows_sharded(tracer, spp, group=None):
 
 def trace_sharded(film, n_photons, seed, group=None):
     """Trace this rank's share of photons [0, n_photons) into `film`, then sum the
-    films of all ranks into every rank's film (NCCL all-reduce on int64)."""
+    films of all ranks into every rank's film: an int64 all-reduce of the
+    device film in place over NCCL, or through host memory on a host backend
+    (gloo).  The film's tiles are then all marked lit (other ranks lit some of
+    them), so its reduction reads every tile."""
     import torch
     import torch.distributed as dist
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     b, e = photon_range(rank, world, n_photons)
     film.dispatch_photons(b, e, seed)
     t = film_tensor(film)
-    check(lib.sc_ctx_synchronize(film.ctx.h))
-    allreduce_film_(t, group)
+    check(lib.sc_ctx_synchronize(film.ctx.h))  # the trace, on the film's stream, is done
+    if dist.get_backend(group) == "nccl":
+        allreduce_film_(t, group)
+    else:
+        host = t.cpu()
+        allreduce_film_(host, group)
+        t.copy_(host)
     torch.cuda.synchronize()
     check(lib.sc_photon_film_mark_all_dirty(film.h))
     return film
