@@ -4,12 +4,15 @@
 // GPU mirror spectral-gpu/src/shaders/trace.wgsl:419-537) as a wavefront:
 //   generate  one path per (pixel, sample): stream key mix2(pixel, sample index),
 //             jittered primary ray, hero-comb wavelength draw (spectrum.rs:20-32);
-//   intersect nearest scene hit (+ the optional spherical emitter) per queued ray;
+//   intersect nearest scene hit (+ the optional spherical emitter) per queued ray
+//             (for primary rays in the generating kernel, for later rays in the
+//             shade kernel that queued them);
 //   shade     background / emission at termination, Fresnel / refract / TIR or
 //             Lambertian scatter, dispersion collapse to the hero lane, optional
 //             Russian roulette; survivors are compacted into the next queue with
 //             warp ballots, one atomic per block and shared-memory staging so the
-//             SoA writes are contiguous;
+//             SoA writes are contiguous, and the compacted rays are intersected
+//             at once;
 //   accumulate each pixel's samples summed in sample order (the CPU's order), so
 //             the image is deterministic and, for scenes without Lambertian
 //             surfaces, bit-identical to the CPU tracer.
@@ -172,25 +175,6 @@ __device__ __forceinline__ bool shade_path(const TracerSmem& s, const SceneView&
     return survive;
 }
 
-__global__ void __launch_bounds__(256) tr_intersect(const TracerParams* __restrict__ gp, uint32_t bounce, RayQueue q,
-                                                    const uint32_t* __restrict__ counts, HitQueue hq) {
-    __shared__ TracerSmem s;
-    extern __shared__ __align__(16) unsigned char dyn[];
-    const uint32_t n = counts[bounce];
-    if (blockIdx.x * blockDim.x >= n) return;  // nothing queued for this CTA (late bounces)
-    const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const f3 o = mk(q.ox[i], q.oy[i], q.oz[i]), d = mk(q.dx[i], q.dy[i], q.dz[i]);
-        float t;
-        f3 nrm;
-        uint32_t info;
-        trace_hit(s, S, o, d, t, nrm, info);
-        hq.t[i] = t;
-        if ((info >> 24) == 1u) { hq.nx[i] = nrm.x; hq.ny[i] = nrm.y; hq.nz[i] = nrm.z; }
-        hq.info[i] = info;
-    }
-}
-
 // Bounce 0 without a ray queue round trip: each path's primary ray is made as
 // tr_generate makes it, intersected at once, and queued with its hit for the
 // first shade (persistent grid, scene in shared memory).
@@ -230,9 +214,13 @@ __global__ void __launch_bounds__(256) tr_primary(const TracerParams* __restrict
     }
 }
 
+// ISECT: the surviving rays, once compacted into shared memory, are also
+// intersected here (the next bounce's hits go to `hout`), so they do not make a
+// queue round trip through a separate intersect launch.
+template <bool ISECT>
 __global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __restrict__ gp, uint32_t bounce,
-                                                          RayQueue q, HitQueue hq, RayQueue out, uint32_t* counts,
-                                                          float* result) {
+                                                          RayQueue q, HitQueue hq, RayQueue out, HitQueue hout,
+                                                          uint32_t* counts, float* result) {
     __shared__ TracerSmem s;
     __shared__ uint32_t warp_base[kShadeThreads / 32 + 1];
     __shared__ uint32_t block_base;
@@ -288,6 +276,16 @@ __global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __
             out.dx[g] = st_f[3][j]; out.dy[g] = st_f[4][j]; out.dz[g] = st_f[5][j];
             out.tp[g] = st_f[6][j]; out.u[g] = st_f[7][j];
             out.rng[g] = st_u[0][j]; out.id[g] = st_u[1][j]; out.flags[g] = st_u[2][j];
+            if (ISECT) {  // the next bounce's hit, by converged (compacted) threads
+                float t;
+                f3 nrm;
+                uint32_t info;
+                trace_hit(s, S, mk(st_f[0][j], st_f[1][j], st_f[2][j]), mk(st_f[3][j], st_f[4][j], st_f[5][j]), t,
+                          nrm, info);
+                hout.t[g] = t;
+                if ((info >> 24) == 1u) { hout.nx[g] = nrm.x; hout.ny[g] = nrm.y; hout.nz[g] = nrm.z; }
+                hout.info[g] = info;
+            }
         }
         __syncthreads();
     }
@@ -323,26 +321,41 @@ __global__ void __launch_bounds__(256) tr_tail(const TracerParams* __restrict__ 
     if ((threadIdx.x & 31u) == 0 && segs) atomicAdd(counts + first + 1, segs);
 }
 
-// Per-pixel sample sum in sample order (tracer.rs:121-135), added to the running sum.
+// Per-pixel sample sum in sample order (tracer.rs:121-135), added to the running
+// sum.  A CTA takes 64 pixels: its 256 threads stage 64 samples of them at a
+// time into shared memory with coalesced loads (the 192 floats of a sample's
+// 64 pixels are contiguous), then 192 threads, one per (pixel, channel), add
+// the staged samples in sample order.
+constexpr uint32_t kAccPixels = 64, kAccSamples = 64;
 __global__ void __launch_bounds__(256) tr_accumulate(uint32_t first_pixel, uint32_t n_pixels, uint32_t spp,
                                                      const float* __restrict__ result, float* sum,
                                                      const uint32_t* __restrict__ counts, uint32_t max_depth,
                                                      unsigned long long* segments) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j == 0) {
+    __shared__ float st[kAccSamples * 3 * kAccPixels];
+    const uint32_t tid = threadIdx.x;
+    if (blockIdx.x == 0 && tid == 0) {
         unsigned long long t = 0;
         for (uint32_t b = 0; b < max_depth; ++b) t += counts[b];
         atomicAdd(segments, t);  // both wave chains add here
     }
-    if (j >= n_pixels) return;
-    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+    const uint32_t p0 = blockIdx.x * kAccPixels;
+    const uint32_t np = min(kAccPixels, n_pixels - p0);
+    const uint32_t row = 3u * np;  // floats of one sample of this CTA's pixels
+    float a = 0.0f;
+    for (uint32_t s0 = 0; s0 < spp; s0 += kAccSamples) {
+        const uint32_t ns = min(kAccSamples, spp - s0);
+        __syncthreads();
+        for (uint32_t k = tid; k < ns * row; k += blockDim.x) {
+            const uint32_t s = k / row, e = k - s * row;
+            st[s * 3u * kAccPixels + e] = result[3u * ((size_t)(s0 + s) * n_pixels + p0) + e];
+        }
+        __syncthreads();
+        if (tid < row) {
 #pragma unroll 8
-    for (uint32_t s = 0; s < spp; ++s) {  // loads run ahead; the adds stay in sample order
-        const float* r = result + 3u * ((size_t)s * n_pixels + j);
-        a0 += r[0]; a1 += r[1]; a2 += r[2];
+            for (uint32_t s = 0; s < ns; ++s) a += st[s * 3u * kAccPixels + tid];
+        }
     }
-    float* o = sum + 3u * (size_t)(first_pixel + j);
-    o[0] += a0; o[1] += a1; o[2] += a2;
+    if (tid < row) sum[3u * (size_t)(first_pixel + p0) + tid] += a;
 }
 
 }  // namespace
@@ -351,8 +364,8 @@ size_t tracer_dyn_smem(uint32_t n_planes) { return (size_t)(n_planes ? n_planes 
 
 int tracer_grid(int sms) {
     int a = 0, b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, tr_intersect, 256, tracer_dyn_smem(SC_MAX_PLANES));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tr_shade, kShadeThreads, tracer_dyn_smem(SC_MAX_PLANES));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, tr_primary, 256, tracer_dyn_smem(SC_MAX_PLANES));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tr_shade<true>, kShadeThreads, tracer_dyn_smem(SC_MAX_PLANES));
     int k = a < b ? a : b;
     return sms * (k > 0 ? k : 1);
 }
@@ -367,22 +380,27 @@ cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch&
     if (wave_bounces == 0)
         tr_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(d_params, first_pixel, n_pixels, n_paths, L.d_base,
                                                            L.qa, L.counts, L.result);
+    // bounce b shades the hits of bounce b and, while more wave bounces follow,
+    // intersects its compacted survivors too (hit queues alternate)
     for (uint32_t b = 0; b < wave_bounces; ++b) {
         const RayQueue& in = (b & 1u) ? L.qb : L.qa;
         const RayQueue& out = (b & 1u) ? L.qa : L.qb;
-        uint32_t g = L.grid;
+        const HitQueue& hin = (b & 1u) ? L.hits2 : L.hits;
+        const HitQueue& hout = (b & 1u) ? L.hits : L.hits2;
+        const uint32_t g = L.grid;
         if (b == 0)
             tr_primary<<<g, 256, dyn, st>>>(d_params, first_pixel, n_pixels, n_paths, L.d_base, in, L.counts, L.hits,
                                             L.result);
+        if (b + 1u < wave_bounces)
+            tr_shade<true><<<g, kShadeThreads, dyn, st>>>(d_params, b, in, hin, out, hout, L.counts, L.result);
         else
-            tr_intersect<<<g, 256, dyn, st>>>(d_params, b, in, L.counts, L.hits);
-        tr_shade<<<g, kShadeThreads, dyn, st>>>(d_params, b, in, L.hits, out, L.counts, L.result);
+            tr_shade<false><<<g, kShadeThreads, dyn, st>>>(d_params, b, in, hin, out, hout, L.counts, L.result);
     }
     if (L.max_depth > wave_bounces)
         tr_tail<<<L.grid, 256, dyn, st>>>(d_params, wave_bounces, (wave_bounces & 1u) ? L.qb : L.qa, L.counts,
                                           L.result);
-    tr_accumulate<<<(n_pixels + 255) / 256, 256, 0, st>>>(first_pixel, n_pixels, L.spp, L.result, L.sum, L.counts,
-                                                           L.max_depth, L.segments);
+    tr_accumulate<<<(n_pixels + kAccPixels - 1) / kAccPixels, 256, 0, st>>>(first_pixel, n_pixels, L.spp, L.result,
+                                                                             L.sum, L.counts, L.max_depth, L.segments);
     return cudaGetLastError();
 }
 

@@ -32,7 +32,7 @@ struct HitQueue {
 
 struct TracerLaunch {
     RayQueue qa, qb;
-    HitQueue hits;
+    HitQueue hits, hits2;   // hits of the bounce being shaded / of the next one
     uint32_t* counts;       // max_depth + 1 queue lengths
     float* result;          // 3 per path of the wave
     float* sum;             // 3 * w * h running sum

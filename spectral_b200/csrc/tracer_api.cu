@@ -52,9 +52,9 @@ struct sc_tracer {
         if (paths <= wave_cap) return SC_OK;
         drop_graph();
         const size_t n = paths;
-        // per chain: 2 ray queues x 8 floats, hits 4 floats, result 3; 2 ray queues x 3 u32, hit info
-        SC_CUDA(qbuf.alloc(kChains * (n * 8 * 2 + n * 4 + 3 * n)));
-        SC_CUDA(qbuf_u.alloc(kChains * (n * 3 * 2 + n)));
+        // per chain: 2 ray queues x 8 floats, 2 hit queues x 4 floats, result 3; 2 ray queues x 3 u32, 2 hit infos
+        SC_CUDA(qbuf.alloc(kChains * (n * 8 * 2 + n * 4 * 2 + 3 * n)));
+        SC_CUDA(qbuf_u.alloc(kChains * (n * 3 * 2 + n * 2)));
         float* f = qbuf.p;
         uint32_t* u = qbuf_u.p;
         for (uint32_t c = 0; c < kChains; ++c) {
@@ -67,12 +67,15 @@ struct sc_tracer {
                 q->rng = u; q->id = u + n; q->flags = u + 2 * n;
                 u += 3 * n;
             }
-            Lc.hits.t = f; Lc.hits.nx = f + n; Lc.hits.ny = f + 2 * n; Lc.hits.nz = f + 3 * n;
-            f += 4 * n;
+            HitQueue* hs[2] = {&Lc.hits, &Lc.hits2};
+            for (HitQueue* hq : hs) {
+                hq->t = f; hq->nx = f + n; hq->ny = f + 2 * n; hq->nz = f + 3 * n;
+                f += 4 * n;
+                hq->info = u;
+                u += n;
+            }
             Lc.result = f;
             f += 3 * n;
-            Lc.hits.info = u;
-            u += n;
         }
         wave_cap = paths;
         return SC_OK;

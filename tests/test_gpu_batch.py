@@ -117,3 +117,36 @@ def test_async_readback_overlaps_next_pass(ctx):
     b.synchronize()
     for k in range(4):
         assert bufs[k].tobytes() == (ref1 if k % 2 == 0 else ref2).tobytes(), k
+
+
+def test_mixed_free_flight_batch_and_variant_switch(ctx):
+    """A batch holding a free-flight job (estimator 3) and uniform ones runs the
+    kernel built with free-flight sampling; each image equals its plain
+    per-scene launch and the oracle.  Switching that job to the uniform
+    estimator with update_jobs swaps the kernel (and the captured graph): the
+    replayed pass gives the images of a fresh batch of the updated jobs."""
+    specs = small_specs(4, seed=0xFF)
+    jobs = prism_jobs(specs)
+    jobs[1].opts.estimator = 3
+    jobs[1].weights.sigma_t = 0.3
+    b = Batch(ctx, jobs)
+    b.run()
+    batched = [b.read_xyz(i) for i in range(len(jobs))]
+    b.run_plain()
+    for i in range(len(jobs)):
+        assert batched[i].tobytes() == b.read_xyz(i).tobytes(), i
+        exp = oracle_xyz(jobs[i])
+        assert exp.sum() > 0 and rel_l1(batched[i], exp) < FAST_TOL, i
+    jobs2 = prism_jobs(specs)
+    jobs2[1].weights.sigma_t = 0.3  # the same weights, now the uniform estimator
+    b.update_jobs(jobs2)
+    b.run()
+    switched = [b.read_xyz(i) for i in range(len(jobs2))]
+    fresh = Batch(ctx, jobs2)
+    fresh.run()
+    for i in range(len(jobs2)):
+        assert switched[i].tobytes() == fresh.read_xyz(i).tobytes(), i
+    assert switched[1].tobytes() != batched[1].tobytes()  # another estimator of the same scene
+    assert rel_l1(switched[1], oracle_xyz(jobs2[1])) < FAST_TOL
+    fresh.close()
+    b.close()
