@@ -1190,7 +1190,8 @@ def run_gpu_batch(args, rank, world, local_rank):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    plain_ms = timed(b.run_plain, max(2, args.steps // 2))
+    with torch.cuda.nvtx.range("plain"):  # nvtx range for an ncu launch list of the plain path
+        plain_ms = timed(b.run_plain, max(2, args.steps // 2))
     # plain per-scene launches through the drop-in object API (what a caller of
     # the reference's GpuPhotonFilm does per scene): create, trace, read back,
     # free.  The film's buffers come from the context's memory pool, so after

@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(256) tr_generate(const TracerParams* __restric
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         counts[0] = n_paths;
-        for (uint32_t b = 1; b <= gp->max_depth; ++b) counts[b] = 0u;
+        for (uint32_t b = 1; b <= gp->max_depth + 1u; ++b) counts[b] = 0u;  // + the tail's work counter
     }
     if (i >= n_paths) return;
     const uint32_t W = gp->width, H = gp->height;
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(256) tr_primary(const TracerParams* __restrict
     extern __shared__ __align__(16) unsigned char dyn[];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         counts[0] = n_paths;
-        for (uint32_t b = 1; b <= gp->max_depth; ++b) counts[b] = 0u;
+        for (uint32_t b = 1; b <= gp->max_depth + 1u; ++b) counts[b] = 0u;  // + the tail's work counter
     }
     if (blockIdx.x * blockDim.x >= n_paths) return;
     const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
@@ -292,9 +292,12 @@ __global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __
 }
 
 // Late bounces: by the third bounce only a few per cent of a wave's paths are
-// alive, and a launch pair per bounce costs more than the work.  One thread per
-// remaining path runs the rest of its bounces in place (the same hit and shade
-// code, so the image is unchanged); its segments are added to counts[first + 1].
+// alive, and a launch pair per bounce costs more than the work.  The rest of
+// each remaining path runs in place (the same hit and shade code, so the image
+// is unchanged), and a lane whose path ends takes the next path of the queue:
+// idle lanes of a warp claim new paths together (one atomic on the work counter
+// counts[max_depth + 1]), so the lanes stay busy although the paths end after
+// different numbers of bounces.  Segments are added to counts[first + 1].
 __global__ void __launch_bounds__(256) tr_tail(const TracerParams* __restrict__ gp, uint32_t first, RayQueue q,
                                                uint32_t* counts, float* result) {
     __shared__ TracerSmem s;
@@ -302,23 +305,46 @@ __global__ void __launch_bounds__(256) tr_tail(const TracerParams* __restrict__ 
     const uint32_t n = counts[first];
     if (blockIdx.x * blockDim.x >= n) return;
     const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
-    uint32_t segs = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        PathState P;
-        P.o = mk(q.ox[i], q.oy[i], q.oz[i]);
-        P.d = mk(q.dx[i], q.dy[i], q.dz[i]);
-        P.tp = q.tp[i]; P.u = q.u[i]; P.rs = q.rng[i]; P.id = q.id[i]; P.flags = q.flags[i];
-        for (uint32_t b = first; b < s.p.max_depth; ++b) {
+    uint32_t* work = counts + s.p.max_depth + 1u;
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t segs = 0, b = first;
+    bool have = false, drained = false;
+    PathState P;
+    P.o = P.d = mk(0.0f, 0.0f, 0.0f);
+    P.tp = P.u = 0.0f;
+    P.rs = P.id = P.flags = 0u;
+    for (;;) {
+        const unsigned idle = drained ? 0u : __ballot_sync(0xffffffffu, !have);
+        if (idle) {
+            const uint32_t leader = (uint32_t)__ffs(idle) - 1u;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(work, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + (uint32_t)__popc(idle) >= n) drained = true;  // the queue is used up
+            if (!have) {
+                const uint32_t i = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
+                if (i < n) {
+                    P.o = mk(q.ox[i], q.oy[i], q.oz[i]);
+                    P.d = mk(q.dx[i], q.dy[i], q.dz[i]);
+                    P.tp = q.tp[i]; P.u = q.u[i]; P.rs = q.rng[i]; P.id = q.id[i]; P.flags = q.flags[i];
+                    b = first;
+                    have = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, have)) break;
+        if (have) {
             float t;
             f3 nrm;
             uint32_t info;
             trace_hit(s, S, P.o, P.d, t, nrm, info);
             if (b > first) ++segs;  // counts[first] already holds this bounce's rays
-            if (!shade_path(s, S, b, P, t, nrm, info, result)) break;
+            have = shade_path(s, S, b, P, t, nrm, info, result);
+            ++b;
         }
     }
     for (int o = 16; o > 0; o >>= 1) segs += __shfl_xor_sync(0xffffffffu, segs, o);
-    if ((threadIdx.x & 31u) == 0 && segs) atomicAdd(counts + first + 1, segs);
+    if (lane == 0 && segs) atomicAdd(counts + first + 1, segs);
 }
 
 // Per-pixel sample sum in sample order (tracer.rs:121-135), added to the running
