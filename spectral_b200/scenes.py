@@ -10,6 +10,8 @@
   photons log-U(2^14, 2^22), square film side log-U(128, 1024)), drawn from a
   PCG-seeded generator so a seed fixes the whole batch.
 """
+import math
+
 import numpy as np
 
 from . import BK7, FUSED_SILICA, SF11, WATER, Beam, Camera, Dielectric, Lambertian, Scene, Screen  # noqa: F401
