@@ -72,10 +72,10 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(const BatchJobDev* __r
         SceneView S;
         S.prims = slot.prims; S.planes = slot.planes; S.mats = slot.mats; S.n_prims = slot.p.n_prims;
         if (SPLIT) {
-            for (uint32_t b0 = 0; b0 < item.count; b0 += 32u)
-                trace_warp_split<true, AGG, FF, kBatchWarpSegs>(slot.p, S, cmf, item.begin + b0 + lane,
-                                                                b0 + lane < item.count, cur_words ? mask : nullptr,
-                                                                split[warp]);
+            const uint32_t first = item.begin;
+            trace_warp_range<true, AGG, FF, kBatchWarpSegs>(slot.p, S, cmf, item.count,
+                                                            [first](uint32_t k) { return first + k; },
+                                                            cur_words ? mask : nullptr, split[warp]);
         } else {
             for (uint32_t i = lane; i < item.count; i += 32u)
                 trace_photon<true, AGG, false, false, FF>(slot.p, S, cmf, item.begin + i, cur_words ? mask : nullptr);

@@ -40,16 +40,17 @@ __global__ void __launch_bounds__(256, MINB) photon_kernel(const PhotonParams p,
     uint32_t* smask;
     const SceneView S = load_scene(p, smem, &cmf, &smask, mask_words);
     if (SPLIT) {  // warp-split transport: per-warp segment buffers after the scene
+        // each warp takes one contiguous share of the launch's photons, which its
+        // lanes work through with refill (the grid is resident at once)
         using WS = WarpSplitSmem<kWarpSegs>;
         WS* ws = reinterpret_cast<WS*>(smem + split_offset(p, mask_words));
-        const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-        const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-        for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < p.photon_count; base += warps * 32u) {
-            const uint32_t i = base + lane;
-            const bool valid = i < p.photon_count;
-            const uint32_t k = p.order && valid ? p.order[i] : i;
-            trace_warp_split<SPEC, AGG, FF, kWarpSegs>(p, S, cmf, p.photon_base + k, valid, smask, ws[warp]);
-        }
+        const uint32_t warp = threadIdx.x >> 5;
+        const uint32_t warps = gridDim.x * (blockDim.x >> 5), gw = blockIdx.x * (blockDim.x >> 5) + warp;
+        const uint32_t begin = (uint32_t)((uint64_t)p.photon_count * gw / warps);
+        const uint32_t end = (uint32_t)((uint64_t)p.photon_count * (gw + 1u) / warps);
+        trace_warp_range<SPEC, AGG, FF, kWarpSegs>(
+            p, S, cmf, end - begin,
+            [&](uint32_t k) { return p.photon_base + (p.order ? p.order[begin + k] : begin + k); }, smask, ws[warp]);
     } else {
         const uint32_t stride = gridDim.x * blockDim.x;
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += stride)

@@ -378,18 +378,17 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
 // uses draw pcg32(state_before + k + 1), exactly the draw the per-photon loop
 // makes, so paths and films are bit-identical to trace_photon's.
 // Segment record: the fast haze constants of the segment, the RNG state
-// before its 4 distance draws, and the photon's bin (spectral films) or lane
-// (XYZ films, whose CMF payload sits in the warp's payload table).
+// before its 4 distance draws, and the photon's splat payload: its bin
+// (spectral films) or the CMF x, y, z of its wavelength (XYZ films).
 struct alignas(16) SegRec {
     HazeSeg hz;
-    uint32_t rng, tag;
-    uint32_t pad[3];
+    uint32_t rng, bin;
+    float cx, cy, cz;
 };
 static_assert(sizeof(SegRec) == 64, "segment record layout");
 template <uint32_t SEGS>
 struct alignas(16) WarpSplitSmem {
     SegRec seg[SEGS];
-    float4 payload[32];  // per lane: CMF x, y, z of the photon (XYZ film)
 };
 // Segments buffered per warp: 64 in the plain photon kernel, 48 in the batch
 // kernel (whose warps also hold a job slot and a dirty mask).
@@ -406,12 +405,8 @@ __device__ __forceinline__ void flush_loop(const PhotonParams& p, WarpSplitSmem<
         uint32_t px, py;
         float contrib;
         const bool ok = haze_fast<FF>(p, hz, draw24, px, py, contrib);
-        if (SPEC) {
-            deposit<true, AGG>(p, smask, ok, px, py, contrib, 0.f, 0.f, 0.f, R.tag, 1.0f);
-        } else {
-            const float4 pl = ws.payload[R.tag];
-            deposit<false, AGG>(p, smask, ok, px, py, contrib, pl.x, pl.y, pl.z, 0u, 1.0f);
-        }
+        if (SPEC) deposit<true, AGG>(p, smask, ok, px, py, contrib, 0.f, 0.f, 0.f, R.bin, 1.0f);
+        else deposit<false, AGG>(p, smask, ok, px, py, contrib, R.cx, R.cy, R.cz, 0u, 1.0f);
     }
 }
 
@@ -425,59 +420,70 @@ __device__ __forceinline__ void flush_segments(const PhotonParams& p, WarpSplitS
     __syncwarp();
 }
 
-// All 32 lanes of the warp must call this together; lanes without a photon pass
-// valid = false.
-template <bool SPEC, int AGG, bool FFOK, uint32_t SEGS>
-__device__ __forceinline__ void trace_warp_split(const PhotonParams& p, const SceneView& S, const float* cmf,
-                                                 uint32_t idx, bool valid, uint32_t* smask, WarpSplitSmem<SEGS>& ws) {
+// The photons of positions [0, count) of a range (photon id = id(k)) through
+// the warp-split transport.  All 32 lanes of the warp call this together.  A
+// lane whose photon has ended (escaped, or out of bounces) takes the next
+// unclaimed photon of the range at the next bounce, so the lanes stay busy
+// through the bounce loop although photons end after different numbers of
+// segments; the photons, their RNG draws and their samples are the same, so
+// the film is bit-identical to the per-photon transport's.
+template <bool SPEC, int AGG, bool FFOK, uint32_t SEGS, class Id>
+__device__ __forceinline__ void trace_warp_range(const PhotonParams& p, const SceneView& S, const float* cmf,
+                                                 uint32_t count, Id id, uint32_t* smask, WarpSplitSmem<SEGS>& ws) {
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
-    Rng r = Rng::make(idx, p.seed);
-    f3 o = mk(0.f, 0.f, 0.f), d = p.bdir;
-    float lambda = 0.0f, power = 1.0f;
-    uint32_t tag = lane;  // spectral films: the photon's bin
-    if (valid) {
-        const float r1 = r.f32();
-        const float r2 = r.f32();
-        o = add(add(p.corner, mul(p.bu, r1)), mul(p.bv, r2));
-        lambda = p.lambda_min + p.lambda_range * r.f32();
-        float cx = 0.f, cy = 0.f, cz = 0.f;
-        uint32_t bin = 0;
-        photon_payload(p, cmf, lambda, cx, cy, cz, bin, SPEC);
-        if (SPEC) tag = bin;
-        else ws.payload[lane] = make_float4(cx, cy, cz, 0.0f);
-    }
     const bool ff = FFOK && free_flight(p);
-    bool alive = valid;
-    uint32_t n = 0;  // buffered segments, the same in every lane
-    uint32_t n_glass = 0xFFFFFFFFu;
+    Rng r;
+    r.state = 0u;
+    f3 o = mk(0.f, 0.f, 0.f), d = p.bdir;
+    float lambda = 0.0f, power = 1.0f, cx = 0.f, cy = 0.f, cz = 0.f;
+    uint32_t bin = 0, bounce = 0, n_glass = 0xFFFFFFFFu;
     float n_cached = 1.0f;
-    for (uint32_t b = 0;; ++b) {
-        const unsigned m = b < p.max_bounces ? __ballot_sync(0xffffffffu, alive) : 0u;
+    bool alive = false;
+    uint32_t next = 0;  // first unclaimed position of the range (the same in every lane)
+    uint32_t n = 0;     // buffered segments (the same in every lane)
+    for (;;) {
+        if (next < count) {  // idle lanes start the next photons of the range
+            const unsigned idle = __ballot_sync(0xffffffffu, !alive);
+            const uint32_t k = next + __popc(idle & below);
+            if (!alive && k < count) {
+                r = Rng::make(id(k), p.seed);
+                const float r1 = r.f32();
+                const float r2 = r.f32();
+                o = add(add(p.corner, mul(p.bu, r1)), mul(p.bv, r2));
+                d = p.bdir;
+                lambda = p.lambda_min + p.lambda_range * r.f32();
+                photon_payload(p, cmf, lambda, cx, cy, cz, bin, SPEC);
+                power = 1.0f;
+                bounce = 0;
+                n_glass = 0xFFFFFFFFu;
+                alive = p.max_bounces > 0u;
+            }
+            next += __popc(idle);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, alive);
         const uint32_t cnt = __popc(m);
-        // one flush site (keeps the inlined haze code single): when this bounce's
-        // segments do not fit, and once when every photon is done
+        // one flush site (keeps the inlined haze code single): when this round's
+        // segments do not fit, and once when the range is done
         if (n + cnt > SEGS || (m == 0u && n)) {
             flush_segments<SPEC, AGG, FFOK, SEGS>(p, ws, n, smask, lane);
             n = 0;
         }
-        if (m == 0u) break;
-        Hit h;
-        uint32_t mi = 0;
-        bool any = false;
-        float seg = 0.0f;
+        if (m == 0u) break;  // nothing alive and nothing left to start
         if (alive) {
-            any = scene_hit(S, o, d, h, mi);
-            seg = any ? h.t : p.max_dist;
-        }
-        if (alive) {
+            Hit h;
+            uint32_t mi = 0;
+            const bool any = scene_hit(S, o, d, h, mi);
+            const float seg = any ? h.t : p.max_dist;
             SegRec& R = ws.seg[n + __popc(m & below)];
             R.hz = ff ? haze_setup<true>(p, o, d, seg, power) : haze_setup<false>(p, o, d, seg, power);
             R.rng = r.state;
-            R.tag = tag;
+            R.bin = bin;
+            R.cx = cx; R.cy = cy; R.cz = cz;
             r.state += 4u;  // this segment's 4 distance draws, made by the flush
-            if (!any) {
-                alive = false;
+            ++bounce;
+            if (!any || bounce >= p.max_bounces) {
+                alive = false;  // escaped, or its last segment: no scatter needed
             } else {
                 const sc_material& mt = S.mats[mi];
                 float nh = 1.0f;

@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(256) tr_generate(const TracerParams* __restric
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         counts[0] = n_paths;
-        for (uint32_t b = 1; b <= gp->max_depth + 1u; ++b) counts[b] = 0u;  // + the tail's work counter
+        for (uint32_t b = 1; b <= gp->max_depth; ++b) counts[b] = 0u;
     }
     if (i >= n_paths) return;
     const uint32_t W = gp->width, H = gp->height;
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(256) tr_primary(const TracerParams* __restrict
     extern __shared__ __align__(16) unsigned char dyn[];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         counts[0] = n_paths;
-        for (uint32_t b = 1; b <= gp->max_depth + 1u; ++b) counts[b] = 0u;  // + the tail's work counter
+        for (uint32_t b = 1; b <= gp->max_depth; ++b) counts[b] = 0u;
     }
     if (blockIdx.x * blockDim.x >= n_paths) return;
     const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
@@ -292,12 +292,9 @@ __global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __
 }
 
 // Late bounces: by the third bounce only a few per cent of a wave's paths are
-// alive, and a launch pair per bounce costs more than the work.  The rest of
-// each remaining path runs in place (the same hit and shade code, so the image
-// is unchanged), and a lane whose path ends takes the next path of the queue:
-// idle lanes of a warp claim new paths together (one atomic on the work counter
-// counts[max_depth + 1]), so the lanes stay busy although the paths end after
-// different numbers of bounces.  Segments are added to counts[first + 1].
+// alive, and a launch pair per bounce costs more than the work.  One thread per
+// remaining path runs the rest of its bounces in place (the same hit and shade
+// code, so the image is unchanged); its segments are added to counts[first + 1].
 __global__ void __launch_bounds__(256) tr_tail(const TracerParams* __restrict__ gp, uint32_t first, RayQueue q,
                                                uint32_t* counts, float* result) {
     __shared__ TracerSmem s;
@@ -305,83 +302,45 @@ __global__ void __launch_bounds__(256) tr_tail(const TracerParams* __restrict__ 
     const uint32_t n = counts[first];
     if (blockIdx.x * blockDim.x >= n) return;
     const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
-    uint32_t* work = counts + s.p.max_depth + 1u;
-    const uint32_t lane = threadIdx.x & 31u;
-    uint32_t segs = 0, b = first;
-    bool have = false, drained = false;
-    PathState P;
-    P.o = P.d = mk(0.0f, 0.0f, 0.0f);
-    P.tp = P.u = 0.0f;
-    P.rs = P.id = P.flags = 0u;
-    for (;;) {
-        const unsigned idle = drained ? 0u : __ballot_sync(0xffffffffu, !have);
-        if (idle) {
-            const uint32_t leader = (uint32_t)__ffs(idle) - 1u;
-            uint32_t base = 0;
-            if (lane == leader) base = atomicAdd(work, (uint32_t)__popc(idle));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (base + (uint32_t)__popc(idle) >= n) drained = true;  // the queue is used up
-            if (!have) {
-                const uint32_t i = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
-                if (i < n) {
-                    P.o = mk(q.ox[i], q.oy[i], q.oz[i]);
-                    P.d = mk(q.dx[i], q.dy[i], q.dz[i]);
-                    P.tp = q.tp[i]; P.u = q.u[i]; P.rs = q.rng[i]; P.id = q.id[i]; P.flags = q.flags[i];
-                    b = first;
-                    have = true;
-                }
-            }
-        }
-        if (!__any_sync(0xffffffffu, have)) break;
-        if (have) {
+    uint32_t segs = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        PathState P;
+        P.o = mk(q.ox[i], q.oy[i], q.oz[i]);
+        P.d = mk(q.dx[i], q.dy[i], q.dz[i]);
+        P.tp = q.tp[i]; P.u = q.u[i]; P.rs = q.rng[i]; P.id = q.id[i]; P.flags = q.flags[i];
+        for (uint32_t b = first; b < s.p.max_depth; ++b) {
             float t;
             f3 nrm;
             uint32_t info;
             trace_hit(s, S, P.o, P.d, t, nrm, info);
             if (b > first) ++segs;  // counts[first] already holds this bounce's rays
-            have = shade_path(s, S, b, P, t, nrm, info, result);
-            ++b;
+            if (!shade_path(s, S, b, P, t, nrm, info, result)) break;
         }
     }
     for (int o = 16; o > 0; o >>= 1) segs += __shfl_xor_sync(0xffffffffu, segs, o);
-    if (lane == 0 && segs) atomicAdd(counts + first + 1, segs);
+    if ((threadIdx.x & 31u) == 0 && segs) atomicAdd(counts + first + 1, segs);
 }
 
 // Per-pixel sample sum in sample order (tracer.rs:121-135), added to the running
-// sum.  A CTA takes 64 pixels: its 256 threads stage 64 samples of them at a
-// time into shared memory with coalesced loads (the 192 floats of a sample's
-// 64 pixels are contiguous), then 192 threads, one per (pixel, channel), add
-// the staged samples in sample order.
-constexpr uint32_t kAccPixels = 64, kAccSamples = 64;
+// sum.  One thread per (pixel, channel) of the wave: consecutive threads read
+// consecutive floats of each sample (coalesced), and each adds its samples in
+// sample order.
 __global__ void __launch_bounds__(256) tr_accumulate(uint32_t first_pixel, uint32_t n_pixels, uint32_t spp,
                                                      const float* __restrict__ result, float* sum,
                                                      const uint32_t* __restrict__ counts, uint32_t max_depth,
                                                      unsigned long long* segments) {
-    __shared__ float st[kAccSamples * 3 * kAccPixels];
-    const uint32_t tid = threadIdx.x;
-    if (blockIdx.x == 0 && tid == 0) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j == 0) {
         unsigned long long t = 0;
         for (uint32_t b = 0; b < max_depth; ++b) t += counts[b];
         atomicAdd(segments, t);  // both wave chains add here
     }
-    const uint32_t p0 = blockIdx.x * kAccPixels;
-    const uint32_t np = min(kAccPixels, n_pixels - p0);
-    const uint32_t row = 3u * np;  // floats of one sample of this CTA's pixels
+    const uint32_t n = 3u * n_pixels;
+    if (j >= n) return;
     float a = 0.0f;
-    for (uint32_t s0 = 0; s0 < spp; s0 += kAccSamples) {
-        const uint32_t ns = min(kAccSamples, spp - s0);
-        __syncthreads();
-        for (uint32_t k = tid; k < ns * row; k += blockDim.x) {
-            const uint32_t s = k / row, e = k - s * row;
-            st[s * 3u * kAccPixels + e] = result[3u * ((size_t)(s0 + s) * n_pixels + p0) + e];
-        }
-        __syncthreads();
-        if (tid < row) {
-#pragma unroll 8
-            for (uint32_t s = 0; s < ns; ++s) a += st[s * 3u * kAccPixels + tid];
-        }
-    }
-    if (tid < row) sum[3u * (size_t)(first_pixel + p0) + tid] += a;
+#pragma unroll 16
+    for (uint32_t s = 0; s < spp; ++s) a += result[(size_t)s * n + j];  // loads run ahead; adds in sample order
+    sum[3u * (size_t)first_pixel + j] += a;
 }
 
 }  // namespace
@@ -425,8 +384,8 @@ cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch&
     if (L.max_depth > wave_bounces)
         tr_tail<<<L.grid, 256, dyn, st>>>(d_params, wave_bounces, (wave_bounces & 1u) ? L.qb : L.qa, L.counts,
                                           L.result);
-    tr_accumulate<<<(n_pixels + kAccPixels - 1) / kAccPixels, 256, 0, st>>>(first_pixel, n_pixels, L.spp, L.result,
-                                                                             L.sum, L.counts, L.max_depth, L.segments);
+    tr_accumulate<<<(3 * n_pixels + 255) / 256, 256, 0, st>>>(first_pixel, n_pixels, L.spp, L.result, L.sum, L.counts,
+                                                               L.max_depth, L.segments);
     return cudaGetLastError();
 }
 
