@@ -30,7 +30,7 @@ struct PhotonParams {
     uint32_t haze_exact;              // 1: haze samples in the CPU crate's operation order (per-photon kernel)
     // Launch constants of the fast haze samples, filled by set_haze_consts()
     // from the fields above just before a launch.
-    float hz_w, hz_h;                 // film width and height
+    float hz_w, hz_h, hz_hw, hz_hh;   // film width and height, and their halves
     float hz_sx, hz_sy;               // W / |horizontal|, -H / |vertical|
     float hz_k, hz_kiso;              // sigma_s * 2^scale / 4 * HG numerator / (4 pi); isotropic estimator's
     float hz_kexp, hz_inv_sigma_t;    // -sigma_t * log2(e), 1 / sigma_t

@@ -297,6 +297,8 @@ void set_haze_consts(PhotonParams& p) {
     const double g = p.g;
     p.hz_w = (float)p.width;
     p.hz_h = (float)p.height;
+    p.hz_hw = 0.5f * p.hz_w;
+    p.hz_hh = 0.5f * p.hz_h;
     p.hz_sx = (float)((double)p.width / (double)p.proj.vw);
     p.hz_sy = (float)(-(double)p.height / (double)p.proj.vh);
     p.hz_k = (float)((double)p.sigma_s * (double)p.scale * 0.25 * (1.0 - g * g) / (4.0 * pi));

@@ -210,22 +210,27 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // expm1(-sigma_t seg) for free-flight distances.
 struct HazeSeg { float c0, c1, a0, a1, b0, b1, s0, s1, h2, k, segs; };
 
+// Dot product with fused multiply-adds (haze constants only: the transport
+// keeps the reference's separate multiplies and adds).
+__device__ __forceinline__ float fdot(f3 a, f3 b) { return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, a.x * b.x)); }
+
 template <bool FF>
 __device__ __forceinline__ HazeSeg haze_setup(const PhotonParams& p, f3 o, f3 d, float seg, float power) {
     const Proj& P = p.proj;
     const f3 D = sub(o, P.o);
     HazeSeg h;
-    h.c0 = dot(D, P.w);
-    h.c1 = dot(d, P.w);
-    h.a0 = dot(D, P.u) * p.hz_sx;
-    h.a1 = dot(d, P.u) * p.hz_sx;
-    h.b0 = dot(D, P.v) * p.hz_sy;
-    h.b1 = dot(d, P.v) * p.hz_sy;
-    const float e2 = dot(d, d);
-    const float tstar = -dot(D, d) / e2;
-    const f3 m = add(D, mul(d, tstar));
-    h.h2 = dot(m, m);
-    h.s1 = sqrtf(e2);
+    h.c0 = fdot(D, P.w);
+    h.c1 = fdot(d, P.w);
+    h.a0 = fdot(D, P.u) * p.hz_sx;
+    h.a1 = fdot(d, P.u) * p.hz_sx;
+    h.b0 = fdot(D, P.v) * p.hz_sy;
+    h.b1 = fdot(d, P.v) * p.hz_sy;
+    const float e2 = fdot(d, d);
+    const float r2 = rsqrt_approx(e2);                 // 1 / |d|
+    const float tstar = -fdot(D, d) * (r2 * r2);
+    const f3 m = mk(__fmaf_rn(d.x, tstar, D.x), __fmaf_rn(d.y, tstar, D.y), __fmaf_rn(d.z, tstar, D.z));
+    h.h2 = fdot(m, m);
+    h.s1 = e2 * r2;                                    // |d|
     h.s0 = -h.s1 * tstar;
     if (FF) {
         const float em = expm1f(-p.sigma_t * seg);
@@ -248,8 +253,8 @@ __device__ __forceinline__ bool haze_fast(const PhotonParams& p, const HazeSeg& 
     else t = (float)draw24 * h.segs;
     const float c = __fmaf_rn(h.c1, t, h.c0);
     const float rc = rcp_approx(-c);
-    const float x = __fmaf_rn(__fmaf_rn(h.a1, t, h.a0), rc, 0.5f * p.hz_w);
-    const float y = __fmaf_rn(__fmaf_rn(h.b1, t, h.b0), rc, 0.5f * p.hz_h);
+    const float x = __fmaf_rn(__fmaf_rn(h.a1, t, h.a0), rc, p.hz_hw);
+    const float y = __fmaf_rn(__fmaf_rn(h.b1, t, h.b0), rc, p.hz_hh);
     contrib = 0.0f;
     px = py = 0u;
     if (!(c < -1e-6f && x >= 0.0f && x < p.hz_w && y > 0.0f && y <= p.hz_h)) return false;
