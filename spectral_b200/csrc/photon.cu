@@ -40,17 +40,23 @@ __global__ void __launch_bounds__(256, MINB) photon_kernel(const PhotonParams p,
     uint32_t* smask;
     const SceneView S = load_scene(p, smem, &cmf, &smask, mask_words);
     if (SPLIT) {  // warp-split transport: per-warp segment buffers after the scene
-        // each warp takes one contiguous share of the launch's photons, which its
-        // lanes work through with refill (the grid is resident at once)
+        // warps take chunks of the launch's photons in grid-stride order (so the
+        // photons in flight stay close in launch order: the wavelength-ordered
+        // dispatch relies on it), and the lanes work through a chunk with refill;
+        // chunks of up to 512 photons, smaller when that leaves warps idle
         using WS = WarpSplitSmem<kWarpSegs>;
         WS* ws = reinterpret_cast<WS*>(smem + split_offset(p, mask_words));
         const uint32_t warp = threadIdx.x >> 5;
         const uint32_t warps = gridDim.x * (blockDim.x >> 5), gw = blockIdx.x * (blockDim.x >> 5) + warp;
-        const uint32_t begin = (uint32_t)((uint64_t)p.photon_count * gw / warps);
-        const uint32_t end = (uint32_t)((uint64_t)p.photon_count * (gw + 1u) / warps);
-        trace_warp_range<SPEC, AGG, FF, kWarpSegs>(
-            p, S, cmf, end - begin,
-            [&](uint32_t k) { return p.photon_base + (p.order ? p.order[begin + k] : begin + k); }, smask, ws[warp]);
+        const uint32_t per = (uint32_t)(((uint64_t)p.photon_count + warps - 1u) / warps);
+        const uint32_t chunk = min(512u, max(32u, (per + 31u) & ~31u));
+        for (uint64_t base = (uint64_t)gw * chunk; base < p.photon_count; base += (uint64_t)warps * chunk) {
+            const uint32_t b0 = (uint32_t)base;
+            const uint32_t cnt = min(chunk, p.photon_count - b0);
+            trace_warp_range<SPEC, AGG, FF, kWarpSegs>(
+                p, S, cmf, cnt, [&](uint32_t k) { return p.photon_base + (p.order ? p.order[b0 + k] : b0 + k); },
+                smask, ws[warp]);
+        }
     } else {
         const uint32_t stride = gridDim.x * blockDim.x;
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += stride)
