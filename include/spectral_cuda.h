@@ -375,7 +375,8 @@ int sc_batch_update_jobs(sc_batch* b, const sc_scene_job* jobs, uint32_t n_jobs)
 /* One pass over every job (graph replay); stream NULL = the batch's stream.
  * Asynchronous; afterwards each job's XYZ image is ready and its film drained. */
 int sc_batch_run(sc_batch* b, void* stream);
-/* The same work as plain per-scene launches (trace + drain/reduce per job). */
+/* The same work as plain per-scene launches (trace + drain/reduce per job),
+ * each trace launched as a single film's is (sc_trace_photons_device). */
 int sc_batch_run_plain(sc_batch* b, void* stream);
 int sc_batch_synchronize(sc_batch* b);
 int sc_batch_read_xyz(sc_batch* b, uint32_t job, float* out);
