@@ -74,7 +74,8 @@ typedef struct {
                                reference): the 4 distances of a segment follow sigma_t exp(-sigma_t t)
                                restricted to the segment, weighted by 1/pdf: the same integral */
     uint32_t haze_exact;    /* 0: haze samples (camera projection, distance, transmittance, phase) in
-                               fast f32 arithmetic, within 1e-3 relative L1 of the CPU crate's film;
+                               fast f32 arithmetic, within 2e-3 relative L1 of the CPU crate's film
+                               (the bar the tests hold it to);
                                1: in the CPU crate's operation order (volume.rs:130-150), film cells
                                within a few fixed-point quanta of it, slower.  Photon paths, the RNG
                                stream and the film's integer sums are the same either way.  Photon
