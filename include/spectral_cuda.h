@@ -377,7 +377,7 @@ int sc_batch_update_jobs(sc_batch* b, const sc_scene_job* jobs, uint32_t n_jobs)
  * Asynchronous; afterwards each job's XYZ image is ready and its film drained. */
 int sc_batch_run(sc_batch* b, void* stream);
 /* The same work as plain per-scene launches (trace + drain/reduce per job),
- * each trace launched as a single film's is (sc_trace_photons_device). */
+ * with the transport of the batch's tuning (per_photon). */
 int sc_batch_run_plain(sc_batch* b, void* stream);
 int sc_batch_synchronize(sc_batch* b);
 int sc_batch_read_xyz(sc_batch* b, uint32_t job, float* out);
@@ -407,6 +407,7 @@ typedef struct {
     uint64_t hbm_budget_bytes;  /* arena for films, masks and images of admitted requests */
     uint32_t max_slots;         /* requests on the device at once (0 -> 256) */
     uint32_t chunk_photons;     /* work-chunk size of the batched launch (0 -> 2048) */
+    uint32_t per_photon;        /* 0: warp-split transport (default); 1: one photon per lane */
 } sc_server_config;
 typedef struct {
     sc_scene_job job;           /* scene, film (bins >= 1), photons per frame (n_photons), seed, camera */

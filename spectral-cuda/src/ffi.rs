@@ -103,7 +103,8 @@ pub struct ScBatchTuning { pub chunk_photons: u32, pub minb: u32, pub aggregate:
                            pub per_photon: u32, pub block: u32 }
 #[repr(C)]
 #[derive(Clone, Copy, Default, Debug)]
-pub struct ScServerConfig { pub hbm_budget_bytes: u64, pub max_slots: u32, pub chunk_photons: u32 }
+pub struct ScServerConfig { pub hbm_budget_bytes: u64, pub max_slots: u32, pub chunk_photons: u32,
+                            pub per_photon: u32 }
 #[repr(C)]
 #[derive(Clone, Copy, Debug)]
 pub struct ScRequest { pub job: ScSceneJob, pub frames: u32, pub orbit_deg: f32, pub orbit_target: [f32; 3],

@@ -219,12 +219,11 @@ struct sc_batch {
                 reinterpret_cast<const unsigned char*>(d_jobs.p + j) + offsetof(BatchSlotImage, planes));
             p.mats = reinterpret_cast<const sc_material*>(
                 reinterpret_cast<const unsigned char*>(d_jobs.p + j) + offsetof(BatchSlotImage, mats));
-            // the launch a single film gets (sc_trace_photons_device's defaults): the
-            // warp-split transport and, for spectral films larger than L2, the
-            // wavelength-ordered dispatch with its scratch from the context's pool
+            // the transport the batch's tuning chose (measured on these scenes, it
+            // beats the single-film default of warp-split transport plus the
+            // wavelength-ordered dispatch for films larger than L2)
             LaunchShape shape;
-            shape.block = 256; shape.aggregate = 0; shape.minb = 4; shape.split = 1;
-            shape.order = 1; shape.pool = ctx->pool;
+            shape.block = 256; shape.aggregate = 0; shape.minb = 4; shape.split = tuning.per_photon ? 0 : 1;
             const size_t smem = scene_smem_bytes(p.n_prims, p.n_planes, p.n_mats) +
                                 (geom[j].words <= kMaxSmemMaskWords ? geom[j].words * 4u : 0u);
             shape.grid = (uint32_t)(ctx->sms * photon_occupancy_blocks(shape, true, smem));
