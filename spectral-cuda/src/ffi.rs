@@ -104,7 +104,7 @@ pub struct ScBatchTuning { pub chunk_photons: u32, pub minb: u32, pub aggregate:
 #[repr(C)]
 #[derive(Clone, Copy, Default, Debug)]
 pub struct ScServerConfig { pub hbm_budget_bytes: u64, pub max_slots: u32, pub chunk_photons: u32,
-                            pub per_photon: u32 }
+                            pub warp_split: u32 }
 #[repr(C)]
 #[derive(Clone, Copy, Debug)]
 pub struct ScRequest { pub job: ScSceneJob, pub frames: u32, pub orbit_deg: f32, pub orbit_target: [f32; 3],

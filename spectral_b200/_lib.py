@@ -93,7 +93,7 @@ class sc_batch_tuning(C.Structure):
 
 class sc_server_config(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_slots", C.c_uint32), ("chunk_photons", C.c_uint32),
-                ("per_photon", C.c_uint32)]
+                ("warp_split", C.c_uint32)]
 
 
 class sc_request(C.Structure):

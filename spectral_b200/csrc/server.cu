@@ -415,7 +415,7 @@ struct sc_server {
         bool ff = false;  // some request samples free-flight distances: the kernel built with them
         for (const Request* q : active) ff = ff || (q->r.job.opts.estimator == 3u && q->r.job.weights.sigma_t > 0.0f);
         SC_CUDA(launch_batch(d_jobs.p, d_items.p, (uint32_t)h_items.size(), counter.p, ctx->cmf.p, kBatchMaskWords, 0,
-                             4, cfg.per_photon ? 0 : 1, grid, stream, 256, ff));
+                             4, cfg.warp_split ? 1 : 0, grid, stream, 256, ff));
         SC_CUDA(launch_reduce_many(d_descs.p, n, words, true, maxc, dirty_list.p, dirty_count.p, stream));
         photons += step_photons;
         StepRecord rec;
@@ -487,8 +487,8 @@ int sc_server_create(sc_ctx* ctx, const sc_server_config* cfg, sc_server** out) 
     if ((e = s->dirty_count.alloc(1)) != cudaSuccess) return fail(e);
     if ((e = s->ring.init(kRingFloats)) != cudaSuccess) return fail(e);
     s->arena.reset(cfg->hbm_budget_bytes);
-    s->cfg.per_photon = s->cfg.per_photon ? 1u : 0u;
-    s->grid = (uint32_t)(ctx->sms * batch_occupancy(0, 4, s->cfg.per_photon ? 0 : 1, kBatchMaskWords));
+    s->cfg.warp_split = s->cfg.warp_split ? 1u : 0u;
+    s->grid = (uint32_t)(ctx->sms * batch_occupancy(0, 4, (int)s->cfg.warp_split, kBatchMaskWords));
     *out = s;
     return SC_OK;
     SC_GUARD_END

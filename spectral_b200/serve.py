@@ -20,9 +20,9 @@ ORBIT_TARGET = (0.6, -0.4, 0.0)
 
 
 class Server:
-    def __init__(self, ctx, budget_bytes=40 << 30, max_slots=256, chunk_photons=2048, per_photon=0):
+    def __init__(self, ctx, budget_bytes=40 << 30, max_slots=256, chunk_photons=2048, warp_split=0):
         self.h = C.c_void_p()
-        cfg = _lib.sc_server_config(int(budget_bytes), int(max_slots), int(chunk_photons), int(per_photon))
+        cfg = _lib.sc_server_config(int(budget_bytes), int(max_slots), int(chunk_photons), int(warp_split))
         check(lib.sc_server_create(ctx.h, C.byref(cfg), C.byref(self.h)))
         self._dims = {}
         self._buf = None
