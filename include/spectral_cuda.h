@@ -407,8 +407,8 @@ typedef struct {
     uint64_t hbm_budget_bytes;  /* arena for films, masks and images of admitted requests */
     uint32_t max_slots;         /* requests on the device at once (0 -> 256) */
     uint32_t chunk_photons;     /* work-chunk size of the batched launch (0 -> 2048) */
-    uint32_t warp_split;        /* 0: one photon per lane (the default: faster on request mixes);
-                                   1: the warp-split transport */
+    uint32_t warp_split;        /* 0: one photon per lane (the default, as the batch autotuner picks
+                                   on uneven scenes); 1: the warp-split transport */
 } sc_server_config;
 typedef struct {
     sc_scene_job job;           /* scene, film (bins >= 1), photons per frame (n_photons), seed, camera */
