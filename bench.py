@@ -862,10 +862,14 @@ def served_summary(ctx, seconds, rank, clk=None):
     served = run_stream(srv, stream, want_image=True)
     srv.close()
     sample = [r for r in stream if r[0] < SERVE["sample_s"]]
-    srv = Server(ctx, budget_bytes=budget)
-    capacity = run_stream(srv, sample, time_scale=0.0, want_image=True)
-    srv.close()
-    plain = run_plain_stream(ctx, sample, time_scale=0.0)
+    capacity, plain = None, None
+    for _ in range(2):  # best of two: both are host-driven loops with run-to-run noise
+        srv = Server(ctx, budget_bytes=budget)
+        c = run_stream(srv, sample, time_scale=0.0, want_image=True)
+        srv.close()
+        p = run_plain_stream(ctx, sample, time_scale=0.0)
+        capacity = c if capacity is None or c["photons_per_s"] > capacity["photons_per_s"] else capacity
+        plain = p if plain is None or p["photons_per_s"] > plain["photons_per_s"] else plain
     return {
         "window_s": seconds, "rate_per_s": SERVE["rate"], "requests": len(stream),
         "sessions": sum(1 for r in stream if r[2] > 1), "frames": sum(r[2] for r in stream),
@@ -878,8 +882,8 @@ def served_summary(ctx, seconds, rank, clk=None):
         "served_over_plain": capacity["photons_per_s"] / plain["photons_per_s"],
         "sample": "latency: the first %.0f s of the stream (seed 0x%X) replayed in real time; capacity and plain: "
                   "its first %.0f s (%d requests, %d frames) submitted at once to the server and to a film object "
-                  "per request" % (seconds, SERVE["seed"] + rank, SERVE["sample_s"], len(sample),
-                                   sum(r[2] for r in sample)),
+                  "per request, best of two runs each" % (seconds, SERVE["seed"] + rank, SERVE["sample_s"],
+                                                           len(sample), sum(r[2] for r in sample)),
         "what": "latency from arrival to the XYZ image in host memory; served_over_plain = capacity / plain on "
                 "the same requests",
     }
