@@ -199,6 +199,8 @@ typedef struct {
     float emitter_center[3];   /* spherical emitter (radius 0 = none) */
     float emitter_radius;
     float emitter_scale;       /* emitted radiance = scale * illuminant(lambda) */
+    uint32_t wave_bounces;     /* bounces run as compacted wavefront stages before the in-place tail
+                                  (0 -> 2); the image is the same for any value */
 } sc_tracer_options;
 /* GpuTracer::new (lib.rs:179-187), CpuTracer::new (tracer.rs:20-37).
  * illuminant 0 D65, 1 A; has_horizon/horizon: Scene::horizon (scene.rs:25-28). */

@@ -364,14 +364,15 @@ class GpuPhotonFilm:
 class GpuTracer:
     """GpuTracer (spectral-gpu/src/lib.rs:165-389): wavefront hero-wavelength
     camera tracer.  Keyword extensions (no reference counterpart): max_depth,
-    rr_start, emitter=(center, radius, scale)."""
+    rr_start, emitter=(center, radius, scale), wave_bounces (compacted
+    wavefront bounces before the in-place tail; scheduling only)."""
 
     def __init__(self, ctx, scene, camera, width, height, illuminant=D65, seed=0, max_depth=8, rr_start=0,
-                 emitter=None):
+                 emitter=None, wave_bounces=0):
         self.width, self.height = int(width), int(height)
         prims, np_, planes, npl, mats, nm = scene.arrays()
         opts = _lib.sc_tracer_options()
-        opts.max_depth, opts.rr_start = int(max_depth), int(rr_start)
+        opts.max_depth, opts.rr_start, opts.wave_bounces = int(max_depth), int(rr_start), int(wave_bounces)
         if emitter is not None:
             c, r, s = emitter
             opts.emitter_center, opts.emitter_radius, opts.emitter_scale = _f3(c), float(r), float(s)

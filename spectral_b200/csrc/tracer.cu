@@ -26,7 +26,6 @@ namespace sc {
 namespace {
 
 constexpr int kShadeThreads = 256;
-constexpr uint32_t kWaveBounces = 2;  // bounces run as compacted wavefront stages; the rest by tr_tail
 constexpr float kLambdaMin = 380.0f, kLambdaRange = 350.0f;
 
 struct TracerSmem {
@@ -361,7 +360,7 @@ cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch&
     const size_t dyn = tracer_dyn_smem(L.n_planes);
     // wavefront with compaction for the first bounces, then the tail in place;
     // bounce 0 makes and intersects the primary rays in one kernel
-    const uint32_t wave_bounces = L.max_depth < kWaveBounces ? L.max_depth : kWaveBounces;
+    const uint32_t wave_bounces = L.max_depth < L.wave_bounces ? L.max_depth : L.wave_bounces;
     if (wave_bounces == 0)
         tr_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(d_params, first_pixel, n_pixels, n_paths, L.d_base,
                                                            L.qa, L.counts, L.result);

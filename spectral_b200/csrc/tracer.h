@@ -39,6 +39,7 @@ struct TracerLaunch {
     const uint32_t* d_base; // sample index of the first sample of this accumulate
     unsigned long long* segments;  // running count of traced segments
     uint32_t spp, max_depth, n_planes, grid;
+    uint32_t wave_bounces;  // compacted wavefront bounces before the tail
 };
 
 size_t tracer_dyn_smem(uint32_t n_planes);

@@ -148,6 +148,7 @@ int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, c
     if (opts) o = *opts;
     if (o.max_depth == 0) o.max_depth = 8;
     SC_REQUIRE(o.max_depth <= 64, SC_E_LIMIT, "max_depth %u > 64", o.max_depth);
+    SC_REQUIRE(o.wave_bounces <= 64, SC_E_INVALID, "wave_bounces %u > 64", o.wave_bounces);
     sc_tracer* t = new sc_tracer();
     t->ctx = ctx; t->w = width; t->h = height;
     DeviceGuard g(ctx->device);
@@ -195,6 +196,7 @@ int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, c
         L.counts = t->counts.p + c * (o.max_depth + 1); L.sum = t->sum.p; L.d_base = t->base.p;
         L.segments = t->segments.p;
         L.max_depth = o.max_depth; L.n_planes = n_planes; L.grid = (uint32_t)tracer_grid(ctx->sms);
+        L.wave_bounces = o.wave_bounces ? o.wave_bounces : 2u;
     }
     if ((e = cudaMemcpy(t->params.p, &hp, sizeof hp, cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e);

@@ -264,3 +264,17 @@ def test_many_waves_on_both_chains_bit_identical(ctx):
     assert cpu.sum() > 0 and gpu.tobytes() == cpu.tobytes()
     paths, segs = t.stats()
     assert paths == w * h * spp and segs >= paths
+
+
+@pytest.mark.parametrize("wave_bounces", [1, 3, 8])
+def test_wave_bounces_is_scheduling_only(ctx, wave_bounces):
+    """How many bounces run as compacted wavefront stages before the in-place
+    tail changes only the schedule: the image is bit-identical."""
+    from spectral_b200.scenes import tracer_workload
+    scene, cam, kw = tracer_workload(96, 64)
+    ref = sb.GpuTracer(ctx, scene, cam, 96, 64, sb.D65, 0x51, **kw)
+    ref.accumulate(8)
+    t = sb.GpuTracer(ctx, scene, cam, 96, 64, sb.D65, 0x51, wave_bounces=wave_bounces, **kw)
+    t.accumulate(8)
+    a, b = ref.read_xyz(), t.read_xyz()
+    assert a.sum() > 0 and a.tobytes() == b.tobytes()
