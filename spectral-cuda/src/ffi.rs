@@ -66,7 +66,8 @@ pub struct ScFilmOptions { pub bins: u32, pub lambda_min: f32, pub lambda_max: f
 #[repr(C)]
 #[derive(Clone, Copy, Default, Debug)]
 pub struct ScTracerOptions { pub max_depth: u32, pub rr_start: u32, pub emitter_center: [f32; 3],
-                             pub emitter_radius: f32, pub emitter_scale: f32, pub wave_bounces: u32 }
+                             pub emitter_radius: f32, pub emitter_scale: f32, pub wave_bounces: u32,
+                             pub chains: u32, pub wave_paths_log2: u32 }
 /// lighttrace::Screen rectangle.
 #[repr(C)]
 #[derive(Clone, Copy, Default, Debug)]

@@ -364,15 +364,17 @@ class GpuPhotonFilm:
 class GpuTracer:
     """GpuTracer (spectral-gpu/src/lib.rs:165-389): wavefront hero-wavelength
     camera tracer.  Keyword extensions (no reference counterpart): max_depth,
-    rr_start, emitter=(center, radius, scale), wave_bounces (compacted
-    wavefront bounces before the in-place tail; scheduling only)."""
+    rr_start, emitter=(center, radius, scale); scheduling only: wave_bounces
+    (compacted wavefront bounces before the in-place tail), chains (waves in
+    flight) and wave_paths_log2 (paths per wave)."""
 
     def __init__(self, ctx, scene, camera, width, height, illuminant=D65, seed=0, max_depth=8, rr_start=0,
-                 emitter=None, wave_bounces=0):
+                 emitter=None, wave_bounces=0, chains=0, wave_paths_log2=0):
         self.width, self.height = int(width), int(height)
         prims, np_, planes, npl, mats, nm = scene.arrays()
         opts = _lib.sc_tracer_options()
         opts.max_depth, opts.rr_start, opts.wave_bounces = int(max_depth), int(rr_start), int(wave_bounces)
+        opts.chains, opts.wave_paths_log2 = int(chains), int(wave_paths_log2)
         if emitter is not None:
             c, r, s = emitter
             opts.emitter_center, opts.emitter_radius, opts.emitter_scale = _f3(c), float(r), float(s)

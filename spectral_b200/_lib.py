@@ -67,7 +67,8 @@ class sc_film_options(C.Structure):
 
 class sc_tracer_options(C.Structure):
     _fields_ = [("max_depth", C.c_uint32), ("rr_start", C.c_uint32), ("emitter_center", F3),
-                ("emitter_radius", C.c_float), ("emitter_scale", C.c_float), ("wave_bounces", C.c_uint32)]
+                ("emitter_radius", C.c_float), ("emitter_scale", C.c_float), ("wave_bounces", C.c_uint32),
+                ("chains", C.c_uint32), ("wave_paths_log2", C.c_uint32)]
 
 
 class sc_trace_desc(C.Structure):

@@ -9,17 +9,20 @@
 using namespace sc;
 
 namespace {
-// Waves run on two chains (two streams, two queue sets), so one wave's short
-// late-bounce launches overlap the next wave's full-width ones; the queues of
-// both chains together (2 x 2^19 paths) stay resident in L2.
-constexpr uint32_t kChains = 2;
-constexpr uint32_t kWavePaths = 1u << 19;  // paths per wave and chain
+// Waves run on chains (one stream and one queue set each; two by default), so
+// one wave's short late-bounce launches overlap the next wave's full-width
+// ones; the queues of two chains of 2^19 paths mostly stay resident in L2.
+constexpr uint32_t kMaxChains = 4;
+constexpr uint32_t kDefaultChains = 2;
+constexpr uint32_t kDefaultWaveLog2 = 19;  // paths per wave and chain: 2^19
 }
 
 struct sc_tracer {
     sc_ctx* ctx = nullptr;
-    cudaStream_t stream = nullptr, stream2 = nullptr;  // chain 0 (the tracer's stream), chain 1
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t stream = nullptr;                    // chain 0: the tracer's stream
+    cudaStream_t extra[kMaxChains - 1] = {};          // chains 1..
+    cudaEvent_t fork = nullptr, join[kMaxChains - 1] = {};
+    uint32_t chains = kDefaultChains, wave_paths = 1u << kDefaultWaveLog2;
     std::mutex mu;
     uint32_t w = 0, h = 0, samples = 0;
     uint32_t row0 = 0, row1 = 0;  // rows traced by accumulate (all by default)
@@ -34,11 +37,21 @@ struct sc_tracer {
     DevBuf<unsigned long long> segments;
     DevBuf<uint32_t> qbuf_u;
     uint32_t wave_cap = 0;  // paths per wave the queues are sized for
-    TracerLaunch L[kChains]{};
+    TracerLaunch L[kMaxChains]{};
     cudaGraphExec_t graph = nullptr;
     uint32_t graph_spp = 0;
     uint64_t last_paths = 0, last_segments = 0;
 
+    void release_streams() {
+        if (stream) cudaStreamDestroy(stream);
+        for (uint32_t c = 0; c + 1 < kMaxChains; ++c) {
+            if (extra[c]) cudaStreamDestroy(extra[c]);
+            if (join[c]) cudaEventDestroy(join[c]);
+        }
+        if (fork) cudaEventDestroy(fork);
+        stream = nullptr;
+        fork = nullptr;
+    }
     void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
@@ -53,11 +66,11 @@ struct sc_tracer {
         drop_graph();
         const size_t n = paths;
         // per chain: 2 ray queues x 8 floats, 2 hit queues x 4 floats, result 3; 2 ray queues x 3 u32, 2 hit infos
-        SC_CUDA(qbuf.alloc(kChains * (n * 8 * 2 + n * 4 * 2 + 3 * n)));
-        SC_CUDA(qbuf_u.alloc(kChains * (n * 3 * 2 + n * 2)));
+        SC_CUDA(qbuf.alloc(chains * (n * 8 * 2 + n * 4 * 2 + 3 * n)));
+        SC_CUDA(qbuf_u.alloc(chains * (n * 3 * 2 + n * 2)));
         float* f = qbuf.p;
         uint32_t* u = qbuf_u.p;
-        for (uint32_t c = 0; c < kChains; ++c) {
+        for (uint32_t c = 0; c < chains; ++c) {
             TracerLaunch& Lc = L[c];
             RayQueue* qs[2] = {&Lc.qa, &Lc.qb};
             for (RayQueue* q : qs) {
@@ -82,26 +95,28 @@ struct sc_tracer {
     }
     int run(uint32_t spp) {
         const uint32_t px0 = row0 * w, px1 = row1 * w, npx = px1 - px0;
-        const uint32_t px_per_wave = std::max(1u, kWavePaths / spp);
+        const uint32_t px_per_wave = std::max(1u, wave_paths / spp);
         int rc = ensure_queues(std::max(1u, std::min(npx, px_per_wave)) * spp);
         if (rc != SC_OK) return rc;
-        for (uint32_t c = 0; c < kChains; ++c) L[c].spp = spp;
+        for (uint32_t c = 0; c < chains; ++c) L[c].spp = spp;
         SC_CUDA(cudaMemcpyAsync(base.p, &samples, 4, cudaMemcpyHostToDevice, stream));
         if (!graph || graph_spp != spp) {
             drop_graph();
             cudaGraph_t g = nullptr;
             SC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-            // fork chain 1 off the tracer's stream, alternate waves, join it back
+            // fork the other chains off the tracer's stream, deal waves round robin, join them back
             cudaError_t e = cudaEventRecord(fork, stream);
-            if (e == cudaSuccess) e = cudaStreamWaitEvent(stream2, fork, 0);
+            for (uint32_t c = 1; c < chains && e == cudaSuccess; ++c) e = cudaStreamWaitEvent(extra[c - 1], fork, 0);
             uint32_t wave = 0;
             for (uint32_t first = px0; first < px1 && e == cudaSuccess; first += px_per_wave, ++wave) {
-                const uint32_t c = wave % kChains;
+                const uint32_t c = wave % chains;
                 e = launch_tracer_wave(params.p, L[c], first, std::min(px_per_wave, px1 - first),
-                                       c ? stream2 : stream);
+                                       c ? extra[c - 1] : stream);
             }
-            if (e == cudaSuccess) e = cudaEventRecord(join, stream2);
-            if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, join, 0);
+            for (uint32_t c = 1; c < chains && e == cudaSuccess; ++c) {
+                e = cudaEventRecord(join[c - 1], extra[c - 1]);
+                if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, join[c - 1], 0);
+            }
             cudaError_t e2 = cudaStreamEndCapture(stream, &g);
             if (e == cudaSuccess) e = e2;
             if (e == cudaSuccess) e = cudaGraphInstantiate(&graph, g, 0);
@@ -149,30 +164,34 @@ int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, c
     if (o.max_depth == 0) o.max_depth = 8;
     SC_REQUIRE(o.max_depth <= 64, SC_E_LIMIT, "max_depth %u > 64", o.max_depth);
     SC_REQUIRE(o.wave_bounces <= 64, SC_E_INVALID, "wave_bounces %u > 64", o.wave_bounces);
+    SC_REQUIRE(o.chains <= kMaxChains, SC_E_INVALID, "chains %u > %u", o.chains, kMaxChains);
+    SC_REQUIRE(o.wave_paths_log2 == 0 || (o.wave_paths_log2 >= 12 && o.wave_paths_log2 <= 22), SC_E_INVALID,
+               "wave_paths_log2 %u outside 12..22", o.wave_paths_log2);
     sc_tracer* t = new sc_tracer();
     t->ctx = ctx; t->w = width; t->h = height;
+    t->chains = o.chains ? o.chains : kDefaultChains;
+    t->wave_paths = 1u << (o.wave_paths_log2 ? o.wave_paths_log2 : kDefaultWaveLog2);
     DeviceGuard g(ctx->device);
     auto fail = [&](cudaError_t e) {
         set_error("tracer setup failed: %s", cudaGetErrorString(e));
-        if (t->stream) cudaStreamDestroy(t->stream);
-        if (t->stream2) cudaStreamDestroy(t->stream2);
-        if (t->fork) cudaEventDestroy(t->fork);
-        if (t->join) cudaEventDestroy(t->join);
+        t->release_streams();
         delete t;
         return e == cudaErrorMemoryAllocation ? SC_E_NOMEM : SC_E_CUDA;
     };
     cudaError_t e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(e);
-    if ((e = cudaStreamCreateWithFlags(&t->stream2, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    for (uint32_t c = 1; c < t->chains; ++c) {
+        if ((e = cudaStreamCreateWithFlags(&t->extra[c - 1], cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+        if ((e = cudaEventCreateWithFlags(&t->join[c - 1], cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+    }
     if ((e = cudaEventCreateWithFlags(&t->fork, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
-    if ((e = cudaEventCreateWithFlags(&t->join, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
     if ((e = t->params.alloc(1)) != cudaSuccess) return fail(e);
     if ((e = t->tables.alloc(5 * kTableN)) != cudaSuccess) return fail(e);
     if ((e = t->prims.alloc(std::max(1u, n_prims))) != cudaSuccess) return fail(e);
     if ((e = t->planes.alloc(std::max(1u, n_planes))) != cudaSuccess) return fail(e);
     if ((e = t->mats.alloc(std::max(1u, n_mats))) != cudaSuccess) return fail(e);
     if ((e = t->sum.alloc(3ull * width * height)) != cudaSuccess) return fail(e);
-    if ((e = t->counts.alloc(kChains * (o.max_depth + 1))) != cudaSuccess) return fail(e);
+    if ((e = t->counts.alloc(t->chains * (o.max_depth + 1))) != cudaSuccess) return fail(e);
     if ((e = t->base.alloc(1)) != cudaSuccess) return fail(e);
     if ((e = t->segments.alloc(1)) != cudaSuccess) return fail(e);
     cudaMemcpy(t->tables.p, ctx->tables, 5 * kTableN * sizeof(float), cudaMemcpyHostToDevice);
@@ -191,7 +210,7 @@ int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, c
     hp.prims = t->prims.p; hp.planes = t->planes.p; hp.mats = t->mats.p;
     hp.n_prims = n_prims; hp.n_planes = n_planes; hp.n_mats = n_mats;
     hp.tables = t->tables.p;
-    for (uint32_t c = 0; c < kChains; ++c) {
+    for (uint32_t c = 0; c < t->chains; ++c) {
         TracerLaunch& L = t->L[c];
         L.counts = t->counts.p + c * (o.max_depth + 1); L.sum = t->sum.p; L.d_base = t->base.p;
         L.segments = t->segments.p;
@@ -215,10 +234,7 @@ int sc_tracer_destroy(sc_tracer* t) {
         t->params.reset(); t->tables.reset(); t->prims.reset(); t->planes.reset(); t->mats.reset();
         t->sum.reset(); t->result.reset(); t->qbuf.reset(); t->qbuf_u.reset(); t->counts.reset(); t->base.reset();
         t->segments.reset();
-        if (t->stream) cudaStreamDestroy(t->stream);
-        if (t->stream2) cudaStreamDestroy(t->stream2);
-        if (t->fork) cudaEventDestroy(t->fork);
-        if (t->join) cudaEventDestroy(t->join);
+        t->release_streams();
     }
     delete t;
     return SC_OK;

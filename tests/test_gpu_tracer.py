@@ -266,15 +266,18 @@ def test_many_waves_on_both_chains_bit_identical(ctx):
     assert paths == w * h * spp and segs >= paths
 
 
-@pytest.mark.parametrize("wave_bounces", [1, 3, 8])
-def test_wave_bounces_is_scheduling_only(ctx, wave_bounces):
+@pytest.mark.parametrize("sched", [dict(wave_bounces=1), dict(wave_bounces=3), dict(wave_bounces=8),
+                                   dict(chains=1), dict(chains=4, wave_paths_log2=12),
+                                   dict(chains=3, wave_paths_log2=13, wave_bounces=3)])
+def test_wave_schedule_is_scheduling_only(ctx, sched):
     """How many bounces run as compacted wavefront stages before the in-place
-    tail changes only the schedule: the image is bit-identical."""
+    tail, how many waves are in flight and how many paths a wave holds change
+    only the schedule: the image is bit-identical."""
     from spectral_b200.scenes import tracer_workload
     scene, cam, kw = tracer_workload(96, 64)
     ref = sb.GpuTracer(ctx, scene, cam, 96, 64, sb.D65, 0x51, **kw)
     ref.accumulate(8)
-    t = sb.GpuTracer(ctx, scene, cam, 96, 64, sb.D65, 0x51, wave_bounces=wave_bounces, **kw)
+    t = sb.GpuTracer(ctx, scene, cam, 96, 64, sb.D65, 0x51, **sched, **kw)
     t.accumulate(8)
     a, b = ref.read_xyz(), t.read_xyz()
     assert a.sum() > 0 and a.tobytes() == b.tobytes()
