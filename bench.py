@@ -575,7 +575,7 @@ def run_gpu(args, rank, world, local_rank):
 # spherical D65 emitter r=0.2 at (2,3,1), 1280x720, 64 spp per step, hero comb
 # of 4 wavelengths, depth 8, Russian roulette after bounce 3.
 TRACER = dict(width=1280, height=720, spp=64, seed=0x7ACE)
-TRACER_WAVE_PATHS = 1 << 19  # paths per wavefront wave (the library's queue size per chain)
+TRACER_WAVE_PATHS = 1 << 22  # paths per wavefront wave (the library's default queue size per chain)
 
 
 def run_cpu_tracer(seconds, threads=None):
@@ -698,9 +698,10 @@ def run_gpu_tracer(args, rank, world, local_rank):
     # emitter sphere test, 60 for the shading step (Fresnel / refraction or
     # cosine sampling, 4-lane throughput and radiance update)
     flops = segments * (14 * n_planes + 20 + 60)
-    # wavefront queue traffic per segment: ray 24 B read by intersect, hit 20 B
-    # written and read, path state 44 B read and written by shade
-    qbytes = segments * (24 + 2 * 20 + 2 * 44)
+    # wavefront queue traffic per segment: the hit (20 B) written by the kernel
+    # that intersects the ray and read by the shade, the path state (44 B)
+    # read and written by the shade
+    qbytes = segments * (2 * 20 + 2 * 44)
     waves = -(-(W * H) // max(1, TRACER_WAVE_PATHS // SPP))
     line = {
         "metric": "path samples/s (hero-wavelength camera tracer, 4 lanes, depth 8)",
@@ -714,15 +715,15 @@ def run_gpu_tracer(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": C.sizeof(cam.c),
                 "d2h_bytes_per_step": 3 * W * H * 4,
                 "path": "sc_tracer_set_camera + clear_accum + accumulate(64) + read_xyz (host f32 XYZ)"},
-        # per wave: primary rays made and intersected, its shade, the second bounce
-        # (intersect + shade), the tail, per-pixel sums
-        "gpu_launches": args.steps * waves * (1 + 2 * min(kw["max_depth"], 2) + (1 if kw["max_depth"] > 2 else 0)),
+        # per wave: primary rays made and intersected, two shades (the first also
+        # intersects the second bounce's rays), the tail, per-pixel sums
+        "gpu_launches": args.steps * waves * (1 + min(kw["max_depth"], 2) + (1 if kw["max_depth"] > 2 else 0) + 1),
         "kernels": {"accumulate_ms": statistics.mean(step_ms)},
         "roofline": {"bound": "hbm", "achieved": qbytes / step_s / 1e9, "peak": hbm, "unit": "GB/s",
                      "frac": qbytes / step_s / 1e9 / hbm, "traffic": ncu_traffic("tracer")[0],
                      "traffic_source": ncu_traffic("tracer")[1], "kernel": "tracer wave kernels (one accumulate)",
                      "peak_source": "%s hbm_gbs" % peak_note,
-                     "algorithmic": "wavefront queue bytes: 176 B per path segment, %d segments per step" % segments},
+                     "algorithmic": "wavefront queue bytes: 128 B per path segment, %d segments per step" % segments},
         "roofline_fp32": {"kernel": "tr_intersect + tr_shade", "counted_flops": flops,
                           "achieved_tflops": flops / step_s / 1e12, "peak_tflops": fp32_peak,
                           "frac": flops / step_s / 1e12 / fp32_peak,

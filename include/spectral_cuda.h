@@ -201,8 +201,8 @@ typedef struct {
     float emitter_scale;       /* emitted radiance = scale * illuminant(lambda) */
     uint32_t wave_bounces;     /* bounces run as compacted wavefront stages before the in-place tail
                                   (0 -> 2); the image is the same for any value */
-    uint32_t chains;           /* waves in flight at once, one stream each (0 -> 2, at most 4) */
-    uint32_t wave_paths_log2;  /* paths per wave 2^k (0 -> 19; 12..22); scheduling only, as above */
+    uint32_t chains;           /* waves in flight at once, one stream each (0 -> 3, at most 4) */
+    uint32_t wave_paths_log2;  /* paths per wave 2^k (0 -> 22; 12..24); scheduling only, as above */
 } sc_tracer_options;
 /* GpuTracer::new (lib.rs:179-187), CpuTracer::new (tracer.rs:20-37).
  * illuminant 0 D65, 1 A; has_horizon/horizon: Scene::horizon (scene.rs:25-28). */
