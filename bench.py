@@ -68,14 +68,14 @@ METRIC_BEAM = "photons/s (forward + photon-beam estimator, volumetric single sca
 # ncu capture of the default workload on a B200 (the profile summaries give the
 # commands); reported only when the workload runs at its default size.
 NCU_TRAFFIC = {
-    "prism": (2092544, "photon_kernel"),
-    "rainbow": (4839725056, "order_count + order_scan + order_scatter + photon_kernel"),
-    "beam": (3842560, "beam_kernel"),
-    "tracer": (8738738944, "all tracer wave kernels of one accumulate(64)"),
+    "prism": (2092544, "photon_kernel, one capture"),
+    "rainbow": (4839725056, "order_count + order_scan + order_scatter + photon_kernel, one capture"),
+    "beam": (3842560, "beam_kernel, one capture"),
+    "tracer": (13906632192, "all tracer wave kernels of one accumulate(64), one capture"),
     "batch": (3953000000, "batch_kernel + reduce_scan + reduce_list, scaled from a capture of the first 64 "
                           "scenes (4.4 GB of films): batch_kernel by photons, reduce_scan by film bytes, reduce_list by "
                           "lit-tile bytes"),
-    "atomics": (24887296, "synthetic_splat_kernel"),
+    "atomics": (24887296, "synthetic_splat_kernel, one capture"),
 }
 
 
