@@ -77,8 +77,9 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(const BatchJobDev* __r
                                                             [first](uint32_t k) { return first + k; },
                                                             cur_words ? mask : nullptr, split[warp]);
         } else {
-            for (uint32_t i = lane; i < item.count; i += 32u)
-                trace_photon<true, AGG, false, false, FF>(slot.p, S, cmf, item.begin + i, cur_words ? mask : nullptr);
+            const uint32_t first = item.begin;
+            trace_lane_range<true, AGG, FF>(slot.p, S, cmf, lane, item.count, 32u,
+                                            [first](uint32_t k) { return first + k; }, cur_words ? mask : nullptr);
         }
         __syncwarp();
     }

@@ -57,11 +57,16 @@ __global__ void __launch_bounds__(256, MINB) photon_kernel(const PhotonParams p,
                 p, S, cmf, cnt, [&](uint32_t k) { return p.photon_base + (p.order ? p.order[b0 + k] : b0 + k); },
                 smask, ws[warp]);
         }
-    } else {
+    } else if (EXACT) {
         const uint32_t stride = gridDim.x * blockDim.x;
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.photon_count; i += stride)
-            trace_photon<SPEC, AGG, false, false, FF, EXACT>(p, S, cmf, p.photon_base + (p.order ? p.order[i] : i),
-                                                              smask);
+            trace_photon<SPEC, AGG, false, false, FF, true>(p, S, cmf, p.photon_base + (p.order ? p.order[i] : i),
+                                                             smask);
+    } else {
+        trace_lane_range<SPEC, AGG, FF>(p, S, cmf, blockIdx.x * blockDim.x + threadIdx.x, p.photon_count,
+                                        gridDim.x * blockDim.x,
+                                        [&](uint32_t i) { return p.photon_base + (p.order ? p.order[i] : i); },
+                                        smask);
     }
     if (smask) {  // publish this CTA's dirty tiles
         __syncthreads();

@@ -373,6 +373,75 @@ __device__ __forceinline__ void trace_photon(const PhotonParams& p, const SceneV
     if (DEBUG) rec->num_states = pairs < 9u ? pairs : 9u;
 }
 
+// One photon per lane over positions [first, count) of a range, stepping `stride`
+// (photon id = id(k)), written as one loop of bounce steps: a lane whose photon
+// has ended starts its next photon inside the loop, so the warp reconverges at
+// every bounce step instead of waiting at the end of each photon for the
+// warp's longest one.  The photons, their draws and their samples are those of
+// trace_photon (fast haze samples), so the film is bit-identical to it.
+template <bool SPEC, int AGG, bool FFOK, class Id>
+__device__ __forceinline__ void trace_lane_range(const PhotonParams& p, const SceneView& S, const float* cmf,
+                                                 uint32_t first, uint32_t count, uint32_t stride, Id id,
+                                                 uint32_t* smask) {
+    const bool ff = FFOK && free_flight(p);
+    Rng r;
+    r.state = 0u;
+    f3 o = mk(0.f, 0.f, 0.f), d = p.bdir;
+    float lambda = 0.0f, power = 1.0f, cx = 0.f, cy = 0.f, cz = 0.f;
+    uint32_t bin = 0, bounce = 0, n_glass = 0xFFFFFFFFu;
+    float n_cached = 1.0f;
+    bool alive = false;
+    uint32_t next = first;
+    for (;;) {
+        if (!alive) {
+            if (next >= count || p.max_bounces == 0u) break;
+            r = Rng::make(id(next), p.seed);
+            next += stride;
+            const float r1 = r.f32();
+            const float r2 = r.f32();
+            o = add(add(p.corner, mul(p.bu, r1)), mul(p.bv, r2));
+            d = p.bdir;
+            lambda = p.lambda_min + p.lambda_range * r.f32();
+            photon_payload(p, cmf, lambda, cx, cy, cz, bin, SPEC);
+            power = 1.0f;
+            bounce = 0;
+            n_glass = 0xFFFFFFFFu;
+            alive = true;
+        }
+        Hit h;
+        uint32_t mi = 0;
+        const bool any = scene_hit(S, o, d, h, mi);
+        const float seg = any ? h.t : p.max_dist;
+        const HazeSeg hz = ff ? haze_setup<true>(p, o, d, seg, power) : haze_setup<false>(p, o, d, seg, power);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t draw24 = r.u32() >> 8;
+            uint32_t px, py;
+            float contrib;
+            const bool ok = ff ? haze_fast<true>(p, hz, draw24, px, py, contrib)
+                               : haze_fast<false>(p, hz, draw24, px, py, contrib);
+            deposit<SPEC, AGG>(p, smask, ok, px, py, contrib, cx, cy, cz, bin, 1.0f);
+        }
+        ++bounce;
+        if (!any || bounce >= p.max_bounces) {
+            alive = false;  // escaped, or its last segment: no scatter needed
+            continue;
+        }
+        const sc_material& m = S.mats[mi];
+        float nh = 1.0f;
+        if (m.kind == 1u) {
+            if (m.glass != n_glass) { n_cached = glass_n(m.glass, p.spectral ? lambda : 550.0f); n_glass = m.glass; }
+            nh = n_cached;
+        }
+        f3 nd;
+        float w;
+        scatter(m, d, h, nh, r, nd, w);
+        power *= w;
+        o = h.point;
+        d = nd;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Warp-split transport.  (a) Every lane traces its photon's path (intersect,
 // Fresnel / refract / TIR scatter) and appends one record per segment to the
