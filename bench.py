@@ -1376,15 +1376,18 @@ def main():
             metric = "photons/s @<=0.5% film err; batched vs plain per-scene launch (forward + volumetric)"
             cfg_line = {"workload": "batch: 256 prism scenes (see the GPU arm)", "scenes": BATCH["n_jobs"]}
         else:
-            cfg = WORKLOADS[args.workload]
+            wl = "rainbow" if args.workload == "split" else args.workload  # the split workload traces the rainbow
+            cfg = WORKLOADS[wl]
             for _ in range(args.warmup):
-                run_cpu(args.workload, 1.0)
+                run_cpu(wl, 1.0)
             for _ in range(args.steps):
-                rate, n_s, dt, th = run_cpu(args.workload, per_step)
+                rate, n_s, dt, th = run_cpu(wl, per_step)
                 rates.append((n_s, dt))
             sample = "per step %d photons from photon 0 (the whole workload repeated when shorter)" % rates[0][0]
-            serial = cpu_serial(args.workload, args.cpu_seconds)
-            metric = METRIC_BEAM if args.workload == "beam" else METRIC_POINT
+            serial = cpu_serial(wl, args.cpu_seconds)
+            metric = METRIC_BEAM if wl == "beam" else METRIC_POINT
+            if args.workload == "split":
+                metric += "; one scene split across GPUs"
             cfg_line = {"workload": args.workload, "photons_per_step": cfg["photons"],
                         "film": [cfg["width"], cfg["height"], cfg["bins"]]}
         tot_n, tot_t = sum(n for n, _ in rates), sum(t for _, t in rates)
@@ -1401,7 +1404,7 @@ def main():
                 "cpu_baseline": {"value": value, "unit": unit, "cores": th, "kind": "port",
                                  "sample": sample + "; CPU restatement of spectral-core %s, %s" % (what, cpu_model())},
                 "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        if args.workload in WORKLOADS:
+        if serial is not None:
             line["cpu_baseline"]["serial"] = serial
         print(json.dumps(line))
         return 0

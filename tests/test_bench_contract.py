@@ -30,7 +30,7 @@ def _run(*args):
                           timeout=600)
 
 
-@pytest.mark.parametrize("workload", ["prism", "tracer", "batch", "serve"])
+@pytest.mark.parametrize("workload", ["prism", "tracer", "batch", "serve", "split"])
 def test_reference_arm_prints_one_contract_line(workload):
     r = _run("--impl", "reference", "--workload", workload, "--steps", "1", "--warmup", "1", "--cpu-seconds", "0.5")
     assert r.returncode == 0, r.stderr[-2000:]
