@@ -44,8 +44,10 @@ class Server:
         check(lib.sc_server_step(self.h, C.byref(a)))
         return a.value
 
-    def poll(self, want_image=True):
-        """(id, xyz or None, (t_submit, t_admit, t_first_frame, t_done)) or None."""
+    def poll(self, want_image=True, copy=True):
+        """(id, xyz or None, (t_submit, t_admit, t_first_frame, t_done)) or None.
+        With copy=False the image is a view of a buffer that the next poll
+        overwrites (the library has already copied it into host memory)."""
         rid, w, h = C.c_uint64(), C.c_uint32(), C.c_uint32()
         times = (C.c_double * 4)()
         # room for the largest image of any request still outstanding (buffer kept between polls)
@@ -59,7 +61,8 @@ class Server:
             return None
         check(rc)
         n = self._dims.pop(rid.value, 0)
-        return rid.value, (buf[:n].copy() if cap else None), tuple(times)
+        img = (buf[:n].copy() if copy else buf[:n]) if cap else None
+        return rid.value, img, tuple(times)
 
     def peek(self, rid):
         """(frames done, current XYZ image) of an active request, or None when
@@ -129,12 +132,14 @@ def run_plain_stream(ctx, stream, time_scale=1.0):
     back to the host and clear; destroy.  Returns the metrics of run_stream."""
     t0 = time.perf_counter()
     lat, ttff, photons = [], [], 0
+    # one host image buffer, as large as the largest image (reused, as the server's is)
+    host_all = np.empty(max(3 * r[1].width * r[1].height for r in stream) if stream else 0, np.float32)
     for arrival, job, nf, orbit in stream:
         now = time.perf_counter() - t0
         if now < arrival * time_scale:
             time.sleep(arrival * time_scale - now)
         f = C.c_void_p()
-        host = np.empty(3 * job.width * job.height, np.float32)
+        host = host_all[:3 * job.width * job.height]
         check(lib.sc_photon_film_create(ctx.h, job.prims, job.n_prims, job.planes, job.n_planes, job.mats,
                                         job.n_mats, 0.0, C.byref(job.cam), C.byref(job.beam), job.width, job.height,
                                         job.n_photons, job.seed, job.max_dist, C.byref(job.weights), None,
@@ -186,7 +191,7 @@ def run_stream(server, stream, time_scale=1.0, idle_sleep=2e-4, want_image=False
         elif k < len(stream):
             time.sleep(min(idle_sleep, max(0.0, stream[k][0] * time_scale - now)))
         while True:
-            r = server.poll(want_image=want_image)
+            r = server.poll(want_image=want_image, copy=False)
             if r is None:
                 break
             rid, _, (ts, ta, tf, td) = r
