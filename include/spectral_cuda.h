@@ -443,7 +443,10 @@ int sc_server_submit(sc_server* s, const sc_request* r, uint64_t* id);
 int sc_server_step(sc_server* s, uint32_t* active);
 /* Pop a finished request: its last frame's XYZ image (3*w*h floats) and the
  * steady-clock times [submit, admit, first frame done, done] in seconds (the
- * last two as seen by the host).  SC_E_STATE when nothing is finished. */
+ * last two as seen by the host).  SC_E_STATE when nothing is finished.
+ * Finished images wait in a 256 MB pinned host ring until polled; while it is
+ * full, further finished images stay on the device (holding their share of
+ * the budget) and are copied as polls make room, so poll as results come. */
 int sc_server_poll(sc_server* s, uint64_t* id, float* xyz_out, size_t capacity, uint32_t* width,
                    uint32_t* height, double times[4]);
 /* The current image of an active request (3*w*h floats): for a progressive

@@ -111,6 +111,7 @@ class PinnedRing {
         return base_ + at;
     }
     void pop() { if (!live_.empty()) live_.pop_front(); }
+    size_t capacity() const { return cap_; }
     void release() {
         if (base_) cudaFreeHost(base_);
         base_ = nullptr;
@@ -134,7 +135,7 @@ struct Request {
     size_t film_cells = 0;
     const float* binw = nullptr;  // bin-averaged CMF of its (bins, band), shared through the context
     float* image = nullptr;       // pinned copy of the last frame's XYZ image
-    bool image_own = false;       // its own pinned allocation (the ring was full), not a ring range
+    bool image_own = false;       // its own pinned allocation (larger than the ring), not a ring range
 };
 
 // Film, dirty mask and image of one request in the arena.
@@ -182,6 +183,11 @@ struct sc_server {
     std::vector<Request*> active;
     std::deque<StepRecord> inflight;  // queued steps, oldest first
     std::deque<Request*> finished;
+    // Requests whose last frame is traced but whose image waits for room in
+    // the ring (results not yet polled); they keep their arena range, so a
+    // caller that does not poll holds admission back instead of pinning more
+    // host memory.
+    std::deque<Request*> unread;
     uint64_t next_id = 1, photons = 0;
     uint32_t grid = 0;
     HostStage stage[2];
@@ -250,9 +256,31 @@ struct sc_server {
 
     // Requests whose images are still being produced or copied.
     uint32_t retiring() const {
-        size_t n = 0;
+        size_t n = unread.size();
         for (const StepRecord& r : inflight) n += r.last.size();
         return (uint32_t)n;
+    }
+
+    // Queue the image copies of waiting requests, oldest first, while the ring
+    // has room; each joins `rec`, whose event follows the copies.  An image
+    // larger than the whole ring, or every waiting image when `own` (nothing
+    // else is left to trace), gets a pinned buffer of its own.
+    int issue_unread(StepRecord& rec, bool own) {
+        while (!unread.empty()) {
+            Request* q = unread.front();
+            const size_t nf = 3ull * q->r.job.width * q->r.job.height;
+            q->image = ring.get(nf);
+            if (!q->image) {
+                if (!own && nf <= ring.capacity()) break;  // room comes back as results are polled
+                SC_CUDA(cudaMallocHost(reinterpret_cast<void**>(&q->image), nf * sizeof(float)));
+                q->image_own = true;
+            }
+            SC_CUDA(cudaMemcpyAsync(q->image, xyz_ptr(q), nf * sizeof(float), cudaMemcpyDeviceToHost, stream));
+            arena.release(q->off, q->bytes);  // later users of the range queue behind this copy
+            rec.last.push_back(q);
+            unread.pop_front();
+        }
+        return SC_OK;
     }
 
     void free_image(Request* q) {
@@ -338,7 +366,16 @@ struct sc_server {
         if (rc == SC_OK) rc = admit(t0);
         if (rc != SC_OK) return rc;
         if (active.empty()) {
-            // nothing to trace: finish what is still queued (a drain loop ends here)
+            // nothing to trace: finish what is still queued (a drain loop ends
+            // here, also one that polls only at the end)
+            if (!unread.empty()) {
+                StepRecord rec;
+                rc = issue_unread(rec, true);
+                if (rc != SC_OK) return rc;
+                SC_CUDA(event(&rec.done));
+                SC_CUDA(cudaEventRecord(rec.done, stream));
+                inflight.push_back(std::move(rec));
+            }
             rc = collect(true);
             if (n_active) *n_active = 0;
             return rc;
@@ -423,21 +460,12 @@ struct sc_server {
         for (Request* q : active) {
             if (q->frame == 0) rec.first.push_back(q);
             ++q->frame;
-            if (q->frame >= q->r.frames) {
-                const size_t nf = 3ull * q->r.job.width * q->r.job.height;
-                q->image = ring.get(nf);
-                if (!q->image) {  // ring full (results not polled): a pinned buffer of its own
-                    SC_CUDA(cudaMallocHost(reinterpret_cast<void**>(&q->image), nf * sizeof(float)));
-                    q->image_own = true;
-                }
-                SC_CUDA(cudaMemcpyAsync(q->image, xyz_ptr(q), nf * sizeof(float), cudaMemcpyDeviceToHost, stream));
-                arena.release(q->off, q->bytes);  // later users of the range queue behind this copy
-                rec.last.push_back(q);
-            } else {
-                still.push_back(q);
-            }
+            if (q->frame >= q->r.frames) unread.push_back(q);
+            else still.push_back(q);
         }
         active.swap(still);
+        rc = issue_unread(rec, false);
+        if (rc != SC_OK) return rc;
         SC_CUDA(event(&rec.done));
         SC_CUDA(cudaEventRecord(rec.done, stream));
         inflight.push_back(std::move(rec));
@@ -505,6 +533,7 @@ int sc_server_destroy(sc_server* s) {
         for (StepRecord& r : s->inflight)
             for (Request* q : r.last) { if (q->image_own) cudaFreeHost(q->image); delete q; }
         for (Request* q : s->finished) { if (q->image_own) cudaFreeHost(q->image); delete q; }
+        for (Request* q : s->unread) delete q;
         s->release_all();
         s->mem.reset(); s->d_jobs.reset(); s->d_descs.reset(); s->d_items.reset(); s->counter.reset();
         if (s->stream) cudaStreamDestroy(s->stream);
@@ -580,13 +609,23 @@ int sc_server_poll(sc_server* s, uint64_t* id, float* xyz_out, size_t capacity, 
         std::memcpy(xyz_out, q->image, nf * sizeof(float));
     }
     s->free_image(q);
+    if (!s->unread.empty()) {  // ring room came back: queue the waiting images' copies
+        StepRecord rec;
+        rc = s->issue_unread(rec, false);
+        if (rc == SC_OK && !rec.last.empty()) {
+            cudaError_t e = s->event(&rec.done);
+            if (e == cudaSuccess) e = cudaEventRecord(rec.done, s->stream);
+            if (e == cudaSuccess) s->inflight.push_back(std::move(rec));
+            else { set_error("%s", cudaGetErrorString(e)); rc = SC_E_CUDA; }
+        }
+    }
     *id = q->id;
     if (width) *width = q->r.job.width;
     if (height) *height = q->r.job.height;
     if (times) { times[0] = q->t_submit; times[1] = q->t_admit; times[2] = q->t_first; times[3] = q->t_done; }
     s->finished.pop_front();
     delete q;
-    return SC_OK;
+    return rc;
     SC_GUARD_END
 }
 

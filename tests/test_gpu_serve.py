@@ -115,6 +115,21 @@ def test_queued_steps_overflowing_image_ring_and_cancel(ctx):
         got[r[0]] = r[1]
     assert sorted(got) == sorted(ids) and s.stats()["bytes_in_use"] == 0
     s.close()
+    # a slow poller (one result per step): finished images wait on the device
+    # for ring room instead of taking pinned buffers of their own
+    s = Server(ctx, budget_bytes=2 << 30, max_slots=8)
+    ids2 = [s.submit(j) for j in big]
+    got2 = {}
+    while s.stats()["queued"] or s.stats()["active"]:
+        s.step()
+        if (r := s.poll()) is not None:
+            got2[r[0]] = r[1]
+    while (r := s.poll()) is not None:
+        got2[r[0]] = r[1]
+    assert sorted(got2) == sorted(ids2) and s.stats()["bytes_in_use"] == 0
+    s.close()
+    for a, b in zip(ids, ids2):
+        assert got2[b].tobytes() == got[a].tobytes()
     for i in (0, 11, 23):
         a = Server(ctx, budget_bytes=1 << 30)
         rid = a.submit(big[i])
