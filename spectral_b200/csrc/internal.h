@@ -10,18 +10,22 @@
 namespace sc {
 
 // One forward photon pass over photons [photon_base, photon_base + photon_count).
-struct PhotonParams {
-    f3 corner, bu, bv, bdir;          // Beam (lighttrace.rs:116-121)
-    Proj proj;                        // Camera::project basis
+struct alignas(16) PhotonParams {
+    // what every haze sample reads, in 16-byte groups
+    float hz_hw, hz_hh, hz_w, hz_h;   // film width and height halves, film width and height
+    float hz_kexp, g, hz_m2g, hz_g2;  // -sigma_t * log2(e); HG g; -2 g; 1 + g^2
     uint32_t width, height, tiles_x, channels;
-    uint32_t photon_base, photon_count, seed, max_bounces;
-    float sigma_s, sigma_t, g, max_dist;
-    float lambda_min, lambda_range, bin_min, bin_inv_width;
-    float scale;
-    uint32_t spectral, estimator, bins;
-    const float* zbuf;                // device, nullable
     unsigned long long* film;         // tile-major int64 film
     uint32_t* flags;                  // per-tile dirty flags, nullable
+    const float* zbuf;                // device, nullable
+    uint32_t estimator, spectral;
+    f3 corner, bu, bv, bdir;          // Beam (lighttrace.rs:116-121)
+    Proj proj;                        // Camera::project basis
+    uint32_t photon_base, photon_count, seed, max_bounces;
+    float sigma_s, sigma_t, max_dist;
+    float lambda_min, lambda_range, bin_min, bin_inv_width;
+    float scale;
+    uint32_t bins;
     const sc_primitive* prims; const sc_plane* planes; const sc_material* mats;
     uint32_t n_prims, n_planes, n_mats;
     const float* cmf;                 // device 3x71 (xbar, ybar, zbar)
@@ -30,11 +34,9 @@ struct PhotonParams {
     uint32_t haze_exact;              // 1: haze samples in the CPU crate's operation order (per-photon kernel)
     // Launch constants of the fast haze samples, filled by set_haze_consts()
     // from the fields above just before a launch.
-    float hz_w, hz_h, hz_hw, hz_hh;   // film width and height, and their halves
     float hz_sx, hz_sy;               // W / |horizontal|, -H / |vertical|
     float hz_k, hz_kiso;              // sigma_s * 2^scale / 4 * HG numerator / (4 pi); isotropic estimator's
-    float hz_kexp, hz_inv_sigma_t;    // -sigma_t * log2(e), 1 / sigma_t
-    float hz_g2, hz_m2g;              // 1 + g^2, -2 g (HG denominator)
+    float hz_inv_sigma_t;             // 1 / sigma_t
 };
 
 // Fills the hz_* launch constants of `p` (host side, before every launch).
