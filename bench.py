@@ -71,7 +71,7 @@ NCU_TRAFFIC = {
     "prism": (2092544, "photon_kernel, one capture"),
     "rainbow": (4839725056, "order_count + order_scan + order_scatter + photon_kernel, one capture"),
     "beam": (3842560, "beam_kernel, one capture"),
-    "tracer": (13906632192, "all tracer wave kernels of one accumulate(64), one capture"),
+    "tracer": (7015925760, "all tracer wave kernels of one accumulate(64), one capture"),
     "batch": (3953000000, "batch_kernel + reduce_scan + reduce_list, scaled from a capture of the first 64 "
                           "scenes (4.4 GB of films): batch_kernel by photons, reduce_scan by film bytes, reduce_list by "
                           "lit-tile bytes"),
@@ -698,10 +698,11 @@ def run_gpu_tracer(args, rank, world, local_rank):
     # emitter sphere test, 60 for the shading step (Fresnel / refraction or
     # cosine sampling, 4-lane throughput and radiance update)
     flops = segments * (14 * n_planes + 20 + 60)
-    # wavefront queue traffic per segment: the hit (20 B) written by the kernel
-    # that intersects the ray and read by the shade, the path state (44 B)
-    # read and written by the shade
-    qbytes = segments * (2 * 20 + 2 * 44)
+    # wavefront queue traffic: per segment after the first (the first bounce
+    # makes its rays in place), the hit (20 B) written by the kernel that
+    # intersects the ray and read by the shade, the path state (44 B) written
+    # and read; per path, its XYZ (12 B) written and read by the per-pixel sums
+    qbytes = (segments - samples) * (2 * 20 + 2 * 44) + samples * 2 * 12
     waves = -(-(W * H) // max(1, TRACER_WAVE_PATHS // SPP))
     line = {
         "metric": "path samples/s (hero-wavelength camera tracer, 4 lanes, depth 8)",
@@ -715,15 +716,16 @@ def run_gpu_tracer(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": C.sizeof(cam.c),
                 "d2h_bytes_per_step": 3 * W * H * 4,
                 "path": "sc_tracer_set_camera + clear_accum + accumulate(64) + read_xyz (host f32 XYZ)"},
-        # per wave: primary rays made and intersected, two shades (the first also
-        # intersects the second bounce's rays), the tail, per-pixel sums
-        "gpu_launches": args.steps * waves * (1 + min(kw["max_depth"], 2) + (1 if kw["max_depth"] > 2 else 0) + 1),
+        # per wave: two shades (the first makes and intersects the primary rays
+        # and intersects the second bounce's rays), the tail, per-pixel sums
+        "gpu_launches": args.steps * waves * (min(kw["max_depth"], 2) + (1 if kw["max_depth"] > 2 else 0) + 1),
         "kernels": {"accumulate_ms": statistics.mean(step_ms)},
         "roofline": {"bound": "hbm", "achieved": qbytes / step_s / 1e9, "peak": hbm, "unit": "GB/s",
                      "frac": qbytes / step_s / 1e9 / hbm, "traffic": ncu_traffic("tracer")[0],
                      "traffic_source": ncu_traffic("tracer")[1], "kernel": "tracer wave kernels (one accumulate)",
                      "peak_source": "%s hbm_gbs" % peak_note,
-                     "algorithmic": "wavefront queue bytes: 128 B per path segment, %d segments per step" % segments},
+                     "algorithmic": "wavefront queue bytes: 128 B per path segment after the first bounce, 24 B of "
+                                    "XYZ per path (%d segments, %d paths per step)" % (segments, samples)},
         "roofline_fp32": {"kernel": "tr_intersect + tr_shade", "counted_flops": flops,
                           "achieved_tflops": flops / step_s / 1e12, "peak_tflops": fp32_peak,
                           "frac": flops / step_s / 1e12 / fp32_peak,

@@ -4,9 +4,9 @@
 // GPU mirror spectral-gpu/src/shaders/trace.wgsl:419-537) as a wavefront:
 //   generate  one path per (pixel, sample): stream key mix2(pixel, sample index),
 //             jittered primary ray, hero-comb wavelength draw (spectrum.rs:20-32);
-//   intersect nearest scene hit (+ the optional spherical emitter) per queued ray
-//             (for primary rays in the generating kernel, for later rays in the
-//             shade kernel that queued them);
+//   intersect nearest scene hit (+ the optional spherical emitter) per ray
+//             (primary rays where they are made, in the first shade kernel;
+//             later rays in the shade kernel that queued them);
 //   shade     background / emission at termination, Fresnel / refract / TIR or
 //             Lambertian scatter, dispersion collapse to the hero lane, optional
 //             Russian roulette; survivors are compacted into the next queue with
@@ -174,62 +174,31 @@ __device__ __forceinline__ bool shade_path(const TracerSmem& s, const SceneView&
     return survive;
 }
 
-// Bounce 0 without a ray queue round trip: each path's primary ray is made as
-// tr_generate makes it, intersected at once, and queued with its hit for the
-// first shade (persistent grid, scene in shared memory).
-__global__ void __launch_bounds__(256) tr_primary(const TracerParams* __restrict__ gp, uint32_t first_pixel,
-                                                  uint32_t n_pixels, uint32_t n_paths,
-                                                  const uint32_t* __restrict__ base, RayQueue q, uint32_t* counts,
-                                                  HitQueue hq, float* result) {
-    __shared__ TracerSmem s;
-    extern __shared__ __align__(16) unsigned char dyn[];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        counts[0] = n_paths;
-        for (uint32_t b = 1; b <= gp->max_depth; ++b) counts[b] = 0u;
-    }
-    if (blockIdx.x * blockDim.x >= n_paths) return;
-    const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
-    const uint32_t W = s.p.width, H = s.p.height, b0 = *base;
-    const f3 org = ld3(s.p.cam.origin);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_paths; i += gridDim.x * blockDim.x) {
-        const uint32_t smp = i / n_pixels, pixel = first_pixel + (i - smp * n_pixels);
-        const uint32_t px = pixel % W, py = pixel / W;
-        Rng r = Rng::make(mix2(pixel, b0 + smp), s.p.seed);
-        const float fs = ((float)px + r.f32()) / (float)W;
-        const float ft = 1.0f - ((float)py + r.f32()) / (float)H;
-        const float u = r.f32();
-        const f3 d = primary_dir(s.p.cam, fs, ft);
-        q.ox[i] = org.x; q.oy[i] = org.y; q.oz[i] = org.z;
-        q.dx[i] = d.x; q.dy[i] = d.y; q.dz[i] = d.z;
-        q.rng[i] = r.state; q.tp[i] = 1.0f; q.u[i] = u; q.id[i] = i; q.flags[i] = 4u;
-        result[3 * i] = 0.0f; result[3 * i + 1] = 0.0f; result[3 * i + 2] = 0.0f;
-        float t;
-        f3 nrm;
-        uint32_t info;
-        trace_hit(s, S, org, d, t, nrm, info);
-        hq.t[i] = t;
-        if ((info >> 24) == 1u) { hq.nx[i] = nrm.x; hq.ny[i] = nrm.y; hq.nz[i] = nrm.z; }
-        hq.info[i] = info;
-    }
-}
-
 // ISECT: the surviving rays, once compacted into shared memory, are also
 // intersected here (the next bounce's hits go to `hout`), so they do not make a
 // queue round trip through a separate intersect launch.
-template <bool ISECT>
+// GEN: the first bounce with no queue in: each path's primary ray is made as
+// tr_generate makes it (paths numbered sample-major over the wave's n_pixels
+// pixels from first_pixel), intersected in place and shaded; counts[1..] are
+// zero at entry.
+template <bool ISECT, bool GEN>
 __global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __restrict__ gp, uint32_t bounce,
                                                           RayQueue q, HitQueue hq, RayQueue out, HitQueue hout,
-                                                          uint32_t* counts, float* result) {
+                                                          uint32_t* counts, float* result, uint32_t first_pixel,
+                                                          uint32_t n_pixels, uint32_t n_paths,
+                                                          const uint32_t* __restrict__ base) {
     __shared__ TracerSmem s;
     __shared__ uint32_t warp_base[kShadeThreads / 32 + 1];
     __shared__ uint32_t block_base;
     __shared__ float st_f[8][kShadeThreads];      // staged survivors: ox oy oz dx dy dz tp u
     __shared__ uint32_t st_u[3][kShadeThreads];   // rng id flags
     extern __shared__ __align__(16) unsigned char dyn[];
-    const uint32_t n = counts[bounce];
+    if (GEN && blockIdx.x == 0 && threadIdx.x == 0) counts[0] = n_paths;
+    const uint32_t n = GEN ? n_paths : counts[bounce];
     if (blockIdx.x * blockDim.x >= n) return;  // nothing queued for this CTA (late bounces)
     const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t b0 = GEN ? *base : 0u;
     for (uint32_t tile = blockIdx.x * blockDim.x; tile < n; tile += gridDim.x * blockDim.x) {
         const uint32_t i = tile + threadIdx.x;
         bool survive = false;
@@ -237,7 +206,24 @@ __global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __
         P.o = P.d = mk(0.0f, 0.0f, 0.0f);
         P.tp = P.u = 0.0f;
         P.rs = P.id = P.flags = 0u;
-        if (i < n) {
+        if (i < n && GEN) {
+            const uint32_t smp = i / n_pixels, pixel = first_pixel + (i - smp * n_pixels);
+            const uint32_t px = pixel % s.p.width, py = pixel / s.p.width;
+            Rng r = Rng::make(mix2(pixel, b0 + smp), s.p.seed);
+            const float fs = ((float)px + r.f32()) / (float)s.p.width;
+            const float ft = 1.0f - ((float)py + r.f32()) / (float)s.p.height;
+            P.u = r.f32();
+            P.o = ld3(s.p.cam.origin);
+            P.d = primary_dir(s.p.cam, fs, ft);
+            P.rs = r.state; P.tp = 1.0f; P.id = i; P.flags = 4u;
+            result[3 * i] = 0.0f; result[3 * i + 1] = 0.0f; result[3 * i + 2] = 0.0f;
+            float t;
+            f3 nrm;
+            uint32_t info;
+            trace_hit(s, S, P.o, P.d, t, nrm, info);
+            if ((info >> 24) != 1u) nrm = mk(0.0f, 0.0f, 0.0f);
+            survive = shade_path(s, S, 0u, P, t, nrm, info, result);
+        } else if (i < n) {
             P.o = mk(q.ox[i], q.oy[i], q.oz[i]);
             P.d = mk(q.dx[i], q.dy[i], q.dz[i]);
             P.tp = q.tp[i]; P.u = q.u[i]; P.rs = q.rng[i]; P.id = q.id[i]; P.flags = q.flags[i];
@@ -348,9 +334,14 @@ size_t tracer_dyn_smem(uint32_t n_planes) { return (size_t)(n_planes ? n_planes 
 
 int tracer_grid(int sms) {
     int a = 0, b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, tr_primary, 256, tracer_dyn_smem(SC_MAX_PLANES));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tr_shade<true>, kShadeThreads, tracer_dyn_smem(SC_MAX_PLANES));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, tr_tail, 256, tracer_dyn_smem(SC_MAX_PLANES));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tr_shade<true, false>, kShadeThreads,
+                                                  tracer_dyn_smem(SC_MAX_PLANES));
+    int c = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, tr_shade<true, true>, kShadeThreads,
+                                                  tracer_dyn_smem(SC_MAX_PLANES));
     int k = a < b ? a : b;
+    k = k < c ? k : c;
     return sms * (k > 0 ? k : 1);
 }
 
@@ -359,7 +350,7 @@ cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch&
     const uint32_t n_paths = n_pixels * L.spp;
     const size_t dyn = tracer_dyn_smem(L.n_planes);
     // wavefront with compaction for the first bounces, then the tail in place;
-    // bounce 0 makes and intersects the primary rays in one kernel
+    // the first bounce makes, intersects and shades the primary rays in one kernel
     const uint32_t wave_bounces = L.max_depth < L.wave_bounces ? L.max_depth : L.wave_bounces;
     if (wave_bounces == 0)
         tr_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(d_params, first_pixel, n_pixels, n_paths, L.d_base,
@@ -372,13 +363,25 @@ cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch&
         const HitQueue& hin = (b & 1u) ? L.hits2 : L.hits;
         const HitQueue& hout = (b & 1u) ? L.hits : L.hits2;
         const uint32_t g = L.grid;
-        if (b == 0)
-            tr_primary<<<g, 256, dyn, st>>>(d_params, first_pixel, n_pixels, n_paths, L.d_base, in, L.counts, L.hits,
-                                            L.result);
-        if (b + 1u < wave_bounces)
-            tr_shade<true><<<g, kShadeThreads, dyn, st>>>(d_params, b, in, hin, out, hout, L.counts, L.result);
-        else
-            tr_shade<false><<<g, kShadeThreads, dyn, st>>>(d_params, b, in, hin, out, hout, L.counts, L.result);
+        const bool isect = b + 1u < wave_bounces;
+        if (b == 0) {
+            // the first bounce makes its primary rays itself: no queue in; later
+            // bounces count their rays from zero
+            cudaError_t e = cudaMemsetAsync(L.counts + 1, 0, L.max_depth * sizeof(uint32_t), st);
+            if (e != cudaSuccess) return e;
+            if (isect)
+                tr_shade<true, true><<<g, kShadeThreads, dyn, st>>>(d_params, 0u, in, hin, out, hout, L.counts,
+                                                                    L.result, first_pixel, n_pixels, n_paths, L.d_base);
+            else
+                tr_shade<false, true><<<g, kShadeThreads, dyn, st>>>(d_params, 0u, in, hin, out, hout, L.counts,
+                                                                     L.result, first_pixel, n_pixels, n_paths, L.d_base);
+        } else if (isect) {
+            tr_shade<true, false><<<g, kShadeThreads, dyn, st>>>(d_params, b, in, hin, out, hout, L.counts, L.result,
+                                                                 0u, 1u, 0u, L.d_base);
+        } else {
+            tr_shade<false, false><<<g, kShadeThreads, dyn, st>>>(d_params, b, in, hin, out, hout, L.counts, L.result,
+                                                                  0u, 1u, 0u, L.d_base);
+        }
     }
     if (L.max_depth > wave_bounces)
         tr_tail<<<L.grid, 256, dyn, st>>>(d_params, wave_bounces, (wave_bounces & 1u) ? L.qb : L.qa, L.counts,
