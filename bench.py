@@ -79,6 +79,37 @@ NCU_TRAFFIC = {
 }
 
 
+# Warp instructions the dominant kernel issues per unit of work (photon or path
+# sample), from one ncu capture of smsp__inst_executed.sum and
+# smsp__thread_inst_executed.sum (a single-pass metric pair), with the lanes
+# active per instruction: the instruction-issue roofline of kernels whose films
+# stay in L2.
+NCU_INST = {
+    "batch": (12863533177 / 2 / 48957886, 21.78, "batch_kernel<0, 4, 0, 0>: two launches on the first 64 scenes "
+                                                  "(48,957,886 photons each), per photon"),
+    "prism": (331895528 / 2 / (1 << 20), 25.65, "photon_kernel: two launches of 2^20 photons, per photon"),
+    "rainbow": (5712815602 / (1 << 26), 24.04, "photon_kernel: one launch of 2^26 photons, per photon"),
+    "tracer": (4585800818 / 58982400, 27.91, "tr_shade, tr_tail, tr_accumulate: the 60 launches of one "
+                                             "accumulate(64), per path sample"),
+}
+
+
+def issue_roofline(workload, units, seconds, sms, sm_mhz, default_size=True):
+    """Warp instructions issued per second (from the captured count per unit)
+    against the issue peak: one warp instruction per clock on each of an SM's
+    four schedulers."""
+    if not default_size or workload not in NCU_INST:
+        return None
+    per_unit, lanes, what = NCU_INST[workload]
+    achieved = per_unit * units / seconds / 1e9
+    peak = sms * 4 * sm_mhz * 1e6 / 1e9
+    return {"achieved": achieved, "peak": peak, "unit": "G warp instructions/s", "frac": achieved / peak,
+            "inst_per_unit": per_unit, "lanes_per_inst": lanes,
+            "source": "ncu smsp__inst_executed.sum of %s" % what,
+            "peak_source": "%d SMs x 4 schedulers x 1 instruction per clock x %.0f MHz (sampled median)"
+                           % (sms, sm_mhz)}
+
+
 def ncu_traffic(workload, default_size=True):
     if not default_size or workload not in NCU_TRAFFIC:
         return None, None
@@ -551,6 +582,7 @@ def run_gpu(args, rank, world, local_rank):
         "roofline_fp32": {"kernel": kname, "counted_flops": flops, "achieved_tflops": flops / trace_s / 1e12,
                           "peak_tflops": fp32_peak, "frac": flops / trace_s / 1e12 / fp32_peak,
                           "peak_source": "%d SMs x 128 FP32 lanes x 2 x %.0f MHz (sampled median)" % (sms, sm_mhz)},
+        "roofline_issue": issue_roofline(args.workload, N, trace_s, sms, sm_mhz, not args.photons),
         "roofline_reduce": {"kernel": "reduce_kernel (drain)", "bound": "hbm",
                             "achieved": (2 * lit_bytes + 12 * W * H) / reduce_s / 1e9, "peak": hbm, "unit": "GB/s",
                             "frac": (2 * lit_bytes + 12 * W * H) / reduce_s / 1e9 / hbm,
@@ -730,6 +762,7 @@ def run_gpu_tracer(args, rank, world, local_rank):
                           "achieved_tflops": flops / step_s / 1e12, "peak_tflops": fp32_peak,
                           "frac": flops / step_s / 1e12 / fp32_peak,
                           "peak_source": "%d SMs x 128 FP32 lanes x 2 x %.0f MHz (sampled median)" % (sms, sm_mhz)},
+        "roofline_issue": issue_roofline("tracer", samples, step_s, sms, sm_mhz),
         "work": {"paths": samples, "segments": segments},
         "clocks": cl,
     }
@@ -1319,6 +1352,9 @@ def run_gpu_batch(args, rank, world, local_rank):
     line["roofline_fp32"] = {"counted_flops": flops, "achieved_tflops": flops / step_s / 1e12,
                              "peak_tflops": fp32_peak, "frac": flops / step_s / 1e12 / fp32_peak,
                              "peak_source": "%d SMs x 128 FP32 lanes x 2 x %.0f MHz (sampled median)" % (sms, sm_mhz)}
+    line["roofline_issue"] = issue_roofline("batch", stats["photons"], step_s, sms, sm_mhz, not args.scenes)
+    if line["roofline_issue"]:
+        line["roofline_issue"]["kernel"] = "batch_kernel, over the whole pass (drain included)"
     if world == 1 and not args.no_cpu_baseline:
         rate, n_s, dt, th, sc = run_cpu_batch(args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": "photons/s", "cores": th, "kind": "port",
