@@ -26,6 +26,11 @@ namespace sc {
 namespace {
 
 constexpr int kShadeThreads = 256;
+// Shade and tail CTAs resident per SM: 5 (48 registers, small spills) hides
+// more of their queue-read and shared-memory latency than 4 (64 registers):
+// accumulate(64) at 1280x720 5.83 -> 5.37 ms; 6 or 8 tail CTAs spill more
+// and are slower again.
+constexpr int kStageCtasPerSm = 5;
 constexpr float kLambdaMin = 380.0f, kLambdaRange = 350.0f;
 
 struct TracerSmem {
@@ -182,7 +187,7 @@ __device__ __forceinline__ bool shade_path(const TracerSmem& s, const SceneView&
 // pixels from first_pixel), intersected in place and shaded; counts[1..] are
 // zero at entry.
 template <bool ISECT, bool GEN>
-__global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __restrict__ gp, uint32_t bounce,
+__global__ void __launch_bounds__(kShadeThreads, kStageCtasPerSm) tr_shade(const TracerParams* __restrict__ gp, uint32_t bounce,
                                                           RayQueue q, HitQueue hq, RayQueue out, HitQueue hout,
                                                           uint32_t* counts, float* result, uint32_t first_pixel,
                                                           uint32_t n_pixels, uint32_t n_paths,
@@ -280,7 +285,7 @@ __global__ void __launch_bounds__(kShadeThreads) tr_shade(const TracerParams* __
 // alive, and a launch pair per bounce costs more than the work.  One thread per
 // remaining path runs the rest of its bounces in place (the same hit and shade
 // code, so the image is unchanged); its segments are added to counts[first + 1].
-__global__ void __launch_bounds__(256) tr_tail(const TracerParams* __restrict__ gp, uint32_t first, RayQueue q,
+__global__ void __launch_bounds__(256, kStageCtasPerSm) tr_tail(const TracerParams* __restrict__ gp, uint32_t first, RayQueue q,
                                                uint32_t* counts, float* result) {
     __shared__ TracerSmem s;
     extern __shared__ __align__(16) unsigned char dyn[];
