@@ -15,6 +15,10 @@ namespace {
 // (queues in L2) 7.47 ms, 3 x 2^20 6.39 ms, 3 x 2^22 6.11 ms, 2 x 2^24
 // 6.14 ms: large waves give the in-place tail enough paths to fill the GPU, and
 // the stages are bound by latency and issue, not by the queues' DRAM traffic.
+// With the first shade making its own rays and 5 stage CTAs per SM: 2 x 2^22
+// 5.52 ms, 3 x 2^21 5.47, 3 x 2^22 5.39, 4 x 2^23 5.35 (within run-to-run
+// spread of 3 x 2^22); two compacted bounces before the tail stay best (one
+// 6.45, three 5.75, four 5.67 ms).
 constexpr uint32_t kMaxChains = 4;
 constexpr uint32_t kDefaultChains = 3;
 constexpr uint32_t kDefaultWaveLog2 = 22;  // paths per wave and chain: 2^22
