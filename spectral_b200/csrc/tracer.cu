@@ -82,33 +82,6 @@ __device__ __forceinline__ void comb_xyz(const TracerSmem& s, float u, float tp,
     out[0] = x; out[1] = y; out[2] = z;
 }
 
-// Paths of a wave are numbered sample-major (path i = sample s of wave pixel j
-// with i = s * n_pixels + j): neighbouring threads trace neighbouring pixels,
-// and the per-pixel sums read the results coalesced.
-__global__ void __launch_bounds__(256) tr_generate(const TracerParams* __restrict__ gp, uint32_t first_pixel,
-                                                   uint32_t n_pixels, uint32_t n_paths,
-                                                   const uint32_t* __restrict__ base, RayQueue q, uint32_t* counts,
-                                                   float* result) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
-        counts[0] = n_paths;
-        for (uint32_t b = 1; b <= gp->max_depth; ++b) counts[b] = 0u;
-    }
-    if (i >= n_paths) return;
-    const uint32_t W = gp->width, H = gp->height;
-    const uint32_t s = i / n_pixels, pixel = first_pixel + (i - s * n_pixels);
-    const uint32_t px = pixel % W, py = pixel / W;
-    Rng r = Rng::make(mix2(pixel, *base + s), gp->seed);
-    const float fs = ((float)px + r.f32()) / (float)W;
-    const float ft = 1.0f - ((float)py + r.f32()) / (float)H;
-    const float u = r.f32();
-    const f3 d = primary_dir(gp->cam, fs, ft);
-    q.ox[i] = gp->cam.origin[0]; q.oy[i] = gp->cam.origin[1]; q.oz[i] = gp->cam.origin[2];
-    q.dx[i] = d.x; q.dy[i] = d.y; q.dz[i] = d.z;
-    q.rng[i] = r.state; q.tp[i] = 1.0f; q.u[i] = u; q.id[i] = i; q.flags[i] = 4u;
-    result[3 * i] = 0.0f; result[3 * i + 1] = 0.0f; result[3 * i + 2] = 0.0f;
-}
-
 // Nearest hit of one ray: scene records and the optional emitter sphere.
 // info = material | front_face << 16 | kind << 24 (0 miss, 1 surface, 2 emitter).
 __device__ __forceinline__ void trace_hit(const TracerSmem& s, const SceneView& S, f3 o, f3 d, float& t, f3& n,
@@ -182,10 +155,12 @@ __device__ __forceinline__ bool shade_path(const TracerSmem& s, const SceneView&
 // ISECT: the surviving rays, once compacted into shared memory, are also
 // intersected here (the next bounce's hits go to `hout`), so they do not make a
 // queue round trip through a separate intersect launch.
-// GEN: the first bounce with no queue in: each path's primary ray is made as
-// tr_generate makes it (paths numbered sample-major over the wave's n_pixels
-// pixels from first_pixel), intersected in place and shaded; counts[1..] are
-// zero at entry.
+// GEN: the first bounce with no queue in: each path's primary ray is made here
+// (stream key mix2(pixel, sample index), jittered through the pixel, hero-comb
+// draw), intersected in place and shaded.  Paths of a wave are numbered
+// sample-major (path i = sample s of wave pixel j with i = s * n_pixels + j):
+// neighbouring threads trace neighbouring pixels, and the per-pixel sums read
+// the results coalesced.  counts[1..] are zero at entry.
 template <bool ISECT, bool GEN>
 __global__ void __launch_bounds__(kShadeThreads, kStageCtasPerSm) tr_shade(const TracerParams* __restrict__ gp, uint32_t bounce,
                                                           RayQueue q, HitQueue hq, RayQueue out, HitQueue hout,
@@ -357,9 +332,6 @@ cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch&
     // wavefront with compaction for the first bounces, then the tail in place;
     // the first bounce makes, intersects and shades the primary rays in one kernel
     const uint32_t wave_bounces = L.max_depth < L.wave_bounces ? L.max_depth : L.wave_bounces;
-    if (wave_bounces == 0)
-        tr_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(d_params, first_pixel, n_pixels, n_paths, L.d_base,
-                                                           L.qa, L.counts, L.result);
     // bounce b shades the hits of bounce b and, while more wave bounces follow,
     // intersects its compacted survivors too (hit queues alternate)
     for (uint32_t b = 0; b < wave_bounces; ++b) {
