@@ -18,6 +18,8 @@
 //             surfaces, bit-identical to the CPU tracer.
 // Queue counts stay on the device: the launch sequence of an accumulate call is
 // fixed, needs no host synchronisation and is replayed from a CUDA graph.
+#include <algorithm>
+
 #include "internal.h"
 #include "tracer.h"
 
@@ -308,7 +310,22 @@ __global__ void __launch_bounds__(256) tr_accumulate(uint32_t first_pixel, uint3
     sum[3u * (size_t)first_pixel + j] += a;
 }
 
+// AccumBuffer::mean (spectral-core/src/lib.rs:16-20): each sum divided by the
+// sample count (an IEEE division, as the host would do it).
+__global__ void __launch_bounds__(256) tr_mean(const float* __restrict__ sum, float* __restrict__ out, size_t n,
+                                               float count) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = sum[i] / count;
+}
+
 }  // namespace
+
+cudaError_t launch_tracer_mean(const float* sum, float* out, size_t n, float count, int sms, cudaStream_t st) {
+    const size_t blocks = std::min<size_t>((n + 255) / 256, (size_t)sms * 8);
+    if (blocks == 0) return cudaSuccess;
+    tr_mean<<<(unsigned)blocks, 256, 0, st>>>(sum, out, n, count);
+    return cudaGetLastError();
+}
 
 size_t tracer_dyn_smem(uint32_t n_planes) { return (size_t)(n_planes ? n_planes : 1u) * sizeof(sc_plane); }
 

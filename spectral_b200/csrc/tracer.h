@@ -42,6 +42,8 @@ struct TracerLaunch {
     uint32_t wave_bounces;  // compacted wavefront bounces before the tail
 };
 
+// out[i] = sum[i] / count for the n floats of the running sums.
+cudaError_t launch_tracer_mean(const float* sum, float* out, size_t n, float count, int sms, cudaStream_t st);
 size_t tracer_dyn_smem(uint32_t n_planes);
 int tracer_grid(int sms);
 cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch& L, uint32_t first_pixel,

@@ -40,6 +40,7 @@ struct sc_tracer {
     DevBuf<sc_plane> planes;
     DevBuf<sc_material> mats;
     DevBuf<float> sum, result, qbuf;
+    DevBuf<float> mean;  // per-pixel means staged for read_xyz (allocated by its first call)
     DevBuf<uint32_t> counts, base;
     DevBuf<unsigned long long> segments;
     DevBuf<uint32_t> qbuf_u;
@@ -240,7 +241,7 @@ int sc_tracer_destroy(sc_tracer* t) {
         t->drop_graph();
         t->params.reset(); t->tables.reset(); t->prims.reset(); t->planes.reset(); t->mats.reset();
         t->sum.reset(); t->result.reset(); t->qbuf.reset(); t->qbuf_u.reset(); t->counts.reset(); t->base.reset();
-        t->segments.reset();
+        t->segments.reset(); t->mean.reset();
         t->release_streams();
     }
     delete t;
@@ -266,11 +267,12 @@ int sc_tracer_read_xyz(sc_tracer* t, float* out) {
     SC_GUARD_BEGIN
     TR_LOCK(t);
     SC_REQUIRE(out, SC_E_INVALID, "null output");
-    SC_CUDA(cudaMemcpyAsync(out, t->sum.p, t->sum.bytes(), cudaMemcpyDeviceToHost, t->stream));
+    // AccumBuffer::mean (spectral-core/src/lib.rs:16-20): sum / max(samples, 1), on the device
+    const size_t n = 3ull * t->w * t->h;
+    if (t->mean.n < n) SC_CUDA(t->mean.alloc(n));
+    SC_CUDA(launch_tracer_mean(t->sum.p, t->mean.p, n, (float)std::max(t->samples, 1u), t->ctx->sms, t->stream));
+    SC_CUDA(cudaMemcpyAsync(out, t->mean.p, n * sizeof(float), cudaMemcpyDeviceToHost, t->stream));
     SC_CUDA(cudaStreamSynchronize(t->stream));
-    // AccumBuffer::mean (spectral-core/src/lib.rs:16-20): sum / max(samples, 1)
-    const float n = (float)std::max(t->samples, 1u);
-    for (size_t i = 0; i < 3ull * t->w * t->h; ++i) out[i] = out[i] / n;
     return SC_OK;
     SC_GUARD_END
 }
