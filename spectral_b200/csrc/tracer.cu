@@ -40,6 +40,7 @@ struct TracerSmem {
     float tables[5 * kTableN];
     sc_primitive prims[SC_MAX_PRIMS];
     sc_material mats[SC_MAX_PRIMS];
+    float4 bounds[SC_MAX_PRIMS];
 };
 
 // Stage params, scene records and sensor tables in shared memory.  Planes live
@@ -51,6 +52,7 @@ __device__ __forceinline__ SceneView load_tracer(const TracerParams* gp, TracerS
     __syncthreads();
     for (uint32_t i = tid; i < s.p.n_prims; i += blockDim.x) s.prims[i] = s.p.prims[i];
     for (uint32_t i = tid; i < s.p.n_mats; i += blockDim.x) s.mats[i] = s.p.mats[i];
+    for (uint32_t i = tid; i < s.p.n_prims; i += blockDim.x) s.bounds[i] = s.p.bounds[i];
     for (uint32_t i = tid; i < s.p.n_planes; i += blockDim.x) planes[i] = s.p.planes[i];
     __syncthreads();
     SceneView S;
@@ -84,13 +86,46 @@ __device__ __forceinline__ void comb_xyz(const TracerSmem& s, float u, float tp,
     out[0] = x; out[1] = y; out[2] = z;
 }
 
+// Whether a ray certainly misses a bounding sphere (centre, radius^2 in b):
+// the origin is outside it and the line's closest approach at t >= 0 is
+// outside it.  The sphere is inflated on the host (1 % + 1e-3) far beyond the
+// rounding of these products; origins farther than 100 radii are not culled
+// (the products would cancel), so a culled solid is one that solid_hit would
+// not hit either.
+__device__ __forceinline__ bool misses_bound(float4 b, f3 o, f3 d) {
+    if (!(b.w < __int_as_float(0x7f800000))) return false;
+    const f3 oc = mk(b.x - o.x, b.y - o.y, b.z - o.z);
+    const float l2 = dot(oc, oc);
+    if (!(l2 > b.w) || l2 > 1e4f * b.w) return false;
+    const float bb = dot(oc, d);
+    if (bb <= 0.0f) return true;  // moving away from the centre, from outside
+    return (l2 - b.w) * dot(d, d) > bb * bb;
+}
+
+// Scene::intersect (scene_hit) skipping convex solids whose bounding sphere
+// the ray misses: the same nearest hit, fewer plane tests.
+__device__ __forceinline__ bool scene_hit_bounded(const TracerSmem& s, const SceneView& S, f3 o, f3 d, Hit& best,
+                                                  uint32_t& mat) {
+    bool any = false;
+    float closest = __int_as_float(0x7f800000);
+    for (uint32_t i = 0; i < S.n_prims; ++i) {
+        const sc_primitive& pr = S.prims[i];
+        if (pr.kind == 1u && misses_bound(s.bounds[i], o, d)) continue;
+        Hit h;
+        bool ok = pr.kind == 0u ? sphere_hit(pr, o, d, 1e-3f, closest, h)
+                : (pr.kind == 1u ? solid_hit(S, pr, o, d, 1e-3f, closest, h) : false);
+        if (ok) { closest = h.t; best = h; mat = pr.material; any = true; }
+    }
+    return any;
+}
+
 // Nearest hit of one ray: scene records and the optional emitter sphere.
 // info = material | front_face << 16 | kind << 24 (0 miss, 1 surface, 2 emitter).
 __device__ __forceinline__ void trace_hit(const TracerSmem& s, const SceneView& S, f3 o, f3 d, float& t, f3& n,
                                           uint32_t& info) {
     Hit h;
     uint32_t mi = 0;
-    const bool any = scene_hit(S, o, d, h, mi);
+    const bool any = scene_hit_bounded(s, S, o, d, h, mi);
     uint32_t kind = any ? 1u : 0u;
     t = any ? h.t : __int_as_float(0x7f800000);
     if (s.p.em_radius > 0.0f) {

@@ -18,6 +18,9 @@ struct TracerParams {
     const sc_primitive* prims; const sc_plane* planes; const sc_material* mats;
     uint32_t n_prims, n_planes, n_mats;
     const float* tables;  // device 5 x 71 sensor table
+    // per primitive: a sphere (centre, radius^2) holding a bounded convex
+    // solid, radius^2 = +inf where there is none (spheres, unbounded solids)
+    const float4* bounds;
 };
 
 // Structure-of-arrays ray / path queue.
