@@ -61,9 +61,18 @@ __device__ __forceinline__ SceneView load_tracer(const TracerParams* gp, TracerS
 }
 
 __device__ __forceinline__ float lane_lambda(float u, int k) {
-    // SpectralSample::from_hero_u: (u*RANGE + k*RANGE/4).rem_euclid(RANGE)
-    float off = fmodf(u * kLambdaRange + (float)k * (kLambdaRange / 4.0f), kLambdaRange);
-    if (off < 0.0f) off += kLambdaRange;
+    // SpectralSample::from_hero_u: (u*RANGE + k*RANGE/4).rem_euclid(RANGE).
+    // For 0 <= x < 2 RANGE (every u in [0, 1)) the remainder is x or x - RANGE,
+    // and x - RANGE is exact there (RANGE <= x < 2 RANGE), so it equals fmodf's
+    // exact remainder without its general loop.
+    const float x = u * kLambdaRange + (float)k * (kLambdaRange / 4.0f);
+    float off;
+    if (x >= 0.0f && x < 2.0f * kLambdaRange) {
+        off = x >= kLambdaRange ? x - kLambdaRange : x;
+    } else {
+        off = fmodf(x, kLambdaRange);
+        if (off < 0.0f) off += kLambdaRange;
+    }
     return kLambdaMin + off;
 }
 
