@@ -81,13 +81,18 @@ __device__ __forceinline__ void comb_xyz(const TracerSmem& s, float u, float tp,
                                          float out[3]) {
     const float pdf = 1.0f / kLambdaRange;
     const float* ill = s.tables + (s.p.illuminant == 1u ? 4 : 3) * kTableN;
+    // dividing by 1 or 4 lanes is scaling by a power of two: the same rounded
+    // quotient as the division
+    const bool pow2 = valid == 1u || valid == 4u;
+    const float inv_valid = valid == 4u ? 0.25f : 1.0f;
     float x = 0.0f, y = 0.0f, z = 0.0f;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float lam = lane_lambda(u, k);
         const float tk = (k == 0 || valid > 1u) ? tp : 0.0f;
         const float rad = 0.0f + tk * e * tab_sample(ill, lam);
-        const float wk = rad / pdf / (float)valid;
+        const float q = rad / pdf;
+        const float wk = pow2 ? q * inv_valid : q / (float)valid;
         x += tab_sample(s.tables, lam) * wk;
         y += tab_sample(s.tables + kTableN, lam) * wk;
         z += tab_sample(s.tables + 2 * kTableN, lam) * wk;
