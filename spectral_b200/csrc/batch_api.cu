@@ -71,6 +71,18 @@ struct sc_batch {
     DevBuf<DirtyTile> dirty_list;  // reduce scratch: room for every tile, and its counter
     DevBuf<uint32_t> counter, dirty_count;
     std::vector<BatchJobDev> h_jobs;
+    // Pinned copy of the job table for its upload, so the host returns at once
+    // (a copy from pageable memory would first wait for the pass before it);
+    // `staged` follows the last upload, which must have read it before the
+    // host rewrites it.
+    BatchJobDev* h_stage = nullptr;
+    cudaEvent_t staged = nullptr;
+    void free_stage() {
+        if (h_stage) cudaFreeHost(h_stage);
+        if (staged) cudaEventDestroy(staged);
+        h_stage = nullptr;
+        staged = nullptr;
+    }
     uint32_t n_items = 0, total_tiles = 0, total_words = 0, max_channels = 0;
     uint64_t total_photons = 0;
     sc_batch_tuning tuning{};
@@ -129,9 +141,17 @@ struct sc_batch {
             d.flags = flags.p + flag_off[j];
             d.mask_words = geom[j].words;
         }
+        if (!h_stage) {
+            SC_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_stage), h_jobs.size() * sizeof(BatchJobDev)));
+            SC_CUDA(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+        } else {
+            SC_CUDA(cudaEventSynchronize(staged));  // the last upload has read the pinned copy
+        }
+        std::memcpy(h_stage, h_jobs.data(), h_jobs.size() * sizeof(BatchJobDev));
         SC_CUDA(cudaStreamWaitEvent(stream, ran, 0));  // the previous pass still reads the table
-        SC_CUDA(cudaMemcpyAsync(d_jobs.p, h_jobs.data(), h_jobs.size() * sizeof(BatchJobDev), cudaMemcpyHostToDevice,
+        SC_CUDA(cudaMemcpyAsync(d_jobs.p, h_stage, h_jobs.size() * sizeof(BatchJobDev), cudaMemcpyHostToDevice,
                                 stream));
+        SC_CUDA(cudaEventRecord(staged, stream));
         return SC_OK;
     }
 
@@ -278,6 +298,7 @@ int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs, cons
         if (b->ran) cudaEventDestroy(b->ran);
         if (b->copied) cudaEventDestroy(b->copied);
         if (b->uploaded) cudaEventDestroy(b->uploaded);
+        b->free_stage();
         delete b;
         return e == cudaErrorMemoryAllocation ? SC_E_NOMEM : SC_E_CUDA;
     };
@@ -329,6 +350,7 @@ int sc_batch_create(sc_ctx* ctx, const sc_scene_job* jobs, uint32_t n_jobs, cons
         if (b->ran) cudaEventDestroy(b->ran);
         if (b->copied) cudaEventDestroy(b->copied);
         if (b->uploaded) cudaEventDestroy(b->uploaded);
+        b->free_stage();
         delete b;
         set_error("%s", msg.c_str());
         return rc;
@@ -354,6 +376,7 @@ int sc_batch_destroy(sc_batch* b) {
         if (b->ran) cudaEventDestroy(b->ran);
         if (b->copied) cudaEventDestroy(b->copied);
         if (b->uploaded) cudaEventDestroy(b->uploaded);
+        b->free_stage();
     }
     delete b;
     return SC_OK;
