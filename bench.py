@@ -89,7 +89,7 @@ NCU_INST = {
                                                   "(48,957,886 photons each), per photon"),
     "prism": (331895528 / 2 / (1 << 20), 25.65, "photon_kernel: two launches of 2^20 photons, per photon"),
     "rainbow": (5712815602 / (1 << 26), 24.04, "photon_kernel: one launch of 2^26 photons, per photon"),
-    "tracer": (4189107130 / 58982400, 26.64, "tr_shade, tr_tail, tr_accumulate: the 60 launches of one "
+    "tracer": (3830617932 / 58982400, 26.62, "tr_shade, tr_tail, tr_accumulate: the 60 launches of one "
                                              "accumulate(64), per path sample"),
 }
 
