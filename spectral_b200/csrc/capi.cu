@@ -73,6 +73,12 @@ static size_t mask_smem(uint32_t w, uint32_t h) {
     return words <= kMaxSmemMaskWords ? words * sizeof(uint32_t) : 0;
 }
 
+// The launch shape of single-film traces: 256-thread CTAs, 4 per SM, the
+// warp-split transport, the wavelength-ordered dispatch for spectral films
+// larger than L2.  The environment variables SPECTRAL_CUDA_AGGREGATE,
+// SPECTRAL_CUDA_MINB (4 or 5), SPECTRAL_CUDA_SPLIT (0: one photon per lane) and
+// SPECTRAL_CUDA_ORDER (0 never, 1 large spectral films, 2 every spectral film)
+// override it for measurements; every setting gives the same film bits.
 static int default_shape(sc_ctx* ctx, bool spectral, int aggregate, size_t smem, LaunchShape& s,
                          uint32_t estimator = 0) {
     s.block = 256;
