@@ -281,3 +281,32 @@ def test_wave_schedule_is_scheduling_only(ctx, sched):
     t.accumulate(8)
     a, b = ref.read_xyz(), t.read_xyz()
     assert a.sum() > 0 and a.tobytes() == b.tobytes()
+
+
+def _shifted(planes, offset):
+    """The same convex solid moved by `offset` (n . (x - c) + d <= 0)."""
+    return [(n, d - (n[0] * offset[0] + n[1] * offset[1] + n[2] * offset[2])) for n, d in planes]
+
+
+@pytest.mark.parametrize("eye", [(0.0, 0.3, 0.0), (0.0, 0.2, -6.0)])
+def test_bounding_spheres_keep_every_hit(ctx, eye):
+    """The tracer skips the plane tests of a convex solid when a ray misses a
+    sphere around it; the nearest hit must not change.  A dielectric scene of
+    21 small boxes (one behind the camera, some that rays graze), a wedge, an
+    unbounded three-plane prism (no caps: never skipped) and a ground
+    half-space renders bit-identically to the oracle, with the eye outside
+    every solid's sphere and with the eye inside a box."""
+    s = sb.Scene(background=1.0, horizon=3.0)
+    s.add_solid([((0.0, 1.0, 0.0), 1.5)], sb.Dielectric(sb.BK7))  # ground half-space y <= -1.5
+    for i in range(-3, 4):
+        for j in range(3):
+            c = (i * 1.2, -0.6 + j * 0.8, -5.0 - j)
+            s.add_solid(axis_box((c[0] - 0.3, c[1] - 0.3, c[2] - 0.3), (c[0] + 0.3, c[1] + 0.3, c[2] + 0.3)),
+                        sb.Dielectric(sb.SF11 if (i + j) % 2 else sb.BK7))
+    s.add_solid(axis_box((-0.4, -0.4, 2.6), (0.4, 0.4, 3.4)), sb.Dielectric(sb.BK7))  # behind the camera
+    s.add_solid(_shifted(triangular_prism(0.4, 0.0)[:3], (2.5, 1.2, 0.0)), sb.Dielectric(sb.SF11))  # no caps
+    from helpers import wedge
+    s.add_solid(_shifted(wedge(40.0, 0.3, 0.5), (-2.2, 1.1, -3.0)), sb.Dielectric(sb.BK7))
+    cam = sb.Camera.look_at(eye, (0.0, 0.0, -10.0), (0.0, 1.0, 0.0), 70.0, 4.0 / 3.0)
+    gpu, cpu, _ = run_both(ctx, s, cam, 96, 72, 4, 0xB0B)
+    assert cpu.sum() > 0 and gpu.tobytes() == cpu.tobytes()
