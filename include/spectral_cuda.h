@@ -287,7 +287,8 @@ int sc_scene_zbuffer(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, c
 /* ---- device-pointer entry points (zero-copy; caller owns device memory) -- */
 /* One plain launch of the forward photon + haze kernel over photons
  * [photon_base, photon_base+count) into a device film the caller allocated
- * with sc_film_bytes().  All pointers are device pointers; stream may be 0. */
+ * with sc_film_bytes().  All pointers are device pointers; stream may be 0.
+ * Films hold at most 2^28 pixels, as film objects do (SC_E_LIMIT). */
 typedef struct {
     const sc_primitive* prims; uint32_t n_prims;
     const sc_plane* planes; uint32_t n_planes;

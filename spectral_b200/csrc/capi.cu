@@ -762,6 +762,8 @@ int sc_trace_photons_device(sc_ctx* ctx, const sc_trace_desc* d, uint32_t base, 
     SC_REQUIRE(d->n_prims <= SC_MAX_PRIMS && d->n_planes <= SC_MAX_PLANES && d->n_mats <= SC_MAX_PRIMS, SC_E_LIMIT,
                "scene exceeds limits");
     SC_REQUIRE(d->width > 0 && d->height > 0, SC_E_INVALID, "empty film");
+    SC_REQUIRE((uint64_t)d->width * d->height <= (1ull << 28), SC_E_LIMIT, "film %ux%u too large", d->width,
+               d->height);
     sc_film_options o;
     resolve_options(&d->opts, o);
     SC_REQUIRE(o.bins <= SC_MAX_BINS && o.lambda_max > o.lambda_min && o.estimator <= 3u && o.haze_exact <= 1u,
@@ -793,6 +795,8 @@ int sc_trace_stats_device(sc_ctx* ctx, const sc_trace_desc* d, uint32_t base, ui
     SC_REQUIRE(ctx && d && out_dev, SC_E_INVALID, "null argument");
     SC_REQUIRE(d->n_prims <= SC_MAX_PRIMS && d->n_planes <= SC_MAX_PLANES && d->n_mats <= SC_MAX_PRIMS, SC_E_LIMIT,
                "scene exceeds limits");
+    SC_REQUIRE((uint64_t)d->width * d->height <= (1ull << 28), SC_E_LIMIT, "film %ux%u too large", d->width,
+               d->height);
     sc_film_options o;
     resolve_options(&d->opts, o);
     SC_REQUIRE(o.estimator != 2u || (d->width < 65536u && d->height < 65536u), SC_E_LIMIT,

@@ -268,9 +268,13 @@ __device__ __forceinline__ unsigned long long to_fixed(float x, float scale) {
 __host__ __device__ __forceinline__ uint32_t film_tile(uint32_t px, uint32_t py, uint32_t tiles_x) {
     return (py >> kTileShift) * tiles_x + (px >> kTileShift);
 }
+// The pixel's index in tile-major order fits 32 bits (every entry point limits
+// a film to 2^28 pixels, and beam films to 65535 x 65535: at most 2^26 tiles of
+// 64 pixels), so it is formed in 32-bit integer arithmetic and widened once, by
+// the multiply with the channel count.
 __host__ __device__ __forceinline__ size_t film_cell(uint32_t px, uint32_t py, uint32_t tiles_x, uint32_t channels) {
-    uint32_t local = ((py & 7u) << 3) | (px & 7u);
-    return ((size_t)film_tile(px, py, tiles_x) * kTilePixels + local) * channels;
+    const uint32_t local = ((py & 7u) << 3) | (px & 7u);
+    return (size_t)((film_tile(px, py, tiles_x) << 6) | local) * channels;
 }
 
 }  // namespace sc
