@@ -308,33 +308,81 @@ __global__ void __launch_bounds__(kShadeThreads, kStageCtasPerSm) tr_shade(const
 }
 
 // Late bounces: by the third bounce only a few per cent of a wave's paths are
-// alive, and a launch pair per bounce costs more than the work.  One thread per
-// remaining path runs the rest of its bounces in place (the same hit and shade
-// code, so the image is unchanged); its segments are added to counts[first + 1].
-__global__ void __launch_bounds__(256, kStageCtasPerSm) tr_tail(const TracerParams* __restrict__ gp, uint32_t first, RayQueue q,
-                                               uint32_t* counts, float* result) {
+// alive, and a launch pair per bounce costs more than the work.  The tail runs
+// them in one launch: each CTA holds up to 256 paths in shared memory with the
+// live ones at the front, runs one bounce of all of them (the same hit and
+// shade code, so the image is unchanged), compacts the survivors with warp
+// ballots, and refills the free slots from the queue with one claim per CTA
+// (counter counts[max_depth + 1], zero at entry), so its warps stay full while
+// the paths end after different numbers of bounces.  Segments after each
+// path's first tail bounce are added to counts[first + 1].
+__global__ void __launch_bounds__(256, kStageCtasPerSm) tr_tail(const TracerParams* __restrict__ gp, uint32_t first,
+                                                                RayQueue q, uint32_t* counts, float* result) {
     __shared__ TracerSmem s;
+    __shared__ float sf[8][256];    // ox oy oz dx dy dz tp u
+    __shared__ uint32_t su[3][256]; // rng id flags
+    __shared__ uint32_t warp_base[8 + 1];
+    __shared__ uint32_t claim_base;
     extern __shared__ __align__(16) unsigned char dyn[];
     const uint32_t n = counts[first];
     if (blockIdx.x * blockDim.x >= n) return;
     const SceneView S = load_tracer(gp, s, reinterpret_cast<sc_plane*>(dyn));
-    uint32_t segs = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t* claim = counts + s.p.max_depth + 1;
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    uint32_t live = 0, segs = 0;
+    for (;;) {
+        if (t == 0) claim_base = atomicAdd(claim, 256u - live);
+        __syncthreads();
+        const uint32_t base = claim_base;
+        const uint32_t got = base >= n ? 0u : min(256u - live, n - base);
+        if (t >= live && t < live + got) {  // coalesced: consecutive slots take consecutive paths
+            const uint32_t i = base + (t - live);
+            sf[0][t] = q.ox[i]; sf[1][t] = q.oy[i]; sf[2][t] = q.oz[i];
+            sf[3][t] = q.dx[i]; sf[4][t] = q.dy[i]; sf[5][t] = q.dz[i];
+            sf[6][t] = q.tp[i]; sf[7][t] = q.u[i];
+            su[0][t] = q.rng[i]; su[1][t] = q.id[i]; su[2][t] = q.flags[i];
+        }
+        live += got;
+        __syncthreads();
+        if (live == 0) break;
+        bool survive = false;
         PathState P;
-        P.o = mk(q.ox[i], q.oy[i], q.oz[i]);
-        P.d = mk(q.dx[i], q.dy[i], q.dz[i]);
-        P.tp = q.tp[i]; P.u = q.u[i]; P.rs = q.rng[i]; P.id = q.id[i]; P.flags = q.flags[i];
-        for (uint32_t b = first; b < s.p.max_depth; ++b) {
-            float t;
+        P.o = P.d = mk(0.0f, 0.0f, 0.0f);
+        P.tp = P.u = 0.0f;
+        P.rs = P.id = P.flags = 0u;
+        if (t < live) {
+            P.o = mk(sf[0][t], sf[1][t], sf[2][t]);
+            P.d = mk(sf[3][t], sf[4][t], sf[5][t]);
+            P.tp = sf[6][t]; P.u = sf[7][t]; P.rs = su[0][t]; P.id = su[1][t]; P.flags = su[2][t];
+            const uint32_t b = (P.flags >> 8) & 0xFFu;  // the bounce this path is at
+            float th;
             f3 nrm;
             uint32_t info;
-            trace_hit(s, S, P.o, P.d, t, nrm, info);
-            if (b > first) ++segs;  // counts[first] already holds this bounce's rays
-            if (!shade_path(s, S, b, P, t, nrm, info, result)) break;
+            trace_hit(s, S, P.o, P.d, th, nrm, info);
+            if (b > first) ++segs;  // counts[first] already holds the first tail bounce's rays
+            survive = shade_path(s, S, b, P, th, nrm, info, result);
         }
+        const unsigned ball = __ballot_sync(0xffffffffu, survive);
+        if (lane == 0) warp_base[warp] = __popc(ball);
+        __syncthreads();  // every slot has been read
+        if (t == 0) {
+            uint32_t acc = 0;
+            for (int w = 0; w < 8; ++w) { const uint32_t c = warp_base[w]; warp_base[w] = acc; acc += c; }
+            warp_base[8] = acc;
+        }
+        __syncthreads();
+        if (survive) {
+            const uint32_t j = warp_base[warp] + __popc(ball & ((1u << lane) - 1u));
+            sf[0][j] = P.o.x; sf[1][j] = P.o.y; sf[2][j] = P.o.z;
+            sf[3][j] = P.d.x; sf[4][j] = P.d.y; sf[5][j] = P.d.z;
+            sf[6][j] = P.tp; sf[7][j] = P.u;
+            su[0][j] = P.rs; su[1][j] = P.id; su[2][j] = P.flags;
+        }
+        live = warp_base[8];
+        __syncthreads();  // the survivors are in place (and warp_base is read) before the next claim
     }
     for (int o = 16; o > 0; o >>= 1) segs += __shfl_xor_sync(0xffffffffu, segs, o);
-    if ((threadIdx.x & 31u) == 0 && segs) atomicAdd(counts + first + 1, segs);
+    if (lane == 0 && segs) atomicAdd(counts + first + 1, segs);
 }
 
 // Per-pixel sample sum in sample order (tracer.rs:121-135), added to the running
@@ -410,7 +458,7 @@ cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch&
         if (b == 0) {
             // the first bounce makes its primary rays itself: no queue in; later
             // bounces count their rays from zero
-            cudaError_t e = cudaMemsetAsync(L.counts + 1, 0, L.max_depth * sizeof(uint32_t), st);
+            cudaError_t e = cudaMemsetAsync(L.counts + 1, 0, (L.max_depth + 1) * sizeof(uint32_t), st);
             if (e != cudaSuccess) return e;
             if (isect)
                 tr_shade<true, true><<<g, kShadeThreads, dyn, st>>>(d_params, 0u, in, hin, out, hout, L.counts,

@@ -36,7 +36,7 @@ struct HitQueue {
 struct TracerLaunch {
     RayQueue qa, qb;
     HitQueue hits, hits2;   // hits of the bounce being shaded / of the next one
-    uint32_t* counts;       // max_depth + 1 queue lengths
+    uint32_t* counts;       // max_depth + 1 queue lengths, then the tail's claim counter
     float* result;          // 3 per path of the wave
     float* sum;             // 3 * w * h running sum
     const uint32_t* d_base; // sample index of the first sample of this accumulate

@@ -274,7 +274,8 @@ int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, c
     if ((e = t->mats.alloc(std::max(1u, n_mats))) != cudaSuccess) return fail(e);
     if ((e = t->bounds.alloc(std::max(1u, n_prims))) != cudaSuccess) return fail(e);
     if ((e = t->sum.alloc(3ull * width * height)) != cudaSuccess) return fail(e);
-    if ((e = t->counts.alloc(t->chains * (o.max_depth + 1))) != cudaSuccess) return fail(e);
+    // per chain: max_depth + 1 queue counts and the tail's claim counter
+    if ((e = t->counts.alloc(t->chains * (o.max_depth + 2))) != cudaSuccess) return fail(e);
     if ((e = t->base.alloc(1)) != cudaSuccess) return fail(e);
     if ((e = t->segments.alloc(1)) != cudaSuccess) return fail(e);
     cudaMemcpy(t->tables.p, ctx->tables, 5 * kTableN * sizeof(float), cudaMemcpyHostToDevice);
@@ -306,7 +307,7 @@ int sc_tracer_create(sc_ctx* ctx, const sc_primitive* prims, uint32_t n_prims, c
     hp.bounds = t->bounds.p;
     for (uint32_t c = 0; c < t->chains; ++c) {
         TracerLaunch& L = t->L[c];
-        L.counts = t->counts.p + c * (o.max_depth + 1); L.sum = t->sum.p; L.d_base = t->base.p;
+        L.counts = t->counts.p + c * (o.max_depth + 2); L.sum = t->sum.p; L.d_base = t->base.p;
         L.segments = t->segments.p;
         L.max_depth = o.max_depth; L.n_planes = n_planes; L.grid = (uint32_t)tracer_grid(ctx->sms);
         L.wave_bounces = o.wave_bounces ? o.wave_bounces : 2u;
