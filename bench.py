@@ -85,11 +85,11 @@ NCU_TRAFFIC = {
 # active per instruction: the instruction-issue roofline of kernels whose films
 # stay in L2.
 NCU_INST = {
-    "batch": (12863533177 / 2 / 48957886, 21.78, "batch_kernel<0, 4, 0, 0>: two launches on the first 64 scenes "
+    "batch": (12734972130 / 2 / 48957886, 21.77, "batch_kernel<0, 4, 0, 0>: two launches on the first 64 scenes "
                                                   "(48,957,886 photons each), per photon"),
-    "prism": (331895528 / 2 / (1 << 20), 25.65, "photon_kernel: two launches of 2^20 photons, per photon"),
-    "rainbow": (5712815602 / (1 << 26), 24.04, "photon_kernel: one launch of 2^26 photons, per photon"),
-    "tracer": (3830617932 / 58982400, 26.62, "tr_shade, tr_tail, tr_accumulate: the 60 launches of one "
+    "prism": (324289908 / 2 / (1 << 20), 25.60, "photon_kernel: two launches of 2^20 photons, per photon"),
+    "rainbow": (5568513387 / (1 << 26), 23.90, "photon_kernel: one launch of 2^26 photons, per photon"),
+    "tracer": (3718315830 / 58982400, 27.64, "tr_shade, tr_tail, tr_accumulate: the 60 launches of one "
                                              "accumulate(64), per path sample"),
 }
 
