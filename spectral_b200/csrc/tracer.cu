@@ -13,6 +13,8 @@
 //             warp ballots, one atomic per block and shared-memory staging so the
 //             SoA writes are contiguous, and the compacted rays are intersected
 //             at once;
+//   tail      the few paths alive after the compacted bounces finish in one
+//             launch, kept compacted per CTA bounce by bounce;
 //   accumulate each pixel's samples summed in sample order (the CPU's order), so
 //             the image is deterministic and, for scenes without Lambertian
 //             surfaces, bit-identical to the CPU tracer.
