@@ -135,6 +135,12 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="window of the 200 req/s Poisson stream replayed in real time for the served numbers "
                          "(batch and serve workloads; 0: none)")
+    ap.add_argument("--tracer-chains", type=int, default=0,
+                    help="tracer schedule: waves in flight (0: the library's default, 3)")
+    ap.add_argument("--tracer-wave-log2", type=int, default=0,
+                    help="tracer schedule: paths per wave 2^k (0: the library's default, 22)")
+    ap.add_argument("--tracer-wave-bounces", type=int, default=0,
+                    help="tracer schedule: compacted bounces before the tail (0: the library's default, 2)")
     return ap.parse_args()
 
 
@@ -652,7 +658,9 @@ def run_gpu_tracer(args, rank, world, local_rank):
     W, H, SPP = TRACER["width"], TRACER["height"], TRACER["spp"]
     scene, cam, kw = tracer_workload(W, H)
     seed = TRACER["seed"] + rank  # each rank: its own independent 64-spp frame
-    tr = sb.GpuTracer(ctx, scene, cam, W, H, sb.D65, seed, **kw)
+    sched = dict(chains=args.tracer_chains, wave_paths_log2=args.tracer_wave_log2,
+                 wave_bounces=args.tracer_wave_bounces)  # scheduling only: the image is the same
+    tr = sb.GpuTracer(ctx, scene, cam, W, H, sb.D65, seed, **sched, **kw)
     sp = C.c_void_p()
     _lib.check(_lib.lib.sc_tracer_stream(tr.h, C.byref(sp)))
     st = torch.cuda.ExternalStream(sp.value, device=dev)
@@ -735,7 +743,9 @@ def run_gpu_tracer(args, rank, world, local_rank):
     # intersects the ray and read by the shade, the path state (44 B) written
     # and read; per path, its XYZ (12 B) written and read by the per-pixel sums
     qbytes = (segments - samples) * (2 * 20 + 2 * 44) + samples * 2 * 12
-    waves = -(-(W * H) // max(1, TRACER_WAVE_PATHS // SPP))
+    wave_paths = 1 << args.tracer_wave_log2 if args.tracer_wave_log2 else TRACER_WAVE_PATHS
+    wb = args.tracer_wave_bounces or 2
+    waves = -(-(W * H) // max(1, wave_paths // SPP))
     line = {
         "metric": "path samples/s (hero-wavelength camera tracer, 4 lanes, depth 8)",
         "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -744,13 +754,14 @@ def run_gpu_tracer(args, rank, world, local_rank):
         "config": {"workload": "tracer: SF11 prism on a diffuse ground (albedo 0.8), D65 sphere emitter r=0.2 at "
                                "(2,3,1), 1280x720, 64 spp, depth 8, roulette after bounce 3",
                    "samples_per_step": samples * world, "l2": "flushed between steps (256 MB write outside the events)",
+                   "schedule": {"chains": args.tracer_chains or 3, "wave_paths": wave_paths, "wave_bounces": wb},
                    "parallelism": "independent frames per rank (own seed), no collective"},
         "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": C.sizeof(cam.c),
                 "d2h_bytes_per_step": 3 * W * H * 4,
                 "path": "sc_tracer_set_camera + clear_accum + accumulate(64) + read_xyz (host f32 XYZ)"},
         # per wave: two shades (the first makes and intersects the primary rays
         # and intersects the second bounce's rays), the tail, per-pixel sums
-        "gpu_launches": args.steps * waves * (min(kw["max_depth"], 2) + (1 if kw["max_depth"] > 2 else 0) + 1),
+        "gpu_launches": args.steps * waves * (min(kw["max_depth"], wb) + (1 if kw["max_depth"] > wb else 0) + 1),
         "kernels": {"accumulate_ms": statistics.mean(step_ms)},
         "roofline": {"bound": "hbm", "achieved": qbytes / step_s / 1e9, "peak": hbm, "unit": "GB/s",
                      "frac": qbytes / step_s / 1e9 / hbm, "traffic": ncu_traffic("tracer")[0],
