@@ -141,9 +141,14 @@ struct sc_batch {
             d.flags = flags.p + flag_off[j];
             d.mask_words = geom[j].words;
         }
-        if (!h_stage) {
-            SC_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_stage), h_jobs.size() * sizeof(BatchJobDev)));
-            SC_CUDA(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+        if (!h_stage || !staged) {
+            free_stage();
+            cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&h_stage), h_jobs.size() * sizeof(BatchJobDev));
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&staged, cudaEventDisableTiming);
+            if (e != cudaSuccess) {
+                free_stage();
+                SC_CUDA(e);
+            }
         } else {
             SC_CUDA(cudaEventSynchronize(staged));  // the last upload has read the pinned copy
         }
