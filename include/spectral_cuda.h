@@ -317,6 +317,38 @@ int sc_sensor_reduce_device(sc_ctx* ctx, uint32_t width, uint32_t height, uint32
                             void* film_dev, uint32_t* flags_dev, float* xyz_dev, int drain,
                             void* stream);
 
+/* ---- one scene split over GPUs (no counterpart in the reference, which runs
+ * one GPU) --------------------------------------------------------------- */
+/* Every GPU traces its range of photons into its own device film
+ * (sc_trace_photons_device); each then reduces its own band of image rows
+ * from the SUM of all the films, reading the other GPUs' films as peer memory
+ * (NVLink), so no film is summed into one or sent whole: a GPU reads 1/N of
+ * every film, and the XYZ bands (a few MB) are gathered.  The int64 sum is
+ * exact: each band is bit-identical to the same rows of the image of one film
+ * that traced every photon.
+ *
+ * sc_ipc_export: a CUDA IPC handle (64 bytes) of the allocation holding
+ * dev_ptr (e.g. a torch tensor's storage) and dev_ptr's offset in it, to pass
+ * to the other processes.  sc_ipc_import: map another process's allocation
+ * into this context (peer access enabled as needed); *dev_ptr = its base +
+ * offset.  sc_ipc_close: unmap it (the same offset).  The exporting process
+ * must keep the memory alive until every importer has closed it. */
+int sc_ipc_export(sc_ctx* ctx, const void* dev_ptr, unsigned char handle[64], size_t* offset);
+int sc_ipc_import(sc_ctx* ctx, const unsigned char handle[64], size_t offset, void** dev_ptr);
+int sc_ipc_close(sc_ctx* ctx, void* dev_ptr, size_t offset);
+/* The sensor reduction (as sc_sensor_reduce_device, without draining) of the
+ * sum of n_films device films of the same geometry (films_dev: a host array
+ * of 1..8 device pointers, this GPU's own film and mapped peer films, 16-byte
+ * aligned) for image rows [row_begin, row_end) only: row_begin a multiple of
+ * 8, row_end a multiple of 8 or the height.  Writes those rows of the full
+ * interleaved XYZ image at xyz_dev (3*w*h floats).  Every film must be
+ * complete (all ranks' traces finished) before the call is ordered; the films
+ * are read, not changed. */
+int sc_sensor_reduce_peers(sc_ctx* ctx, uint32_t width, uint32_t height, uint32_t channels,
+                           float lambda_min, float lambda_max, uint32_t scale_log2,
+                           const int64_t* const* films_dev, uint32_t n_films, uint32_t row_begin,
+                           uint32_t row_end, float* xyz_dev, void* stream);
+
 /* ---- allocation-free render (no counterpart in the reference) ----------
  * For callers that cannot allocate device memory: hosts whose framework owns
  * all device memory through its own pool (a raw cudaMalloc would bypass it and

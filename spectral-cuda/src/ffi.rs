@@ -186,6 +186,13 @@ extern "C" {
     pub fn sc_trace_photons_device(ctx: *mut ScCtx, desc: *const ScTraceDesc, photon_base: u32, count: u32, film_dev: *mut c_void, flags_dev: *mut u32, stream: *mut c_void) -> c_int;
     pub fn sc_trace_stats_device(ctx: *mut ScCtx, desc: *const ScTraceDesc, photon_base: u32, count: u32, out_dev: *mut u64, stream: *mut c_void) -> c_int;
     pub fn sc_sensor_reduce_device(ctx: *mut ScCtx, width: u32, height: u32, channels: u32, lambda_min: f32, lambda_max: f32, scale_log2: u32, film_dev: *mut c_void, flags_dev: *mut u32, xyz_dev: *mut f32, drain: c_int, stream: *mut c_void) -> c_int;
+
+    // One scene split over GPUs: IPC mapping of the peers' films and the
+    // band reduction of their sum.
+    pub fn sc_ipc_export(ctx: *mut ScCtx, dev_ptr: *const c_void, handle: *mut u8, offset: *mut usize) -> c_int;
+    pub fn sc_ipc_import(ctx: *mut ScCtx, handle: *const u8, offset: usize, dev_ptr: *mut *mut c_void) -> c_int;
+    pub fn sc_ipc_close(ctx: *mut ScCtx, dev_ptr: *mut c_void, offset: usize) -> c_int;
+    pub fn sc_sensor_reduce_peers(ctx: *mut ScCtx, width: u32, height: u32, channels: u32, lambda_min: f32, lambda_max: f32, scale_log2: u32, films_dev: *const *const i64, n_films: u32, row_begin: u32, row_end: u32, xyz_dev: *mut f32, stream: *mut c_void) -> c_int;
     pub fn sc_trace_xyz_noalloc(tables_5x71: *const f32, desc: *const ScTraceDesc, photon_base: u32, count: u32, xyz_dev: *mut f32, stream: *mut c_void) -> c_int;
     pub fn sc_batch_create(ctx: *mut ScCtx, jobs: *const ScSceneJob, n_jobs: u32, tuning: *const ScBatchTuning, out: *mut *mut ScBatch) -> c_int;
     pub fn sc_batch_destroy(b: *mut ScBatch) -> c_int;

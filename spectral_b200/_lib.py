@@ -203,6 +203,10 @@ PROTOTYPES = {
     "sc_server_stats": (_i32, [_vp, P(_u64), P(_u64), P(_u32), P(_u32), P(_u32)]),
     "sc_trace_xyz_noalloc": (_i32, [P(_f32), P(sc_trace_desc), _u32, _u32, _vp, _vp]),
     "sc_film_bytes": (_sz, [_u32, _u32, _u32]),
+    "sc_ipc_export": (_i32, [_vp, _vp, P(C.c_ubyte), P(_sz)]),
+    "sc_ipc_import": (_i32, [_vp, P(C.c_ubyte), _sz, P(_vp)]),
+    "sc_ipc_close": (_i32, [_vp, _vp, _sz]),
+    "sc_sensor_reduce_peers": (_i32, [_vp, _u32, _u32, _u32, _f32, _f32, _u32, P(_vp), _u32, _u32, _u32, _vp, _vp]),
     "sc_film_flag_bytes": (_sz, [_u32, _u32]),
     "sc_trace_photons_device": (_i32, [_vp, P(sc_trace_desc), _u32, _u32, _vp, _vp, _vp]),
     "sc_sensor_reduce_device": (_i32, [_vp, _u32, _u32, _u32, _f32, _f32, _u32, _vp, _vp, _vp, _i32, _vp]),

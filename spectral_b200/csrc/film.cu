@@ -154,6 +154,34 @@ __global__ void __launch_bounds__(kReduceThreads, 3) reduce_kernel(const ReduceP
         sm, part);
 }
 
+// The sum of several films (one per GPU of a split scene: this GPU's own and
+// its peers', read over NVLink) reduced for a range of tiles.  Each tile is
+// staged as the exact int64 sum of the films' cells, then reduced by the
+// single-film code, so a band equals the same band of the summed film's
+// image.  The films are read, not drained; every tile counts as lit.
+__global__ void __launch_bounds__(kReduceThreads, 3) reduce_peers_kernel(const ReduceParams p, const PeerFilms pf,
+                                                                         uint32_t tile_begin, uint32_t tile_end) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* part = reinterpret_cast<double*>(smem);
+    unsigned long long* sm = reinterpret_cast<unsigned long long*>(smem + 4 * 64 * 3 * sizeof(double));
+    const uint32_t n2 = kTilePixels * p.channels / 2u;
+    for (uint32_t tile = tile_begin + blockIdx.x; tile < tile_end; tile += gridDim.x) {
+        const size_t off2 = (size_t)tile * kTilePixels * p.channels / 2u;
+        for (uint32_t i = threadIdx.x; i < n2; i += blockDim.x) {
+            ulonglong2 acc = make_ulonglong2(0ull, 0ull);
+            for (uint32_t f = 0; f < pf.n; ++f) {
+                const ulonglong2 v = __ldcs(reinterpret_cast<const ulonglong2*>(pf.film[f]) + off2 + i);
+                acc.x += v.x;
+                acc.y += v.y;
+            }
+            reinterpret_cast<ulonglong2*>(sm)[i] = acc;
+        }
+        __syncthreads();
+        reduce_staged(tile_ref(p, tile, true), false, sm, part);
+        __syncthreads();
+    }
+}
+
 // Many films, step 1: one warp per dirty-mask word (32 tiles).  Clean tiles get
 // zeros in the image; dirty ones go to the list (one atomic per warp), and
 // when draining the word is cleared.  Words are numbered over all films
@@ -386,6 +414,16 @@ cudaError_t launch_reduce(const ReduceParams& p, bool drain, cudaStream_t s) {
     if (grid == 0) return cudaSuccess;
     if (drain) reduce_kernel<true><<<grid, kReduceThreads, smem, s>>>(p);
     else reduce_kernel<false><<<grid, kReduceThreads, smem, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_peers(const ReduceParams& p, const PeerFilms& films, uint32_t tile_begin, uint32_t tile_end,
+                                cudaStream_t s) {
+    if (tile_end <= tile_begin || films.n == 0) return cudaSuccess;
+    const size_t smem = reduce_smem(p.channels);
+    uint32_t grid = reduce_grid(reinterpret_cast<const void*>(&reduce_peers_kernel), 2, smem);
+    if (grid > tile_end - tile_begin) grid = tile_end - tile_begin;
+    reduce_peers_kernel<<<grid, kReduceThreads, smem, s>>>(p, films, tile_begin, tile_end);
     return cudaGetLastError();
 }
 

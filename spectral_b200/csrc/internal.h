@@ -110,6 +110,17 @@ struct ReduceParams {
 };
 cudaError_t launch_reduce(const ReduceParams& p, bool drain, cudaStream_t s);
 
+// Up to 8 films of the same geometry (one per GPU of a split scene, peers'
+// films mapped into this process); the reduction of their exact sum for tiles
+// [tile_begin, tile_end) into p.xyz (p.film and p.flags unused).
+constexpr uint32_t kMaxPeerFilms = 8;
+struct PeerFilms {
+    const unsigned long long* film[kMaxPeerFilms];
+    uint32_t n;
+};
+cudaError_t launch_reduce_peers(const ReduceParams& p, const PeerFilms& films, uint32_t tile_begin, uint32_t tile_end,
+                                cudaStream_t s);
+
 // Batched reduction over many films described in device memory.
 struct FilmDesc {
     unsigned long long* film; uint32_t* flags; float* xyz; const float* binw;

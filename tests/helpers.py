@@ -78,3 +78,20 @@ def oracle_job_xyz(job):
     _, _, fs = oracle.render_point(sc, cam, beam, p, 0, job.n_photons, f32=False, xyz=False, spec=True)
     w = oracle.bin_weights(o.bins, o.lambda_min, o.lambda_max).astype(np.float64)
     return (fs.reshape(-1, o.bins).astype(np.float64) @ w.T).reshape(-1) * 2.0 ** -32
+
+
+def device_desc(sb, _lib, torch, scene, cam, beam, w, h, seed, bins, keep, estimator=0, scale_log2=32):
+    """An sc_trace_desc for the device-pointer entry points, its scene records
+    copied to the device (the tensors are appended to `keep`)."""
+    prims, np_, planes, npl, mats, nm = scene.arrays()
+
+    def dev(arr, n, size):
+        t = torch.frombuffer(bytearray(bytes(arr)[: n * size] or b"\0"), dtype=torch.uint8).cuda()
+        keep.append(t)
+        return t.data_ptr()
+
+    opts = _lib.sc_film_options(bins, 380.0, 730.0, 8, scale_log2, estimator)
+    w8 = sb.VolWeights()
+    return _lib.sc_trace_desc(dev(prims, np_, 32), np_, dev(planes, npl, 16), npl, dev(mats, nm, 16), nm, cam.c,
+                              beam.c, _lib.sc_vol_weights(w8.sigma_s, w8.sigma_t, w8.g), w, h, seed, 1, 14.0, opts,
+                              None)
