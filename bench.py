@@ -135,6 +135,9 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="window of the 200 req/s Poisson stream replayed in real time for the served numbers "
                          "(batch and serve workloads; 0: none)")
+    ap.add_argument("--split-exchange", choices=["allreduce", "peer"], default="allreduce",
+                    help="split workload: sum the films with one NCCL all-reduce, or reduce each rank's band of "
+                         "tile rows from every rank's film mapped as peer memory (CUDA IPC) and gather the bands")
     ap.add_argument("--tracer-chains", type=int, default=0,
                     help="tracer schedule: waves in flight (0: the library's default, 3)")
     ap.add_argument("--tracer-wave-log2", type=int, default=0,
@@ -1018,8 +1021,46 @@ def run_gpu_split(args, rank, world, local_rank):
     xyz = torch.empty(3 * W * H, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     sp = C.c_void_p(stream.cuda_stream)
+    peer = args.split_exchange == "peer"
+    if peer:
+        from spectral_b200.shard import PeerFilms, reduce_band_peers, tile_row_band
+        peers = PeerFilms(ctx, film) if dist else None
+        ptrs = peers.ptrs if dist else [film.data_ptr()]
+        rb, re_ = tile_row_band(rank, world, H)
+        rows = max(e - b for b, e in (tile_row_band(r, world, H) for r in range(world)))
+        band = torch.zeros((rows, W, 3), dtype=torch.float32, device=dev)
+        bands = torch.empty((world, rows, W, 3), dtype=torch.float32, device=dev)
+        ready = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def step_peer(ev=None):
+        # trace; a one-word all-reduce orders every rank's trace before any
+        # band reads it; each rank reduces its band from all films; gathering
+        # the bands orders every read before the films are cleared
+        if ev:
+            ev[0].record(stream)
+        _lib.check(_lib.lib.sc_trace_photons_device(ctx.h, C.byref(desc), b0, b1 - b0, C.c_void_p(film.data_ptr()),
+                                                    C.c_void_p(flags.data_ptr()), sp))
+        if ev:
+            ev[1].record(stream)
+        if dist:
+            dist.all_reduce(ready)
+        reduce_band_peers(ctx, ptrs, W, H, B, opts, rb, re_, xyz.data_ptr(), stream.cuda_stream)
+        if dist:
+            band[: re_ - rb].copy_(xyz.view(H, W, 3)[rb:re_])
+            dist.all_gather_into_tensor(bands, band)
+            for r in range(world):
+                b, e = tile_row_band(r, world, H)
+                xyz.view(H, W, 3)[b:e].copy_(bands[r, : e - b])
+        if ev:
+            ev[2].record(stream)
+        film.zero_()
+        flags.zero_()
+        if ev:
+            ev[3].record(stream)
 
     def step(ev=None):
+        if peer:
+            return step_peer(ev)
         if ev:
             ev[0].record(stream)
         _lib.check(_lib.lib.sc_trace_photons_device(ctx.h, C.byref(desc), b0, b1 - b0, C.c_void_p(film.data_ptr()),
@@ -1067,7 +1108,13 @@ def run_gpu_split(args, rank, world, local_rank):
                           lambda_min=cfg["lambda_min"], lambda_max=cfg["lambda_max"], max_bounces=cfg["max_bounces"])
     host_xyz = torch.empty(3 * W * H, dtype=torch.float32, pin_memory=True).numpy()
 
+    host_t = torch.from_numpy(host_xyz)
+
     def e2e_step():
+        if peer:  # the device-pointer path with the peer-band exchange, the image back to the host
+            step_peer()
+            host_t.copy_(xyz)
+            return
         if dist:
             trace_sharded(pf, N, cfg["seed"])
         else:
@@ -1090,6 +1137,10 @@ def run_gpu_split(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     pf.close()
+    if peer and dist:
+        torch.cuda.synchronize()
+        dist.barrier()  # every rank is done with the others' films
+        peers.close()
     if rank != 0:
         return None
     film_bytes = film.numel() * 8
@@ -1102,15 +1153,22 @@ def run_gpu_split(args, rank, world, local_rank):
         "config": {"workload": "split: the rainbow scene (water sphere r=1, beam 2.2, 1920x1080x64 bins), %d photons "
                                "split into contiguous ranges over %d rank(s)" % (N, world),
                    "photons_per_step": N, "film": [W, H, B],
-                   "parallelism": "photon ranges per rank + one int64 NCCL all-reduce of the film per step"},
-        "kernels": {"trace_ms": statistics.mean(parts[0]), "allreduce_ms": ar_ms,
-                    "reduce_ms": statistics.mean(parts[2])},
-        "allreduce": {"bytes": film_bytes, "ms": ar_ms,
+                   "parallelism": ("photon ranges per rank; each rank reduces its band of tile rows from every "
+                                   "rank's film as peer memory, bands all-gathered" if peer else
+                                   "photon ranges per rank + one int64 NCCL all-reduce of the film per step"),
+                   "exchange": args.split_exchange},
+        "kernels": ({"trace_ms": statistics.mean(parts[0]), "band_reduce_and_gather_ms": ar_ms,
+                     "clear_ms": statistics.mean(parts[2])} if peer else
+                    {"trace_ms": statistics.mean(parts[0]), "allreduce_ms": ar_ms,
+                     "reduce_ms": statistics.mean(parts[2])}),
+        "allreduce": None if peer else {"bytes": film_bytes, "ms": ar_ms,
                       "bus_gbs": (film_bytes * 2 * (world - 1) / world / (ar_ms / 1e3) / 1e9) if world > 1 and ar_ms > 0
                       else None},
         "e2e": {"value": N * e2e_steps / e2e_s, "unit": "photons/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 3 * W * H * 4,
-                "path": "shard.trace_sharded (own range + film all-reduce) + read_accum (host f32 XYZ) + clear"},
+                "path": ("sc_trace_photons_device (own range) + sc_sensor_reduce_peers (own band of every film) + "
+                         "band all-gather + image to pinned host memory" if peer else
+                         "shard.trace_sharded (own range + film all-reduce) + read_accum (host f32 XYZ) + clear")},
         "gpu_launches": args.steps * (2 + 3),  # per step: sort (3) + photon kernel, drain
         "clocks": clk.summary(),
     }
