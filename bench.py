@@ -71,7 +71,7 @@ NCU_TRAFFIC = {
     "prism": (2092544, "photon_kernel, one capture"),
     "rainbow": (4839725056, "order_count + order_scan + order_scatter + photon_kernel, one capture"),
     "beam": (3842560, "beam_kernel, one capture"),
-    "tracer": (7015925760, "all tracer wave kernels of one accumulate(64), one capture"),
+    "tracer": (6145474816, "all tracer wave kernels of one accumulate(64), one capture"),
     "batch": (3953000000, "batch_kernel + reduce_scan + reduce_list, scaled from a capture of the first 64 "
                           "scenes (4.4 GB of films): batch_kernel by photons, reduce_scan by film bytes, reduce_list by "
                           "lit-tile bytes"),
@@ -89,7 +89,7 @@ NCU_INST = {
                                                   "(48,957,886 photons each), per photon"),
     "prism": (324289908 / 2 / (1 << 20), 25.60, "photon_kernel: two launches of 2^20 photons, per photon"),
     "rainbow": (5568513387 / (1 << 26), 23.90, "photon_kernel: one launch of 2^26 photons, per photon"),
-    "tracer": (3718315830 / 58982400, 27.64, "tr_shade, tr_tail, tr_accumulate: the 60 launches of one "
+    "tracer": (3642531467 / 58982400, 27.66, "tr_shade, tr_tail, tr_accumulate: the 60 launches of one "
                                              "accumulate(64), per path sample"),
 }
 
@@ -742,10 +742,10 @@ def run_gpu_tracer(args, rank, world, local_rank):
     # cosine sampling, 4-lane throughput and radiance update)
     flops = segments * (14 * n_planes + 20 + 60)
     # wavefront queue traffic: per segment after the first (the first bounce
-    # makes its rays in place), the hit (20 B) written by the kernel that
-    # intersects the ray and read by the shade, the path state (44 B) written
-    # and read; per path, its XYZ (12 B) written and read by the per-pixel sums
-    qbytes = (segments - samples) * (2 * 20 + 2 * 44) + samples * 2 * 12
+    # makes its rays in place), the path state (44 B) written by the bounce
+    # before and read by the one that intersects and shades it; per path, its
+    # XYZ (12 B) written and read by the per-pixel sums
+    qbytes = (segments - samples) * 2 * 44 + samples * 2 * 12
     wave_paths = 1 << args.tracer_wave_log2 if args.tracer_wave_log2 else TRACER_WAVE_PATHS
     wb = args.tracer_wave_bounces or 2
     waves = -(-(W * H) // max(1, wave_paths // SPP))
@@ -770,8 +770,8 @@ def run_gpu_tracer(args, rank, world, local_rank):
                      "frac": qbytes / step_s / 1e9 / hbm, "traffic": ncu_traffic("tracer")[0],
                      "traffic_source": ncu_traffic("tracer")[1], "kernel": "tracer wave kernels (one accumulate)",
                      "peak_source": "%s hbm_gbs" % peak_note,
-                     "algorithmic": "wavefront queue bytes: 128 B per path segment after the first bounce, 24 B of "
-                                    "XYZ per path (%d segments, %d paths per step)" % (segments, samples)},
+                     "algorithmic": "wavefront queue bytes: 88 B of path state per path segment after the first "
+                                    "bounce, 24 B of XYZ per path (%d segments, %d paths per step)" % (segments, samples)},
         "roofline_fp32": {"kernel": "tr_intersect + tr_shade", "counted_flops": flops,
                           "achieved_tflops": flops / step_s / 1e12, "peak_tflops": fp32_peak,
                           "frac": flops / step_s / 1e12 / fp32_peak,

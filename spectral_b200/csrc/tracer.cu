@@ -4,15 +4,14 @@
 // GPU mirror spectral-gpu/src/shaders/trace.wgsl:419-537) as a wavefront:
 //   generate  one path per (pixel, sample): stream key mix2(pixel, sample index),
 //             jittered primary ray, hero-comb wavelength draw (spectrum.rs:20-32);
-//   intersect nearest scene hit (+ the optional spherical emitter) per ray
-//             (primary rays where they are made, in the first shade kernel;
-//             later rays in the shade kernel that queued them);
+//   intersect nearest scene hit (+ the optional spherical emitter) per ray,
+//             in the kernel that shades it (primary rays where they are made;
+//             later rays as the next bounce reads them from the dense queue);
 //   shade     background / emission at termination, Fresnel / refract / TIR or
 //             Lambertian scatter, dispersion collapse to the hero lane, optional
 //             Russian roulette; survivors are compacted into the next queue with
 //             warp ballots, one atomic per block and shared-memory staging so the
-//             SoA writes are contiguous, and the compacted rays are intersected
-//             at once;
+//             SoA writes are contiguous;
 //   tail      the few paths alive after the compacted bounces finish in one
 //             launch, kept compacted per CTA bounce by bounce;
 //   accumulate each pixel's samples summed in sample order (the CPU's order), so
@@ -205,18 +204,18 @@ __device__ __forceinline__ bool shade_path(const TracerSmem& s, const SceneView&
     return survive;
 }
 
-// ISECT: the surviving rays, once compacted into shared memory, are also
-// intersected here (the next bounce's hits go to `hout`), so they do not make a
-// queue round trip through a separate intersect launch.
+// One compacted bounce: each path's ray is intersected and shaded here, and
+// the survivors are compacted into the next ray queue (no hit queue: the
+// bounce that reads a ray intersects it, from the dense queue).
 // GEN: the first bounce with no queue in: each path's primary ray is made here
 // (stream key mix2(pixel, sample index), jittered through the pixel, hero-comb
 // draw), intersected in place and shaded.  Paths of a wave are numbered
 // sample-major (path i = sample s of wave pixel j with i = s * n_pixels + j):
 // neighbouring threads trace neighbouring pixels, and the per-pixel sums read
 // the results coalesced.  counts[1..] are zero at entry.
-template <bool ISECT, bool GEN>
+template <bool GEN>
 __global__ void __launch_bounds__(kShadeThreads, kStageCtasPerSm) tr_shade(const TracerParams* __restrict__ gp, uint32_t bounce,
-                                                          RayQueue q, HitQueue hq, RayQueue out, HitQueue hout,
+                                                          RayQueue q, RayQueue out,
                                                           uint32_t* counts, float* result, uint32_t first_pixel,
                                                           uint32_t n_pixels, uint32_t n_paths,
                                                           const uint32_t* __restrict__ base) {
@@ -260,9 +259,12 @@ __global__ void __launch_bounds__(kShadeThreads, kStageCtasPerSm) tr_shade(const
             P.o = mk(q.ox[i], q.oy[i], q.oz[i]);
             P.d = mk(q.dx[i], q.dy[i], q.dz[i]);
             P.tp = q.tp[i]; P.u = q.u[i]; P.rs = q.rng[i]; P.id = q.id[i]; P.flags = q.flags[i];
-            const uint32_t info = hq.info[i];
-            const f3 nrm = (info >> 24) == 1u ? mk(hq.nx[i], hq.ny[i], hq.nz[i]) : mk(0.0f, 0.0f, 0.0f);
-            survive = shade_path(s, S, bounce, P, hq.t[i], nrm, info, result);
+            float t;
+            f3 nrm;
+            uint32_t info;
+            trace_hit(s, S, P.o, P.d, t, nrm, info);
+            if ((info >> 24) != 1u) nrm = mk(0.0f, 0.0f, 0.0f);
+            survive = shade_path(s, S, bounce, P, t, nrm, info, result);
         }
         const f3 o = P.o, d = P.d;
         const float tp = P.tp, u = P.u;
@@ -294,16 +296,6 @@ __global__ void __launch_bounds__(kShadeThreads, kStageCtasPerSm) tr_shade(const
             out.dx[g] = st_f[3][j]; out.dy[g] = st_f[4][j]; out.dz[g] = st_f[5][j];
             out.tp[g] = st_f[6][j]; out.u[g] = st_f[7][j];
             out.rng[g] = st_u[0][j]; out.id[g] = st_u[1][j]; out.flags[g] = st_u[2][j];
-            if (ISECT) {  // the next bounce's hit, by converged (compacted) threads
-                float t;
-                f3 nrm;
-                uint32_t info;
-                trace_hit(s, S, mk(st_f[0][j], st_f[1][j], st_f[2][j]), mk(st_f[3][j], st_f[4][j], st_f[5][j]), t,
-                          nrm, info);
-                hout.t[g] = t;
-                if ((info >> 24) == 1u) { hout.nx[g] = nrm.x; hout.ny[g] = nrm.y; hout.nz[g] = nrm.z; }
-                hout.info[g] = info;
-            }
         }
         __syncthreads();
     }
@@ -431,10 +423,10 @@ size_t tracer_dyn_smem(uint32_t n_planes) { return (size_t)(n_planes ? n_planes 
 int tracer_grid(int sms) {
     int a = 0, b = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, tr_tail, 256, tracer_dyn_smem(SC_MAX_PLANES));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tr_shade<true, false>, kShadeThreads,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, tr_shade<false>, kShadeThreads,
                                                   tracer_dyn_smem(SC_MAX_PLANES));
     int c = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, tr_shade<true, true>, kShadeThreads,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, tr_shade<true>, kShadeThreads,
                                                   tracer_dyn_smem(SC_MAX_PLANES));
     int k = a < b ? a : b;
     k = k < c ? k : c;
@@ -448,32 +440,21 @@ cudaError_t launch_tracer_wave(const TracerParams* d_params, const TracerLaunch&
     // wavefront with compaction for the first bounces, then the tail in place;
     // the first bounce makes, intersects and shades the primary rays in one kernel
     const uint32_t wave_bounces = L.max_depth < L.wave_bounces ? L.max_depth : L.wave_bounces;
-    // bounce b shades the hits of bounce b and, while more wave bounces follow,
-    // intersects its compacted survivors too (hit queues alternate)
+    // bounce b intersects and shades the rays of bounce b and queues its
+    // compacted survivors (ray queues alternate)
     for (uint32_t b = 0; b < wave_bounces; ++b) {
         const RayQueue& in = (b & 1u) ? L.qb : L.qa;
         const RayQueue& out = (b & 1u) ? L.qa : L.qb;
-        const HitQueue& hin = (b & 1u) ? L.hits2 : L.hits;
-        const HitQueue& hout = (b & 1u) ? L.hits : L.hits2;
-        const uint32_t g = L.grid;
-        const bool isect = b + 1u < wave_bounces;
         if (b == 0) {
             // the first bounce makes its primary rays itself: no queue in; later
-            // bounces count their rays from zero
+            // bounces (and the tail's claim counter) count from zero
             cudaError_t e = cudaMemsetAsync(L.counts + 1, 0, (L.max_depth + 1) * sizeof(uint32_t), st);
             if (e != cudaSuccess) return e;
-            if (isect)
-                tr_shade<true, true><<<g, kShadeThreads, dyn, st>>>(d_params, 0u, in, hin, out, hout, L.counts,
-                                                                    L.result, first_pixel, n_pixels, n_paths, L.d_base);
-            else
-                tr_shade<false, true><<<g, kShadeThreads, dyn, st>>>(d_params, 0u, in, hin, out, hout, L.counts,
-                                                                     L.result, first_pixel, n_pixels, n_paths, L.d_base);
-        } else if (isect) {
-            tr_shade<true, false><<<g, kShadeThreads, dyn, st>>>(d_params, b, in, hin, out, hout, L.counts, L.result,
-                                                                 0u, 1u, 0u, L.d_base);
+            tr_shade<true><<<L.grid, kShadeThreads, dyn, st>>>(d_params, 0u, in, out, L.counts, L.result, first_pixel,
+                                                              n_pixels, n_paths, L.d_base);
         } else {
-            tr_shade<false, false><<<g, kShadeThreads, dyn, st>>>(d_params, b, in, hin, out, hout, L.counts, L.result,
-                                                                  0u, 1u, 0u, L.d_base);
+            tr_shade<false><<<L.grid, kShadeThreads, dyn, st>>>(d_params, b, in, out, L.counts, L.result, 0u, 1u, 0u,
+                                                               L.d_base);
         }
     }
     if (L.max_depth > wave_bounces)

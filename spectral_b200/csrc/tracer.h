@@ -28,14 +28,8 @@ struct RayQueue {
     float *ox, *oy, *oz, *dx, *dy, *dz, *tp, *u;
     uint32_t *rng, *id, *flags;  // flags: valid lanes (bits 0-7), depth (bits 8-15)
 };
-struct HitQueue {
-    float *t, *nx, *ny, *nz;
-    uint32_t* info;  // material | front_face << 16 | kind << 24 (0 miss, 1 surface, 2 emitter)
-};
-
 struct TracerLaunch {
-    RayQueue qa, qb;
-    HitQueue hits, hits2;   // hits of the bounce being shaded / of the next one
+    RayQueue qa, qb;        // rays of the bounce being shaded / of the next one
     uint32_t* counts;       // max_depth + 1 queue lengths, then the tail's claim counter
     float* result;          // 3 per path of the wave
     float* sum;             // 3 * w * h running sum

@@ -79,9 +79,9 @@ struct sc_tracer {
         if (paths <= wave_cap) return SC_OK;
         drop_graph();
         const size_t n = paths;
-        // per chain: 2 ray queues x 8 floats, 2 hit queues x 4 floats, result 3; 2 ray queues x 3 u32, 2 hit infos
-        SC_CUDA(qbuf.alloc(chains * (n * 8 * 2 + n * 4 * 2 + 3 * n)));
-        SC_CUDA(qbuf_u.alloc(chains * (n * 3 * 2 + n * 2)));
+        // per chain: 2 ray queues x 8 floats, result 3; 2 ray queues x 3 u32
+        SC_CUDA(qbuf.alloc(chains * (n * 8 * 2 + 3 * n)));
+        SC_CUDA(qbuf_u.alloc(chains * (n * 3 * 2)));
         float* f = qbuf.p;
         uint32_t* u = qbuf_u.p;
         for (uint32_t c = 0; c < chains; ++c) {
@@ -93,13 +93,6 @@ struct sc_tracer {
                 f += 8 * n;
                 q->rng = u; q->id = u + n; q->flags = u + 2 * n;
                 u += 3 * n;
-            }
-            HitQueue* hs[2] = {&Lc.hits, &Lc.hits2};
-            for (HitQueue* hq : hs) {
-                hq->t = f; hq->nx = f + n; hq->ny = f + 2 * n; hq->nz = f + 3 * n;
-                f += 4 * n;
-                hq->info = u;
-                u += n;
             }
             Lc.result = f;
             f += 3 * n;
