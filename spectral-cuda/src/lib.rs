@@ -438,3 +438,46 @@ pub fn check_determinism(ctx: &CudaContext, width: u32, height: u32, seed: u32, 
     check(unsafe { ffi::sc_atomic_film_check_determinism(ctx.raw, width, height, seed, n, &mut first) });
     if first < 0 { Ok(()) } else { Err(first as usize) }
 }
+
+/// One scene split over GPUs without an all-reduce: every process traces its
+/// photon range into its own device film (`ffi::sc_trace_photons_device`),
+/// maps the other processes' films with `ipc_import`, and reduces its band of
+/// whole tile rows from the exact sum of all of them (`reduce_band_peers`);
+/// the XYZ bands are then gathered by the caller's transport.
+pub mod split {
+    use super::{check, ffi, CudaContext};
+    use std::os::raw::c_void;
+
+    /// A CUDA IPC handle of the allocation holding `dev_ptr`, and the offset of
+    /// `dev_ptr` in it, to send to the other processes.
+    pub fn ipc_export(ctx: &CudaContext, dev_ptr: *const c_void) -> ([u8; 64], usize) {
+        let mut handle = [0u8; 64];
+        let mut offset = 0usize;
+        check(unsafe { ffi::sc_ipc_export(ctx.raw, dev_ptr, handle.as_mut_ptr(), &mut offset) });
+        (handle, offset)
+    }
+
+    /// Another process's device memory mapped into this context (close it with
+    /// `ipc_close` before that process frees it).
+    pub fn ipc_import(ctx: &CudaContext, handle: &[u8; 64], offset: usize) -> *mut c_void {
+        let mut p = std::ptr::null_mut();
+        check(unsafe { ffi::sc_ipc_import(ctx.raw, handle.as_ptr(), offset, &mut p) });
+        p
+    }
+
+    pub fn ipc_close(ctx: &CudaContext, dev_ptr: *mut c_void, offset: usize) {
+        check(unsafe { ffi::sc_ipc_close(ctx.raw, dev_ptr, offset) });
+    }
+
+    /// Rows [row_begin, row_end) of the XYZ image of the sum of `films` (device
+    /// pointers, this GPU's and mapped peers'), written into `xyz_dev`.
+    #[allow(clippy::too_many_arguments)]
+    pub fn reduce_band_peers(ctx: &CudaContext, films: &[*const i64], width: u32, height: u32, channels: u32,
+                             lambda_min: f32, lambda_max: f32, scale_log2: u32, row_begin: u32, row_end: u32,
+                             xyz_dev: *mut f32, stream: *mut c_void) {
+        check(unsafe {
+            ffi::sc_sensor_reduce_peers(ctx.raw, width, height, channels, lambda_min, lambda_max, scale_log2,
+                                        films.as_ptr(), films.len() as u32, row_begin, row_end, xyz_dev, stream)
+        });
+    }
+}
