@@ -184,3 +184,17 @@ def test_two_rank_film_reduce_is_exact(tmp_path):
 def test_float_films_are_refused():
     with pytest.raises(TypeError):
         allreduce_film_(torch.zeros(4, dtype=torch.float32))
+
+
+def test_tile_row_bands_cover_the_image_on_tile_boundaries():
+    """The peer-band split gives every rank a band of whole 8-row tile rows:
+    contiguous, covering [0, height), each starting on a multiple of 8."""
+    from spectral_b200.shard import tile_row_band
+    for height in (1, 7, 8, 9, 75, 80, 720, 1080):
+        for world in (1, 2, 3, 5, 8, 16):
+            bands = [tile_row_band(r, world, height) for r in range(world)]
+            assert bands[0][0] == 0 and bands[-1][1] == height
+            for (b0, e0), (b1, e1) in zip(bands, bands[1:]):
+                assert e0 == b1
+            for b, e in bands:
+                assert b <= e and b % 8 == 0 and (e % 8 == 0 or e == height)
